@@ -1,0 +1,443 @@
+"""Benchmark of the SPLA local contraction on B200.
+
+Workload (default): complex-double pgemm_ssb, C = A^H B, m = n = 1024,
+k = 250000, A and B complex Gaussian scaled by 1/sqrt(k), beta = 0, C on a
+1x1 block-cyclic grid with 128x128 blocks (the ZGEMM-SSB configuration of the
+headline metric). One step = one contraction of the whole problem.
+
+  value : TFLOP/s (8 m n k flops per step) of the headline path with A, B
+          already resident in HBM, through the kernel-level C ABI (splab_gemm)
+          on one stream, CUDA-event timed. The headline path is the Ozaki INT8
+          path when it is built and meets <= 1e-14, else FP64 DMMA.
+  e2e   : the same metric through the public C ABI (spla_pzgemm_ssb) with A, B,
+          C in pinned HOST memory: every step streams A and B to the GPU and
+          reads C back inside the timed region.
+  paths : TFLOP/s and relative Frobenius error (vs the double-double oracle on
+          sampled columns) of each contraction path.
+
+Multi-GPU (torchrun, one rank per GPU): every rank runs its own replica of the
+single-rank problem (the single-rank path has no exchange step); value is the
+sum of all ranks' flops over the max-over-ranks time.
+
+--impl reference times the reference's own CPU path (oracle/_ref, the
+reference library compiled from its sources, else the oracle's C
+restatement) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+M = N = 1024
+K = 250000
+SEED = 20250002  # seed = 20250000 + configuration index
+FLOPS = 8.0 * M * N * K
+
+
+def cpu_env():
+    """Thread count and an explicit OpenBLAS core type (must precede loading BLAS)."""
+    n = os.cpu_count() or 1
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(n))
+    os.environ.setdefault("OMP_NUM_THREADS", str(n))
+    try:
+        flags = Path("/proc/cpuinfo").read_text()
+        if "avx512f" in flags and "GenuineIntel" in flags:
+            os.environ.setdefault("OPENBLAS_CORETYPE", "SkylakeX")
+        elif "AuthenticAMD" in flags:
+            os.environ.setdefault("OPENBLAS_CORETYPE", "Zen")
+        elif "avx2" in flags:
+            os.environ.setdefault("OPENBLAS_CORETYPE", "Haswell")
+    except OSError:
+        pass
+    return n
+
+
+def cpu_model():
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(f"/tmp/spla_b200_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for ln in self.path.read_text().splitlines():
+                p = [x.strip() for x in ln.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        except OSError:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        loaded = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# helpers
+
+
+def make_inputs(torch, device):
+    g = torch.Generator(device=device)
+    g.manual_seed(SEED)
+    s = (1.0 / (2.0 * K)) ** 0.5
+    # column-major k x m (k contiguous) == row-major (m, k)
+    A = torch.randn((M, K), dtype=torch.complex128, device=device, generator=g) * s
+    B = torch.randn((N, K), dtype=torch.complex128, device=device, generator=g) * s
+    return A, B
+
+
+def measured_peaks(torch, device):
+    """FP64 and INT8 tensor roofs measured here with library GEMMs (cuBLAS via
+    torch): the denominators for the DMMA and Ozaki kernels."""
+    out = {}
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, a)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e9
+    for _ in range(5):
+        e0.record()
+        torch.matmul(a, a)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    out["fp64_tflops"] = 2 * 8192 ** 3 / best / 1e12
+    del a
+    try:
+        x = torch.randint(-127, 127, (8192, 8192), dtype=torch.int8, device=device)
+        y = torch.randint(-127, 127, (8192, 8192), dtype=torch.int8, device=device).t()
+        for _ in range(3):
+            torch._int_mm(x, y)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(10):
+            e0.record()
+            torch._int_mm(x, y)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        out["int8_tops"] = 2 * 8192 ** 3 / best / 1e12
+    except Exception as ex:  # pragma: no cover - depends on the torch build
+        out["int8_tops"] = None
+        out["int8_error"] = str(ex)[:100]
+    return out
+
+
+def rel_err_sampled(dC, A, B, cols=(0, 511, 1023)):
+    """Relative Frobenius error of columns `cols` of C against the Dot2 oracle."""
+    import numpy as np
+    import oracle
+    An = A.cpu().numpy().ravel()
+    Bs = B[list(cols)].cpu().numpy().ravel()
+    ref = np.zeros(M * len(cols), np.complex128)
+    assert oracle.gemm(2, 0, M, len(cols), K, 1.0, An, K, Bs, K, 0.0, ref, M) == 0
+    got = dC.view(N, M)[list(cols)].cpu().numpy().ravel()
+    return oracle.rel_fro(got, ref)
+
+
+def time_device_path(torch, spla, path, A, B, steps, warmup, rank):
+    """Kernel-level timing of one path, device-resident operands, one stream."""
+    import ctypes as ct
+    L = spla.lib()
+    dC = torch.zeros(M * N, dtype=torch.complex128, device=A.device)
+    ws_bytes = spla.splab_gemm_workspace_size("complex128", path, 2, 0, M, N, K)
+    ws = torch.empty(max(1, ws_bytes), dtype=torch.uint8, device=A.device)
+    stream = torch.cuda.Stream(device=A.device)
+    nphase = 3
+    pev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nphase)]
+    handles = (ct.c_void_p * (2 * nphase))(*[e.cuda_event for e in pev])
+
+    def step():
+        rc = spla.splab_gemm("complex128", path, 2, 0, M, N, K, 1.0, A, K, B, K, 0.0, dC, M,
+                             workspace=ws, workspace_bytes=ws_bytes, stream=stream.cuda_stream)
+        if rc != 0:
+            raise RuntimeError(f"splab_gemm path {path}: {L.splab_status_string(rc).decode()}")
+
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            step()
+        stream.synchronize()
+        phase_ms = [0.0] * nphase
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if torch.distributed.is_initialized():
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for _ in range(steps):
+            L.splab_set_phase_events(handles, nphase)
+            step()
+            L.splab_set_phase_events(None, 0)
+            stream.synchronize()
+            for p in range(nphase):
+                try:
+                    phase_ms[p] += pev[2 * p].elapsed_time(pev[2 * p + 1])
+                except RuntimeError:
+                    pass
+        t1.record(stream)
+        torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / steps
+    return dC, ms, [x / steps for x in phase_ms]
+
+
+def e2e_public_api(torch, spla, path, A, B, steps, warmup):
+    """Public C ABI with pinned host operands: H2D of A, B and D2H of C per step."""
+    hA = torch.empty(A.shape, dtype=A.dtype, pin_memory=True)
+    hB = torch.empty(B.shape, dtype=B.dtype, pin_memory=True)
+    hA.copy_(A)
+    hB.copy_(B)
+    hC = torch.zeros(M * N, dtype=torch.complex128).pin_memory()
+    ctx = spla.Context(spla.PU_GPU)
+    ctx.set_fp64_path(path)
+    dist = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128,
+                                                             128)
+
+    def step():
+        spla.pgemm_ssb(M, N, K, spla.OP_CONJ_TRANSPOSE, 1.0, hA, K, hB, K, 0.0, hC, M, 0, 0, dist,
+                       ctx)
+
+    for _ in range(warmup):
+        step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if torch.distributed.is_initialized():
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return ms, hC
+
+
+def cpu_reference_run(steps, warmup, budget_s=12.0):
+    """The reference's CPU path on a bounded sample of the workload (same m, n;
+    k reduced), all host threads. Returns (TFLOP/s, info)."""
+    import numpy as np
+    cores = cpu_env()
+    from inputs import buffer
+    import oracle
+    ksamp = 16384
+    A = buffer(np.complex128, ksamp, M, SEED, "gauss_k", K)
+    B = buffer(np.complex128, ksamp, N, SEED + 1, "gauss_k", K)
+    C = np.zeros(M * N, np.complex128)
+    if oracle.REF_LIB.exists():
+        from capi import SplaCAPI
+        ref = SplaCAPI(oracle.REF_LIB)
+        ctx = ref.ctx(0)
+        _, dist = ref.block_cyclic(1, 1, 128, 128)
+
+        def call():
+            assert ref.pgemm_ssb(np.complex128, M, N, ksamp, 2, 1.0, A, ksamp, B, ksamp, 0.0, C,
+                                 M, 0, 0, dist, ctx) == 0
+        kind = "reference"
+    else:
+        def call():
+            assert oracle.pgemm_ssb(M, N, ksamp, 2, 1.0, A, ksamp, B, ksamp, 0.0, C, M, 0, 0) == 0
+        kind = "port"
+    for _ in range(max(1, warmup)):
+        call()
+    times = []
+    t_end = time.perf_counter() + budget_s
+    for i in range(max(1, steps)):
+        t0 = time.perf_counter()
+        call()
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() > t_end and i >= 0:
+            break
+    t = statistics.median(times)
+    flops = 8.0 * M * N * ksamp
+    return flops / t / 1e12, dict(kind=kind, cores=cores, sample=(
+        f"pzgemm_ssb m=n={M} k={ksamp} (k sampled from {K}), op=C, {len(times)} timed calls, "
+        f"median {t * 1e3:.1f} ms, OPENBLAS_CORETYPE={os.environ.get('OPENBLAS_CORETYPE')}, "
+        f"cpu={cpu_model()}"))
+
+
+# ---------------------------------------------------------------------------
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--paths", default="dmma,ozaki")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        value, info = cpu_reference_run(args.steps, 1)
+        line = {"metric": "ZGEMM-SSB TFLOP/s (reference CPU path)", "value": value,
+                "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": 1,
+                "higher_is_better": True, "impl": "reference", "dtype": "complex128",
+                "data": "synthetic", "config": {"workload": "pzgemm_ssb m=n=1024 k=250000 op=C",
+                                                "sample": info["sample"]},
+                "cpu_baseline": {"value": value, "unit": "TFLOP/s", **info},
+                "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}, "vs_baseline": None}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    import spla_b200 as spla
+    if not spla.LIB_PATH.exists():
+        from spla_b200.build import build
+        build()
+
+    A, B = make_inputs(torch, device)
+    peaks = measured_peaks(torch, device)
+    names = {"dmma": spla.PATH_DMMA, "ozaki": spla.PATH_OZAKI}
+    results = {}
+    with ClockSampler(local) as clk:
+        for pname in [p for p in args.paths.split(",") if p]:
+            try:
+                dC, ms, phases = time_device_path(torch, spla, names[pname], A, B, args.steps,
+                                                  warmup, rank)
+            except RuntimeError as ex:
+                results[pname] = {"error": str(ex)}
+                continue
+            t = torch.tensor([ms], device=device)
+            if world > 1:
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+            results[pname] = {"ms_per_step": ms, "tflops": FLOPS * world / (ms / 1e3) / 1e12,
+                              "phase_ms": phases, "dC": dC}
+    clocks = clk.summary()
+    for pname, r in results.items():
+        if "dC" in r:
+            r["rel_err_vs_oracle"] = rel_err_sampled(r.pop("dC"), A, B) if rank == 0 else None
+
+    # headline: Ozaki if it ran and met the accuracy bar, else DMMA
+    head = "dmma"
+    oz = results.get("ozaki", {})
+    if "tflops" in oz and oz.get("rel_err_vs_oracle") is not None and oz["rel_err_vs_oracle"] <= 1e-14:
+        head = "ozaki"
+    hr = results[head]
+    head_path = names[head]
+
+    e2e = None
+    if not args.no_e2e:
+        ms_e2e, _ = e2e_public_api(torch, spla, head_path, A, B, max(1, min(args.steps, 3)), 1)
+        t = torch.tensor([ms_e2e], device=device)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+        e2e = {"value": FLOPS * world / (ms_e2e / 1e3) / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": int(16 * K * (M + N)), "d2h_bytes_per_step": int(16 * M * N),
+               "ms_per_step": ms_e2e, "operands": "pinned host memory, streamed in k-chunks"}
+
+    if rank != 0:
+        torch.distributed.destroy_process_group() if world > 1 else None
+        return
+
+    # roofline of the dominant kernel
+    if head == "dmma":
+        k_ms = hr["phase_ms"][0] or hr["ms_per_step"]
+        achieved = FLOPS / (k_ms / 1e3) / 1e12
+        peak = peaks["fp64_tflops"]
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None,
+                "kernel": "dmma_gemm_kernel (mma.sync f64)",
+                "peak_source": "measured here: cuBLAS DGEMM 8192^3 via torch.matmul float64"}
+        launches = 2 * args.steps
+    else:
+        k_ms = hr["phase_ms"][1] or hr["ms_per_step"]
+        achieved = None
+        roof = {"bound": "tensor", "achieved": None, "peak": peaks.get("int8_tops"),
+                "unit": "TOP/s", "frac": None, "traffic": None, "kernel": "ozaki int8 residue GEMM"}
+        launches = 3 * args.steps
+
+    cpu = None
+    if not args.no_cpu and world >= 1:
+        v, info = cpu_reference_run(3, 1)
+        cpu = {"value": v, "unit": "TFLOP/s", **info}
+
+    line = {
+        "metric": "ZGEMM-SSB TFLOP/s: Ozaki-INT8 vs FP64-DMMA at <=1e-14 rel err, 1 B200",
+        "value": hr["tflops"], "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": warmup, "ms_per_step": hr["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)",
+        "data": "synthetic: complex Gaussian / sqrt(k), seeded",
+        "config": {"workload": "pzgemm_ssb C=A^H B complex double m=n=1024 k=250000, 1x1 grid "
+                               "128x128 blocks, beta=0", "path": head,
+                   "l2": "inputs (8.2 GB) larger than L2, no flush",
+                   "parallelism": f"replicas x{world}"},
+        "paths": {k: {kk: vv for kk, vv in v.items()} for k, v in results.items()},
+        "roofline": roof, "peaks_measured": peaks, "e2e": e2e, "cpu_baseline": cpu,
+        "clocks": clocks, "gpu_launches": launches,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

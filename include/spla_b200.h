@@ -1,0 +1,24 @@
+/* Extensions of this library beyond the SPLA interface (no reference
+ * counterpart). Declared separately so that include/spla/ stays identical in
+ * content to the interface it replaces. */
+#ifndef SPLA_B200_H
+#define SPLA_B200_H
+#include "spla/context.h"
+#include "spla/errors.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Select the contraction path a context uses for double and complex double:
+ * path 0 = automatic, 1 = FP64 tensor cores (DMMA), 2 = Ozaki scheme II on
+ * INT8 tensor cores. moduli = number of CRT moduli for path 2 (0 = default,
+ * sized for <= 1e-14 relative error); valid range 0..20. The environment
+ * variables SPLA_B200_PATH (auto|dmma|ozaki) and SPLA_B200_OZAKI_MODULI set the
+ * defaults of new contexts. */
+SPLA_EXPORT SplaError spla_b200_ctx_set_fp64_path(SplaContext ctx, int path, int moduli);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,98 @@
+/*
+ * splab: the kernel-level C ABI of the B200 implementation of SPLA's local
+ * contraction. Plain pointers, 64-bit sizes and a CUDA stream (passed as
+ * void*); no allocation inside except where stated; never throws. The SPLA
+ * host layer (spla_* in include/spla/) validates arguments, manages memory
+ * and calls these. Each entry point names the reference interface whose
+ * work it performs.
+ *
+ * Conventions
+ *   dtype : SPLAB_R32, SPLAB_R64, SPLAB_C32, SPLAB_C64 (complex interleaved re,im)
+ *   op    : 0 = none, 1 = transpose, 2 = conjugate transpose (SplaOperation)
+ *   alpha, beta : HOST pointers to one scalar of the dtype (complex: 2 values)
+ *   A, B, C     : DEVICE pointers, column-major with leading dimensions lda/ldb/ldc
+ *   fill        : 0 full, 1 upper, 2 lower; tiles of C that do not intersect
+ *                 the triangle (with C's offsets ro/co in the distributed
+ *                 matrix) are skipped and left unchanged
+ *   workspace   : DEVICE scratch of at least splab_gemm_workspace_size() bytes
+ *   Return value: SPLAB_OK or an SPLAB_ERR_* code (splab_status_string()).
+ */
+#ifndef SPLAB_H
+#define SPLAB_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifndef SPLAB_API
+#define SPLAB_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPLAB_R32 0
+#define SPLAB_R64 1
+#define SPLAB_C32 2
+#define SPLAB_C64 3
+
+/* Compute paths for the contraction. */
+#define SPLAB_PATH_AUTO 0  /* DMMA for float/double unless the Ozaki path is selected */
+#define SPLAB_PATH_DMMA 1  /* FP64 tensor cores (mma.sync f64); float inputs accumulate in FP64 */
+#define SPLAB_PATH_OZAKI 2 /* double / complex double only: Ozaki scheme II on INT8 tcgen05 */
+
+#define SPLAB_OK 0
+#define SPLAB_ERR_INVALID 1     /* bad argument (sizes, leading dimensions, dtype, path) */
+#define SPLAB_ERR_WORKSPACE 2   /* workspace missing or too small */
+#define SPLAB_ERR_LAUNCH 3      /* a CUDA launch or runtime call failed */
+#define SPLAB_ERR_UNSUPPORTED 4 /* path not available for this dtype / device */
+#define SPLAB_ERR_TIMEOUT 5     /* a bounded device-side wait gave up */
+
+SPLAB_API const char *splab_status_string(int status);
+
+/* Bytes of device scratch splab_gemm needs for this problem (0 if none). */
+SPLAB_API size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t m, int64_t n,
+                                 int64_t k);
+
+/*
+ * C <- alpha * op(A) * op(B) + beta * C on the device, asynchronous on `stream`.
+ * Performs the local work of spla_?gemm (reference src/gemm/gemm_gpu.cpp:59-174
+ * and src/gpu_util/multiply_gpu.cpp:78-143), which the single-rank pgemm_ssb
+ * (src/pgemm_ssb/pgemm_ssb_gpu.cpp:259-262, opA in {T,C}, opB = N) and
+ * pgemm_sbs (src/pgemm_sbs/pgemm_sbs_gpu.cpp:246-249, N,N) reduce to, plus the
+ * fill-mode tile skipping of pgemm_ssbtr (src/block_generation/block.hpp:58-66).
+ * ozakiModuli: number of CRT moduli for SPLAB_PATH_OZAKI (0 = default for
+ * <= 1e-14 relative error); ignored otherwise.
+ */
+SPLAB_API int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int64_t k,
+               const void *alpha, const void *A, int64_t lda, const void *B, int64_t ldb,
+               const void *beta, void *C, int64_t ldc, int fill, int64_t ro, int64_t co,
+               int ozakiModuli, void *workspace, size_t workspaceBytes, void *stream);
+
+/*
+ * Block-cyclic index map on the device: for each of `count` block indices in
+ * blockIdx (device, column-major block order) write 9 int64 values to out
+ * (device): global row, global col, global sub-row, global sub-col, local row,
+ * local col, rows, cols, owning rank. Same mapping as the reference's
+ * BlockCyclicGenerator::get_block_info
+ * (src/block_generation/block_cyclic_generator.cpp:59-100).
+ */
+SPLAB_API int splab_block_cyclic_info(int64_t rowsInBlock, int64_t colsInBlock, int64_t gridRows,
+                            int64_t gridCols, int64_t globalRows, int64_t globalCols,
+                            int64_t rowOffset, int64_t colOffset, const int64_t *blockIdx,
+                            int64_t count, int64_t *out, void *stream);
+
+/*
+ * Phase timing for measurement harnesses (no reference counterpart). When
+ * `events` is non-null, every following splab_gemm on the calling host thread
+ * records events[2p] / events[2p+1] (cudaEvent_t handles created by the
+ * caller) on its stream around phase p, for p < count:
+ *   DMMA path : 0 = contraction kernel, 1 = split-K reduction
+ *   Ozaki path: 0 = slicing, 1 = INT8 residue GEMMs, 2 = reconstruction
+ * Pass events = NULL to stop. Returns SPLAB_OK.
+ */
+SPLAB_API int splab_set_phase_events(void **events, int count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,507 @@
+// FP64 tensor-core contraction for the SPLA local path (sm_100a).
+//
+// C(m x n) <- alpha * op(A) * op(B) + beta * C for real/complex, float/double,
+// with op in {N, T, C} on both operands: the single-rank work of pgemm_ssb
+// (opA in {T, C}, opB = N: src/pgemm_ssb/pgemm_ssb_host.cpp:168-171),
+// pgemm_sbs (N, N: src/pgemm_sbs/pgemm_sbs_host.cpp:179-183) and gemm()
+// (src/gemm/gemm_gpu.cpp:59-174).
+//
+// tcgen05 has no f64 kind, so the FP64 tensor path is warp-level
+// mma.sync.m8n8k4.f64 fed from a cp.async multi-stage shared-memory pipeline.
+// Float inputs go through the same kernel: products of two floats are exact
+// in double and the sums run in FP64, so the float result is the double-
+// precision result rounded once.
+//
+// Split-K: the long dimension k is cut into `splits` ranges (grid.y). With one
+// split the epilogue applies alpha/beta and writes C directly; otherwise each
+// CTA writes its FP64 partial tile and splab_reduce_partials() sums the splits
+// in a fixed order (deterministic) and applies alpha/beta. Every per-element
+// FP64 chain is at most k/splits long and the splits are summed pairwise-free
+// in order, which keeps the complex k=250000 case near 2e-15 relative error.
+//
+// Fill mode: tiles of C that do not intersect the requested triangle are
+// skipped (C left unchanged), with the reference's block predicate
+// (src/block_generation/block.hpp:58-66) applied per tile.
+#include <algorithm>
+
+#include "common.cuh"
+#include "gemm_dmma.cuh"
+
+namespace splab {
+
+template <int DT>
+struct Elem;
+template <>
+struct Elem<kR64> {
+  using S = double;
+  static constexpr bool cplx = false;
+};
+template <>
+struct Elem<kR32> {
+  using S = float;
+  static constexpr bool cplx = false;
+};
+template <>
+struct Elem<kC64> {
+  using S = double2;
+  static constexpr bool cplx = true;
+};
+template <>
+struct Elem<kC32> {
+  using S = float2;
+  static constexpr bool cplx = true;
+};
+
+__device__ __forceinline__ void to_re_im(double v, double& re, double& im) { re = v; im = 0.0; }
+__device__ __forceinline__ void to_re_im(float v, double& re, double& im) {
+  re = static_cast<double>(v);
+  im = 0.0;
+}
+__device__ __forceinline__ void to_re_im(double2 v, double& re, double& im) { re = v.x; im = v.y; }
+__device__ __forceinline__ void to_re_im(float2 v, double& re, double& im) {
+  re = static_cast<double>(v.x);
+  im = static_cast<double>(v.y);
+}
+
+// Copy one element (global -> shared) asynchronously, zero-filled when invalid.
+template <typename S>
+__device__ __forceinline__ void cp_elem(S* dst, const S* src, bool valid) {
+  if constexpr (sizeof(S) == 4) {
+    cp_async_4(dst, src, valid);
+  } else if constexpr (sizeof(S) == 8) {
+    cp_async_8(dst, src, valid);
+  } else {
+    cp_async_8(dst, src, valid);
+    cp_async_8(reinterpret_cast<char*>(dst) + 8, reinterpret_cast<const char*>(src) + 8, valid);
+  }
+}
+
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// Row stride (in elements) of a staged operand tile, chosen so that the
+// fragment reads of one mma.m8n8k4 are free of shared-memory bank conflicts.
+template <int BYTES, bool KMAJ, int T, int BK>
+struct SmemStride {
+  static constexpr int value =
+      KMAJ ? (BK + 4) : (BYTES == 4 ? T + 8 : (BYTES == 8 ? T + 4 : T + 2));
+};
+
+template <int DT_, bool AK_, bool BK_MAJ_, int BM_, int BN_, int BK_, int WM_, int WN_, int ST_>
+struct DmmaCfg {
+  static constexpr int DT = DT_;
+  using S = typename Elem<DT>::S;
+  static constexpr bool CPLX = Elem<DT>::cplx;
+  static constexpr bool A_KMAJ = AK_;
+  static constexpr bool B_KMAJ = BK_MAJ_;
+  static constexpr int BM = BM_, BN = BN_, BK = BK_, WM = WM_, WN = WN_, STAGES = ST_;
+  static constexpr int WARPS_M = BM / WM, WARPS_N = BN / WN;
+  static constexpr int THREADS = 32 * WARPS_M * WARPS_N;
+  static constexpr int SA = SmemStride<sizeof(S), A_KMAJ, BM, BK>::value;
+  static constexpr int SB = SmemStride<sizeof(S), B_KMAJ, BN, BK>::value;
+  static constexpr int A_ELEMS = A_KMAJ ? BM * SA : BK * SA;
+  static constexpr int B_ELEMS = B_KMAJ ? BN * SB : BK * SB;
+  static constexpr int STAGE_BYTES = (A_ELEMS + B_ELEMS) * int(sizeof(S));
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES;
+  static_assert((BM * BK) % THREADS == 0 && (BN * BK) % THREADS == 0, "tile/threads");
+  static_assert(BK % 4 == 0 && WM % 8 == 0 && WN % 8 == 0, "mma shape");
+};
+
+// Stage one T x BK operand tile. KMAJ: element (r, c) at X[(r0+r)*ld + k0+c];
+// otherwise at X[(k0+c)*ld + r0+r]. Rows >= rows_total or k >= kend read zero.
+template <typename S, bool KMAJ, int T, int BK, int STRIDE, int THREADS>
+__device__ __forceinline__ void stage_tile(S* smem, const S* X, int64_t ld, int64_t r0,
+                                           int64_t rows_total, int64_t k0, int64_t kend) {
+  constexpr int ELEMS = T * BK;
+#pragma unroll
+  for (int i = 0; i < ELEMS / THREADS; ++i) {
+    const int e = threadIdx.x + i * THREADS;
+    int r, c;
+    if constexpr (KMAJ) {
+      c = e % BK;
+      r = e / BK;
+    } else {
+      r = e % T;
+      c = e / T;
+    }
+    const int64_t gr = r0 + r, gk = k0 + c;
+    const bool valid = (gr < rows_total) && (gk < kend);
+    const S* src = valid ? (KMAJ ? X + gr * ld + gk : X + gk * ld + gr) : X;
+    S* dst = KMAJ ? smem + r * STRIDE + c : smem + c * STRIDE + r;
+    cp_elem(dst, src, valid);
+  }
+}
+
+template <typename S, bool KMAJ, int STRIDE>
+__device__ __forceinline__ S frag_load(const S* smem, int row, int kidx) {
+  return KMAJ ? smem[row * STRIDE + kidx] : smem[kidx * STRIDE + row];
+}
+
+// C[idx] <- alpha * x + beta * C[idx] over the dtype of C, reading C only if
+// beta != 0 (BLAS semantics).
+template <int DT>
+__device__ __forceinline__ void store_alpha_beta_impl(void* C, int64_t idx, double xr, double xi,
+                                                      double alr, double ali, double ber,
+                                                      double bei) {
+  double outr = alr * xr - ali * xi;
+  double outi = alr * xi + ali * xr;
+  const bool read_c = (ber != 0.0 || bei != 0.0);
+  if constexpr (DT == kR64) {
+    double* c = static_cast<double*>(C) + idx;
+    *c = read_c ? fma(ber, *c, outr) : outr;
+  } else if constexpr (DT == kR32) {
+    float* c = static_cast<float*>(C) + idx;
+    *c = static_cast<float>(read_c ? fma(ber, static_cast<double>(*c), outr) : outr);
+  } else if constexpr (DT == kC64) {
+    double2* c = static_cast<double2*>(C) + idx;
+    if (read_c) {
+      const double2 v = *c;
+      outr += ber * v.x - bei * v.y;
+      outi += ber * v.y + bei * v.x;
+    }
+    *c = make_double2(outr, outi);
+  } else {
+    float2* c = static_cast<float2*>(C) + idx;
+    if (read_c) {
+      const float2 v = *c;
+      outr += ber * double(v.x) - bei * double(v.y);
+      outi += ber * double(v.y) + bei * double(v.x);
+    }
+    *c = make_float2(static_cast<float>(outr), static_cast<float>(outi));
+  }
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS) dmma_gemm_kernel(DmmaParams p) {
+  using S = typename Cfg::S;
+  constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, WM = Cfg::WM, WN = Cfg::WN;
+  constexpr int FM = WM / 8, FN = WN / 8, STAGES = Cfg::STAGES;
+  constexpr bool CPLX = Cfg::CPLX;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* smem = reinterpret_cast<S*>(smem_raw);
+
+  const int64_t tiles_m = (p.m + BM - 1) / BM;
+  const int64_t tm = blockIdx.x % tiles_m, tn = blockIdx.x / tiles_m;
+  const int64_t m0 = tm * BM, n0 = tn * BN;
+  if (!tile_is_active(p.fill_mode, m0, n0, ::min((int64_t)BM, p.m - m0),
+                      ::min((int64_t)BN, p.n - n0), p.fill_ro, p.fill_co))
+    return;
+
+  const int64_t kbeg = static_cast<int64_t>(blockIdx.y) * p.k_per_split;
+  const int64_t kend = min(p.k, kbeg + p.k_per_split);
+  const int nkt = kend > kbeg ? static_cast<int>((kend - kbeg + BK - 1) / BK) : 0;
+
+  const S* A = static_cast<const S*>(p.A);
+  const S* B = static_cast<const S*>(p.B);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp % Cfg::WARPS_M, wn = warp / Cfg::WARPS_M;
+  const int g = lane >> 2, t = lane & 3;
+  const unsigned long long maskA = p.conj_a ? 0x8000000000000000ull : 0ull;
+  const unsigned long long maskB = p.conj_b ? 0x8000000000000000ull : 0ull;
+  constexpr unsigned long long kNeg = 0x8000000000000000ull;
+
+  double accr[FM][FN][2];
+  double acci[CPLX ? FM : 1][CPLX ? FN : 1][2];
+#pragma unroll
+  for (int i = 0; i < FM; ++i)
+#pragma unroll
+    for (int j = 0; j < FN; ++j) {
+      accr[i][j][0] = accr[i][j][1] = 0.0;
+      if constexpr (CPLX) acci[i][j][0] = acci[i][j][1] = 0.0;
+    }
+
+  auto stage_ptr_a = [&](int s) { return smem + s * (Cfg::A_ELEMS + Cfg::B_ELEMS); };
+  auto stage_ptr_b = [&](int s) { return smem + s * (Cfg::A_ELEMS + Cfg::B_ELEMS) + Cfg::A_ELEMS; };
+  auto load_stage = [&](int s, int64_t k0) {
+    stage_tile<S, Cfg::A_KMAJ, BM, BK, Cfg::SA, Cfg::THREADS>(stage_ptr_a(s), A, p.lda, m0, p.m,
+                                                             k0, kend);
+    stage_tile<S, Cfg::B_KMAJ, BN, BK, Cfg::SB, Cfg::THREADS>(stage_ptr_b(s), B, p.ldb, n0, p.n,
+                                                             k0, kend);
+  };
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nkt) load_stage(s, kbeg + static_cast<int64_t>(s) * BK);
+    cp_async_commit();
+  }
+
+  for (int kt = 0; kt < nkt; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const int pf = kt + STAGES - 1;
+    if (pf < nkt) load_stage(pf % STAGES, kbeg + static_cast<int64_t>(pf) * BK);
+    cp_async_commit();
+
+    const S* As = stage_ptr_a(kt % STAGES);
+    const S* Bs = stage_ptr_b(kt % STAGES);
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double ar[FM], ai[FM], ain[FM], br[FN], bi[FN];
+#pragma unroll
+      for (int i = 0; i < FM; ++i) {
+        double re, im;
+        to_re_im(frag_load<S, Cfg::A_KMAJ, Cfg::SA>(As, wm * WM + i * 8 + g, kk + t), re, im);
+        ar[i] = re;
+        ai[i] = xor_sign(im, maskA);
+        ain[i] = xor_sign(ai[i], kNeg);
+      }
+#pragma unroll
+      for (int j = 0; j < FN; ++j) {
+        double re, im;
+        to_re_im(frag_load<S, Cfg::B_KMAJ, Cfg::SB>(Bs, wn * WN + j * 8 + g, kk + t), re, im);
+        br[j] = re;
+        bi[j] = xor_sign(im, maskB);
+      }
+#pragma unroll
+      for (int i = 0; i < FM; ++i)
+#pragma unroll
+        for (int j = 0; j < FN; ++j) {
+          dmma_8x8x4(accr[i][j][0], accr[i][j][1], ar[i], br[j]);
+          if constexpr (CPLX) {
+            dmma_8x8x4(accr[i][j][0], accr[i][j][1], ain[i], bi[j]);
+            dmma_8x8x4(acci[i][j][0], acci[i][j][1], ar[i], bi[j]);
+            dmma_8x8x4(acci[i][j][0], acci[i][j][1], ai[i], br[j]);
+          }
+        }
+    }
+  }
+  cp_async_wait<0>();
+
+  // Epilogue: element (i, j) of the warp's sub-tile (fi, fj, e).
+#pragma unroll
+  for (int fi = 0; fi < FM; ++fi) {
+    const int64_t i = m0 + wm * WM + fi * 8 + g;
+    if (i >= p.m) continue;
+#pragma unroll
+    for (int fj = 0; fj < FN; ++fj) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int64_t j = n0 + wn * WN + fj * 8 + 2 * t + e;
+        if (j >= p.n) continue;
+        const double xr = accr[fi][fj][e];
+        const double xi = CPLX ? acci[CPLX ? fi : 0][CPLX ? fj : 0][e] : 0.0;
+        if (p.partial) {
+          const int64_t idx = static_cast<int64_t>(blockIdx.y) * p.m * p.n + j * p.m + i;
+          if constexpr (CPLX) {
+            reinterpret_cast<double2*>(p.P)[idx] = make_double2(xr, xi);
+          } else {
+            reinterpret_cast<double*>(p.P)[idx] = xr;
+          }
+        } else {
+          store_alpha_beta_impl<Cfg::DT>(p.C, i + j * p.ldc, xr, xi, p.alpha_r, p.alpha_i,
+                                            p.beta_r, p.beta_i);
+        }
+      }
+    }
+  }
+}
+
+// Sum the FP64 split-K partials of each element in split order, then
+// C <- alpha * sum + beta * C. Elements of tiles outside the fill triangle are
+// left untouched (the same tile predicate as the GEMM kernel).
+template <int DT>
+__global__ void reduce_partials_kernel(const void* __restrict__ P, int splits, int64_t m,
+                                       int64_t n, void* C, int64_t ldc, double alr, double ali,
+                                       double ber, double bei, int fill_mode, int64_t ro,
+                                       int64_t co, int tile_m, int tile_n) {
+  constexpr bool CPLX = dtype_is_complex(DT);
+  const int64_t total = m * n;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = idx % m, j = idx / m;
+    if (fill_mode != 0) {
+      const int64_t ti = (i / tile_m) * tile_m, tj = (j / tile_n) * tile_n;
+      if (!tile_is_active(fill_mode, ti, tj, ::min((int64_t)tile_m, m - ti),
+                          ::min((int64_t)tile_n, n - tj), ro, co))
+        continue;
+    }
+    double sr = 0.0, si = 0.0;
+    if constexpr (CPLX) {
+      const double2* q = static_cast<const double2*>(P) + idx;
+      for (int s = 0; s < splits; ++s) {
+        const double2 v = q[s * total];
+        sr += v.x;
+        si += v.y;
+      }
+    } else {
+      const double* q = static_cast<const double*>(P) + idx;
+      for (int s = 0; s < splits; ++s) sr += q[s * total];
+    }
+    store_alpha_beta_impl<DT>(C, i + j * ldc, sr, si, alr, ali, ber, bei);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side: configuration per (dtype, operand layouts), split selection.
+
+namespace {
+
+template <int DT, bool AK, bool BKM>
+struct CfgFor;
+// complex: 64x64 CTA tile, 2x2 warps of 32x32, BK = 8 complex
+template <bool AK, bool BKM>
+struct CfgFor<kC64, AK, BKM> {
+  using type = DmmaCfg<kC64, AK, BKM, 64, 64, 8, 32, 32, 3>;
+};
+template <bool AK, bool BKM>
+struct CfgFor<kC32, AK, BKM> {
+  using type = DmmaCfg<kC32, AK, BKM, 64, 64, 8, 32, 32, 3>;
+};
+// real: 128x64 CTA tile, 4x2 warps of 32x32, BK = 16
+template <bool AK, bool BKM>
+struct CfgFor<kR64, AK, BKM> {
+  using type = DmmaCfg<kR64, AK, BKM, 128, 64, 16, 32, 32, 3>;
+};
+template <bool AK, bool BKM>
+struct CfgFor<kR32, AK, BKM> {
+  using type = DmmaCfg<kR32, AK, BKM, 128, 64, 16, 32, 32, 3>;
+};
+
+template <class Cfg>
+int occupancy() {
+  static int occ = -1;
+  if (occ < 0) {
+    cudaFuncSetAttribute(dmma_gemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         Cfg::SMEM_BYTES);
+    int o = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, dmma_gemm_kernel<Cfg>, Cfg::THREADS,
+                                                      Cfg::SMEM_BYTES) != cudaSuccess ||
+        o < 1)
+      o = 1;
+    occ = o;
+  }
+  return occ;
+}
+
+template <class Cfg>
+DmmaPlan plan_for(const GemmProblem& pr, int num_sms, int force_splits) {
+  DmmaPlan plan{Cfg::BM, Cfg::BN, 1, pr.k, 0};
+  const int64_t tiles = ((pr.m + Cfg::BM - 1) / Cfg::BM) * ((pr.n + Cfg::BN - 1) / Cfg::BN);
+  const int64_t slots = int64_t(num_sms) * occupancy<Cfg>();
+  const double flop_per_k = double(Cfg::BM) * Cfg::BN * (Cfg::CPLX ? 8.0 : 2.0);
+  const double slot_rate = 37e12 / double(slots);  // FP64 tensor rate per resident CTA
+  const double esz = Cfg::CPLX ? 16.0 : 8.0;
+  int best_s = 1;
+  if (force_splits > 0) {
+    best_s = force_splits;
+  } else {
+    double best_t = 1e300;
+    const int64_t s_max = std::max<int64_t>(1, std::min<int64_t>(4096, pr.k / (8 * Cfg::BK)));
+    for (int64_t s = 1; s <= s_max; ++s) {
+      const int64_t kps = ((pr.k + s - 1) / s + Cfg::BK - 1) / Cfg::BK * Cfg::BK;
+      const int64_t s_eff = (pr.k + kps - 1) / kps;
+      if (s_eff != s) continue;
+      const double waves = double((tiles * s + slots - 1) / slots);
+      const double t = waves * double(kps) * flop_per_k / slot_rate +
+                       (s > 1 ? double(s) * pr.m * pr.n * esz * 2.0 / 6.0e12 : 0.0) +
+                       (s > 1 ? 4e-6 : 0.0);
+      if (t < best_t * 0.995) {
+        best_t = t;
+        best_s = int(s);
+      }
+    }
+  }
+  int64_t kps = ((pr.k + best_s - 1) / best_s + Cfg::BK - 1) / Cfg::BK * Cfg::BK;
+  if (kps < 1) kps = Cfg::BK;
+  plan.splits = int(std::max<int64_t>(1, (pr.k + kps - 1) / kps));
+  plan.k_per_split = kps;
+  plan.workspace_bytes = plan.splits > 1 ? size_t(plan.splits) * pr.m * pr.n * size_t(esz) : 0;
+  return plan;
+}
+
+template <class Cfg>
+cudaError_t launch_cfg(const GemmProblem& pr, const DmmaPlan& plan, void* ws, cudaStream_t st) {
+  occupancy<Cfg>();  // also sets the dynamic shared memory attribute
+  DmmaParams p{};
+  p.A = pr.A;
+  p.B = pr.B;
+  p.C = pr.C;
+  p.P = ws;
+  p.lda = pr.lda;
+  p.ldb = pr.ldb;
+  p.ldc = pr.ldc;
+  p.m = pr.m;
+  p.n = pr.n;
+  p.k = pr.k;
+  p.k_per_split = plan.k_per_split;
+  p.alpha_r = pr.alpha[0];
+  p.alpha_i = pr.alpha[1];
+  p.beta_r = pr.beta[0];
+  p.beta_i = pr.beta[1];
+  p.conj_a = pr.opA == 2;
+  p.conj_b = pr.opB == 2;
+  p.partial = plan.splits > 1;
+  p.fill_mode = pr.fill_mode;
+  p.fill_ro = pr.fill_ro;
+  p.fill_co = pr.fill_co;
+  const int64_t tiles = ((pr.m + Cfg::BM - 1) / Cfg::BM) * ((pr.n + Cfg::BN - 1) / Cfg::BN);
+  dim3 grid(unsigned(tiles), unsigned(plan.splits));
+  phase_mark(0, false, st);
+  dmma_gemm_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(p);
+  phase_mark(0, true, st);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || plan.splits == 1) return e;
+  phase_mark(1, false, st);
+  e = reduce_partials(pr, ws, plan.splits, Cfg::BM, Cfg::BN, st);
+  phase_mark(1, true, st);
+  return e;
+}
+
+template <int DT, class F>
+auto with_cfg(const GemmProblem& pr, F&& f) {
+  const bool ak = pr.opA != 0;   // op(A) = A^T / A^H: A is k x m, k contiguous
+  const bool bk = pr.opB == 0;   // op(B) = B: B is k x n, k contiguous
+  if (ak && bk) return f(typename CfgFor<DT, true, true>::type{});
+  if (ak && !bk) return f(typename CfgFor<DT, true, false>::type{});
+  if (!ak && bk) return f(typename CfgFor<DT, false, true>::type{});
+  return f(typename CfgFor<DT, false, false>::type{});
+}
+
+template <class F>
+auto dispatch(const GemmProblem& pr, F&& f) {
+  switch (pr.dtype) {
+    case kR32: return with_cfg<kR32>(pr, f);
+    case kR64: return with_cfg<kR64>(pr, f);
+    case kC32: return with_cfg<kC32>(pr, f);
+    default: return with_cfg<kC64>(pr, f);
+  }
+}
+
+}  // namespace
+
+DmmaPlan dmma_plan(const GemmProblem& pr, int num_sms, int force_splits) {
+  return dispatch(pr, [&](auto cfg) {
+    return plan_for<decltype(cfg)>(pr, num_sms, force_splits);
+  });
+}
+
+cudaError_t dmma_gemm(const GemmProblem& pr, const DmmaPlan& plan, void* ws, cudaStream_t st) {
+  if (pr.m <= 0 || pr.n <= 0) return cudaSuccess;
+  return dispatch(pr, [&](auto cfg) { return launch_cfg<decltype(cfg)>(pr, plan, ws, st); });
+}
+
+cudaError_t reduce_partials(const GemmProblem& pr, const void* P, int splits, int tile_m,
+                            int tile_n, cudaStream_t st) {
+  const int64_t total = pr.m * pr.n;
+  const int threads = 256;
+  const int64_t blocks = std::min<int64_t>((total + threads - 1) / threads, 148 * 16);
+  auto go = [&](auto kern) {
+    kern<<<unsigned(blocks), threads, 0, st>>>(P, splits, pr.m, pr.n, pr.C, pr.ldc, pr.alpha[0],
+                                               pr.alpha[1], pr.beta[0], pr.beta[1], pr.fill_mode,
+                                               pr.fill_ro, pr.fill_co, tile_m, tile_n);
+    return cudaGetLastError();
+  };
+  switch (pr.dtype) {
+    case kR32: return go(reduce_partials_kernel<kR32>);
+    case kR64: return go(reduce_partials_kernel<kR64>);
+    case kC32: return go(reduce_partials_kernel<kC32>);
+    default: return go(reduce_partials_kernel<kC64>);
+  }
+}
+
+}  // namespace splab

@@ -1,0 +1,188 @@
+// splab_* C ABI: argument checks and dispatch to the sm_100a kernels.
+#include <algorithm>
+#include <cstring>
+
+#include "../../../include/splab.h"
+#include "common.cuh"
+#include "gemm_dmma.cuh"
+#include "ozaki.cuh"
+
+namespace splab {
+
+PhaseEvents& phase_events() {
+  static thread_local PhaseEvents pe;
+  return pe;
+}
+
+namespace {
+
+int num_sms() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static int cached[64] = {0};
+  if (dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v < 1)
+      v = 148;
+    cached[dev] = v;
+  }
+  return cached[dev];
+}
+
+bool valid_problem(int dtype, int opA, int opB, int64_t m, int64_t n, int64_t k, int64_t lda,
+                   int64_t ldb, int64_t ldc) {
+  if (dtype < 0 || dtype > 3) return false;
+  if (opA < 0 || opA > 2 || opB < 0 || opB > 2) return false;
+  if (m < 0 || n < 0 || k < 0) return false;
+  if (lda < std::max<int64_t>(1, opA == 0 ? m : k)) return false;
+  if (ldb < std::max<int64_t>(1, opB == 0 ? k : n)) return false;
+  if (ldc < std::max<int64_t>(1, m)) return false;
+  return true;
+}
+
+GemmProblem make_problem(int dtype, int opA, int opB, int64_t m, int64_t n, int64_t k,
+                         const void* alpha, const void* A, int64_t lda, const void* B, int64_t ldb,
+                         const void* beta, void* C, int64_t ldc, int fill, int64_t ro,
+                         int64_t co) {
+  GemmProblem p{};
+  p.dtype = dtype;
+  p.opA = opA;
+  p.opB = opB;
+  p.m = m;
+  p.n = n;
+  p.k = k;
+  p.A = A;
+  p.lda = lda;
+  p.B = B;
+  p.ldb = ldb;
+  p.C = C;
+  p.ldc = ldc;
+  p.fill_mode = fill;
+  p.fill_ro = ro;
+  p.fill_co = co;
+  const bool dbl = dtype_is_double(dtype), cplx = dtype_is_complex(dtype);
+  for (int i = 0; i < 2; ++i) {
+    p.alpha[i] = p.beta[i] = 0.0;
+    if (i == 1 && !cplx) break;
+    p.alpha[i] = dbl ? static_cast<const double*>(alpha)[i] : static_cast<const float*>(alpha)[i];
+    p.beta[i] = dbl ? static_cast<const double*>(beta)[i] : static_cast<const float*>(beta)[i];
+  }
+  return p;
+}
+
+int use_ozaki(int dtype, int path) {
+  if (path == SPLAB_PATH_OZAKI) return 1;
+  (void)dtype;
+  return 0;
+}
+
+__global__ void block_cyclic_info_kernel(int64_t rb, int64_t cb, int64_t gr, int64_t gc,
+                                         int64_t nr, int64_t nc, int64_t ro, int64_t co,
+                                         const int64_t* __restrict__ ids, int64_t count,
+                                         int64_t* __restrict__ out) {
+  const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (t >= count) return;
+  const int64_t firstRow = (ro / rb) * rb, firstCol = (co / cb) * cb;
+  const int64_t numBlockRows = (ro - firstRow + nr + rb - 1) / rb;
+  const int64_t b = ids[t];
+  const int64_t bRow = b % numBlockRows, bCol = b / numBlockRows;
+  const int64_t gbRow = bRow + ro / rb, gbCol = bCol + co / cb;
+  const int64_t gRow = max(ro, firstRow + bRow * rb), gCol = max(co, firstCol + bCol * cb);
+  const int64_t endRow = min((gbRow + 1) * rb, ro + nr), endCol = min((gbCol + 1) * cb, co + nc);
+  int64_t* o = out + 9 * t;
+  o[0] = gRow;
+  o[1] = gCol;
+  o[2] = gRow - ro;
+  o[3] = gCol - co;
+  o[4] = (gbRow / gr) * rb + gRow % rb;
+  o[5] = (gbCol / gc) * cb + gCol % cb;
+  o[6] = endRow - gRow;
+  o[7] = endCol - gCol;
+  o[8] = (gbRow % gr) + (gbCol % gc) * gr;
+}
+
+}  // namespace
+}  // namespace splab
+
+using namespace splab;
+
+extern "C" {
+
+const char* splab_status_string(int status) {
+  switch (status) {
+    case SPLAB_OK: return "ok";
+    case SPLAB_ERR_INVALID: return "invalid argument";
+    case SPLAB_ERR_WORKSPACE: return "workspace missing or too small";
+    case SPLAB_ERR_LAUNCH: return "CUDA launch or runtime error";
+    case SPLAB_ERR_UNSUPPORTED: return "path not supported for this dtype or device";
+    case SPLAB_ERR_TIMEOUT: return "bounded device wait timed out";
+    default: return "unknown status";
+  }
+}
+
+size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t m, int64_t n,
+                                 int64_t k) {
+  if (dtype < 0 || dtype > 3 || m <= 0 || n <= 0 || k <= 0) return 0;
+  GemmProblem p{};
+  p.dtype = dtype;
+  p.opA = opA;
+  p.opB = opB;
+  p.m = m;
+  p.n = n;
+  p.k = k;
+  if (use_ozaki(dtype, path)) return ozaki_workspace_bytes(p, 0);
+  return dmma_plan(p, num_sms()).workspace_bytes;
+}
+
+int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int64_t k,
+               const void* alpha, const void* A, int64_t lda, const void* B, int64_t ldb,
+               const void* beta, void* C, int64_t ldc, int fill, int64_t ro, int64_t co,
+               int ozakiModuli, void* workspace, size_t workspaceBytes, void* stream) {
+  if (!valid_problem(dtype, opA, opB, m, n, k, lda, ldb, ldc)) return SPLAB_ERR_INVALID;
+  if (path < 0 || path > 2 || fill < 0 || fill > 2 || !alpha || !beta) return SPLAB_ERR_INVALID;
+  if (m == 0 || n == 0) return SPLAB_OK;
+  if (!C || (k > 0 && (!A || !B))) return SPLAB_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  GemmProblem p = make_problem(dtype, opA, opB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                               fill, ro, co);
+  cudaError_t err;
+  if (use_ozaki(dtype, path)) {
+    if (!dtype_is_double(dtype)) return SPLAB_ERR_UNSUPPORTED;
+    const size_t need = ozaki_workspace_bytes(p, ozakiModuli);
+    if (need > workspaceBytes || (need && !workspace)) return SPLAB_ERR_WORKSPACE;
+    err = ozaki_gemm(p, ozakiModuli, workspace, workspaceBytes, st);
+  } else {
+    const DmmaPlan plan = dmma_plan(p, num_sms());
+    if (plan.workspace_bytes > workspaceBytes || (plan.workspace_bytes && !workspace))
+      return SPLAB_ERR_WORKSPACE;
+    err = dmma_gemm(p, plan, workspace, st);
+  }
+  return err == cudaSuccess ? SPLAB_OK : SPLAB_ERR_LAUNCH;
+}
+
+int splab_set_phase_events(void** events, int count) {
+  PhaseEvents& pe = phase_events();
+  pe.ev = reinterpret_cast<cudaEvent_t*>(events);
+  pe.count = events ? count : 0;
+  return SPLAB_OK;
+}
+
+int splab_block_cyclic_info(int64_t rowsInBlock, int64_t colsInBlock, int64_t gridRows,
+                            int64_t gridCols, int64_t globalRows, int64_t globalCols,
+                            int64_t rowOffset, int64_t colOffset, const int64_t* blockIdx,
+                            int64_t count, int64_t* out, void* stream) {
+  if (rowsInBlock < 1 || colsInBlock < 1 || gridRows < 1 || gridCols < 1 || globalRows < 0 ||
+      globalCols < 0 || rowOffset < 0 || colOffset < 0 || count < 0)
+    return SPLAB_ERR_INVALID;
+  if (count == 0) return SPLAB_OK;
+  if (!blockIdx || !out) return SPLAB_ERR_INVALID;
+  const int threads = 256;
+  const int64_t blocks = (count + threads - 1) / threads;
+  block_cyclic_info_kernel<<<unsigned(blocks), threads, 0, static_cast<cudaStream_t>(stream)>>>(
+      rowsInBlock, colsInBlock, gridRows, gridCols, globalRows, globalCols, rowOffset, colOffset,
+      blockIdx, count, out);
+  return cudaGetLastError() == cudaSuccess ? SPLAB_OK : SPLAB_ERR_LAUNCH;
+}
+
+}  // extern "C"
