@@ -1,6 +1,7 @@
 // spla::Context and the spla_ctx_* C ABI (reference include/spla/context.h,
 // src/spla/context.cpp, src/spla/context_internal.hpp). Defaults and setter
 // validation equal the reference's (context_internal.hpp:58-64, :122-140).
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
@@ -12,6 +13,9 @@ namespace spla {
 
 void check_cuda(cudaError_t err) {
   if (err == cudaSuccess) return;
+  if (std::getenv("SPLA_B200_DEBUG"))
+    std::fprintf(stderr, "spla_b200: CUDA error %s (%s)\n", cudaGetErrorName(err),
+                 cudaGetErrorString(err));
   cudaGetLastError();  // clear a sticky-free error so the context stays usable
   switch (err) {
     case cudaErrorMemoryAllocation: throw GPUAllocationError();
@@ -27,6 +31,9 @@ void check_cuda(cudaError_t err) {
 }
 
 void check_splab(int status) {
+  if (status != SPLAB_OK && std::getenv("SPLA_B200_DEBUG"))
+    std::fprintf(stderr, "spla_b200: splab status %d (%s), last CUDA error %s\n", status,
+                 splab_status_string(status), cudaGetErrorName(cudaPeekAtLastError()));
   switch (status) {
     case SPLAB_OK: return;
     case SPLAB_ERR_INVALID: throw InvalidParameterError();

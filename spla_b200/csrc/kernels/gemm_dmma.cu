@@ -380,7 +380,8 @@ int occupancy() {
 
 template <class Cfg>
 DmmaPlan plan_for(const GemmProblem& pr, int num_sms, int force_splits) {
-  DmmaPlan plan{Cfg::BM, Cfg::BN, 1, pr.k, 0};
+  DmmaPlan plan{Cfg::BM, Cfg::BN, 1, Cfg::BK, 0};
+  if (pr.k <= 0) return plan;  // C <- beta C only: one pass, no partials
   const int64_t tiles = ((pr.m + Cfg::BM - 1) / Cfg::BM) * ((pr.n + Cfg::BN - 1) / Cfg::BN);
   const int64_t slots = int64_t(num_sms) * occupancy<Cfg>();
   const double flop_per_k = double(Cfg::BM) * Cfg::BN * (Cfg::CPLX ? 8.0 : 2.0);

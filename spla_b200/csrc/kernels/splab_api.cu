@@ -1,5 +1,7 @@
 // splab_* C ABI: argument checks and dispatch to the sm_100a kernels.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "../../../include/splab.h"
@@ -158,6 +160,10 @@ int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int6
       return SPLAB_ERR_WORKSPACE;
     err = dmma_gemm(p, plan, workspace, st);
   }
+  if (err != cudaSuccess && std::getenv("SPLA_B200_DEBUG"))
+    std::fprintf(stderr, "splab_gemm: %s (%s) dtype %d path %d m %lld n %lld k %lld\n",
+                 cudaGetErrorName(err), cudaGetErrorString(err), dtype, path, (long long)m,
+                 (long long)n, (long long)k);
   return err == cudaSuccess ? SPLAB_OK : SPLAB_ERR_LAUNCH;
 }
 

@@ -193,3 +193,27 @@ def test_cfg1_full(ours, ctx):
                         ctx)
     assert rc == 0
     assert oracle.rel_fro(host(dC), g["C"]) < 1e-14
+
+
+@pytest.mark.parametrize("dtn,opA", [("z", 2), ("d", 1), ("c", 2), ("s", 1)])
+def test_ssb_streamed_host_operands(dtn, opA):
+    """Host-resident A and B streamed in many k-chunks (tile_size_gpu forced
+    small): the chunked accumulation (beta on the first chunk, 1 after) equals
+    the oracle on the same inputs."""
+    import spla_b200 as spla
+    import oracle
+    from inputs import buffer
+    dt = gc.DT[dtn]
+    m, n, k = 70, 45, 5003
+    A = buffer(dt, k + 1, m, 101, "uniform11")
+    B = buffer(dt, k + 2, n, 102, "uniform11")
+    C = buffer(dt, m + 3, n, 103, "uniform11")
+    ref = C.copy()
+    alpha, beta = (0.5 + 0.25j, -1.0 + 0.5j) if dtn in "cz" else (0.5, -1.0)
+    assert oracle.pgemm_ssb(m, n, k, opA, alpha, A, k + 1, B, k + 2, beta, ref, m + 3, 0, 0) == 0
+    ctx = spla.Context(spla.PU_GPU)
+    ctx.set_tile_size_gpu(64)
+    dist = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 64, 64)
+    spla.pgemm_ssb(m, n, k, opA, alpha, A, k + 1, B, k + 2, beta, C, m + 3, 0, 0, dist, ctx)
+    tol = 1e-6 if dtn in "sc" else 1e-14
+    assert oracle.rel_fro(C, ref) <= tol
