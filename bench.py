@@ -199,6 +199,9 @@ def time_device_path(torch, spla, path, A, B, steps, warmup, rank):
     stream = torch.cuda.Stream(device=A.device)
     nphase = 3
     pev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nphase)]
+    for e in pev:  # torch creates the CUDA event on first record
+        e.record(stream)
+    stream.synchronize()
     handles = (ct.c_void_p * (2 * nphase))(*[e.cuda_event for e in pev])
 
     def step():
@@ -218,9 +221,13 @@ def time_device_path(torch, spla, path, A, B, steps, warmup, rank):
         torch.cuda.synchronize()
         t0.record(stream)
         for _ in range(steps):
+            for e in pev:
+                e.record(stream)  # phases a path does not have read as zero
             L.splab_set_phase_events(handles, nphase)
-            step()
-            L.splab_set_phase_events(None, 0)
+            try:
+                step()
+            finally:
+                L.splab_set_phase_events(None, 0)
             stream.synchronize()
             for p in range(nphase):
                 try:

@@ -60,7 +60,9 @@ struct PhaseEvents {
 PhaseEvents& phase_events();
 inline void phase_mark(int phase, bool end, cudaStream_t st) {
   PhaseEvents& pe = phase_events();
-  if (pe.ev && phase < pe.count) cudaEventRecord(pe.ev[2 * phase + (end ? 1 : 0)], st);
+  if (pe.ev && phase < pe.count &&
+      cudaEventRecord(pe.ev[2 * phase + (end ? 1 : 0)], st) != cudaSuccess)
+    cudaGetLastError();  // a bad timing event must not fail the computation
 }
 
 }  // namespace splab
