@@ -36,9 +36,10 @@ extern "C" {
 #define SPLAB_C64 3
 
 /* Compute paths for the contraction. */
-#define SPLAB_PATH_AUTO 0  /* DMMA for float/double unless the Ozaki path is selected */
+#define SPLAB_PATH_AUTO 0  /* Ozaki for large double/complex-double ssb shapes, else DMMA */
 #define SPLAB_PATH_DMMA 1  /* FP64 tensor cores (mma.sync f64); float inputs accumulate in FP64 */
-#define SPLAB_PATH_OZAKI 2 /* double / complex double only: Ozaki scheme II on INT8 tcgen05 */
+#define SPLAB_PATH_OZAKI 2 /* Ozaki scheme II on INT8 tcgen05 for double / complex double with
+                              op(A) in {T, C}, op(B) = N; other problems use DMMA */
 
 #define SPLAB_OK 0
 #define SPLAB_ERR_INVALID 1     /* bad argument (sizes, leading dimensions, dtype, path) */
@@ -49,9 +50,10 @@ extern "C" {
 
 SPLAB_API const char *splab_status_string(int status);
 
-/* Bytes of device scratch splab_gemm needs for this problem (0 if none). */
-SPLAB_API size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t m, int64_t n,
-                                 int64_t k);
+/* Bytes of device scratch splab_gemm needs for this problem (0 if none);
+ * ozakiModuli as for splab_gemm. */
+SPLAB_API size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t m,
+                                           int64_t n, int64_t k, int ozakiModuli);
 
 /*
  * C <- alpha * op(A) * op(B) + beta * C on the device, asynchronous on `stream`.
@@ -60,13 +62,21 @@ SPLAB_API size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB
  * (src/pgemm_ssb/pgemm_ssb_gpu.cpp:259-262, opA in {T,C}, opB = N) and
  * pgemm_sbs (src/pgemm_sbs/pgemm_sbs_gpu.cpp:246-249, N,N) reduce to, plus the
  * fill-mode tile skipping of pgemm_ssbtr (src/block_generation/block.hpp:58-66).
- * ozakiModuli: number of CRT moduli for SPLAB_PATH_OZAKI (0 = default for
- * <= 1e-14 relative error); ignored otherwise.
+ * ozakiModuli: number of CRT moduli for SPLAB_PATH_OZAKI (0 = default, 15, for
+ * <= 1e-14 relative error; 8..20); ignored otherwise. A bounded device wait
+ * that gives up makes the next splab_gemm_check() return SPLAB_ERR_TIMEOUT.
  */
 SPLAB_API int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int64_t k,
                const void *alpha, const void *A, int64_t lda, const void *B, int64_t ldb,
                const void *beta, void *C, int64_t ldc, int fill, int64_t ro, int64_t co,
                int ozakiModuli, void *workspace, size_t workspaceBytes, void *stream);
+
+/*
+ * Synchronise `stream` and report a device-side failure of the last
+ * splab_gemm that used `workspace` (SPLAB_OK or SPLAB_ERR_TIMEOUT).
+ */
+SPLAB_API int splab_gemm_check(int dtype, int path, int opA, int opB, int64_t m, int64_t n,
+                               int64_t k, int ozakiModuli, void *workspace, void *stream);
 
 /*
  * Block-cyclic index map on the device: for each of `count` block indices in

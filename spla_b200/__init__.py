@@ -87,7 +87,11 @@ def _declare(L):
     L.splab_gemm.argtypes = [i, i, i, i, i64, i64, i64, vp, vp, i64, vp, i64, vp, vp, i64, i, i64,
                              i64, i, vp, sz, vp]
     L.splab_gemm.restype = i
-    L.splab_gemm_workspace_size.argtypes = [i, i, i, i, i64, i64, i64]
+    L.splab_gemm_workspace_size.argtypes = [i, i, i, i, i64, i64, i64, i]
+    L.splab_gemm_check.argtypes = [i, i, i, i, i64, i64, i64, i, vp, vp]
+    L.splab_gemm_check.restype = i
+    L.splab_set_phase_events.argtypes = [vp, i]
+    L.splab_set_phase_events.restype = i
     L.splab_gemm_workspace_size.restype = sz
     L.splab_status_string.argtypes = [i]
     L.splab_status_string.restype = ct.c_char_p
@@ -367,5 +371,11 @@ def splab_gemm(dtype, path, opA, opB, m, n, k, alpha, A, lda, B, ldb, beta, C, l
                             ro, co, moduli, _addr(workspace)[0], workspace_bytes, stream)
 
 
-def splab_gemm_workspace_size(dtype, path, opA, opB, m, n, k):
-    return lib().splab_gemm_workspace_size(_dtype_of(dtype=dtype), path, opA, opB, m, n, k)
+def splab_gemm_workspace_size(dtype, path, opA, opB, m, n, k, moduli=0):
+    return lib().splab_gemm_workspace_size(_dtype_of(dtype=dtype), path, opA, opB, m, n, k,
+                                           moduli)
+
+
+def splab_gemm_check(dtype, path, opA, opB, m, n, k, moduli=0, workspace=None, stream=0):
+    return lib().splab_gemm_check(_dtype_of(dtype=dtype), path, opA, opB, m, n, k, moduli,
+                                  _addr(workspace)[0], stream)

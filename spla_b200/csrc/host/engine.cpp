@@ -119,10 +119,11 @@ void local_gemm(ContextInternal& ctx, SplaOperation opA, SplaOperation opB, int 
   }
 
   if (devA && devB) {
-    const size_t ws = splab_gemm_workspace_size(dtype, path, opA, opB, m, n, k);
+    const size_t ws = splab_gemm_workspace_size(dtype, path, opA, opB, m, n, k, moduli);
     void* w = ws ? ctx.device_pool().get(1, ws) : nullptr;
     check_splab(splab_gemm(dtype, path, opA, opB, m, n, k, &alpha, A, lda, B, ldb, &beta, dC,
                            dldc, fill, ro, co, moduli, w, ws, cs));
+    check_splab(splab_gemm_check(dtype, path, opA, opB, m, n, k, moduli, w, cs));
   } else {
     // Stream A and B in k-chunks: chunk c is copied on the copy stream into
     // buffer c % 2 while the compute stream contracts chunk c - 1; beta applies
@@ -143,8 +144,9 @@ void local_gemm(ContextInternal& ctx, SplaOperation opA, SplaOperation opB, int 
       if (!devB) bufB[b] = static_cast<T*>(ctx.device_pool().get(4 + b, bbytes));
     }
     const int64_t klast = k - (chunks - 1) * kc;
-    const size_t ws = std::max(splab_gemm_workspace_size(dtype, path, opA, opB, m, n, kc),
-                               splab_gemm_workspace_size(dtype, path, opA, opB, m, n, klast));
+    const size_t ws =
+        std::max(splab_gemm_workspace_size(dtype, path, opA, opB, m, n, kc, moduli),
+                 splab_gemm_workspace_size(dtype, path, opA, opB, m, n, klast, moduli));
     void* w = ws ? ctx.device_pool().get(1, ws) : nullptr;
     cudaStream_t xs = ctx.copy_stream();
     // C (if staged) must be in place before the first contraction
@@ -181,6 +183,7 @@ void local_gemm(ContextInternal& ctx, SplaOperation opA, SplaOperation opB, int 
                              c == 0 ? &beta : &one, dC, dldc, fill, ro, co, moduli, w, ws, cs));
       check_cuda(cudaEventRecord(ctx.event(2 + b), cs));  // buffer b consumed
     }
+    check_splab(splab_gemm_check(dtype, path, opA, opB, m, n, klast, moduli, w, cs));
   }
 
   if (!devC)

@@ -1,9 +1,755 @@
-// Ozaki scheme II contraction (placeholder until the tcgen05 kernels land).
+// Ozaki scheme II contraction on INT8 tensor cores (tcgen05, sm_100a).
+//
+// C <- alpha * op(A) * op(B) + beta * C for double / complex double with
+// op(A) in {T, C} and op(B) = N (the layout of pgemm_ssb: both operands
+// K-major, reference src/pgemm_ssb/pgemm_ssb_host.cpp:168-171).
+//
+// Method (Ozaki, Uchino & Imamura, "Ozaki Scheme II: A GEMM-oriented emulation
+// of floating-point matrix multiplication using an integer modular
+// technique", 2025), restated here in our own formulation:
+//   1. Real form. A complex product is one real GEMM of twice the depth: row i
+//      of op(A) read as 2k reals (its interleaved memory), against two real
+//      rows per column j of B, u_j = (br, -s bi) and v_j = (bi, s br)
+//      interleaved, s = -1 for A^H, +1 for A^T:  Re C_ij = a_i . u_j,
+//      Im C_ij = a_i . v_j.
+//   2. Scaling. Every row x is scaled by 2^sigma so that ||2^sigma x||_2 < 2^Q
+//      and rounded to integers A', B' (exact in double, |.| < 2^Q).
+//      Then |(A' B'^T)_ij| <= ||A'_i|| ||B'_j|| < 2^(2Q) by Cauchy-Schwarz.
+//   3. Residues. For pairwise coprime moduli p_t <= 256 with product
+//      P > 2^(2Q+1), the residues A' mod p_t, B' mod p_t (symmetric, int8)
+//      are multiplied exactly on the INT8 tensor cores with INT32
+//      accumulation (k-chunks of at most 124928 so that 128*128*chunk < 2^31),
+//      reduced mod p_t and accumulated over chunks.
+//   4. Reconstruction. The Chinese remainder theorem gives X = A' B'^T exactly
+//      (|X| < P/2); C = 2^(-sigma_i - tau_j) X, then alpha/beta.
+// The only rounding is the integer rounding of step 2 (relative to each row's
+// 2-norm, 2^-Q) and the final conversion of X to double.
+//
+// Kernels: oz_row_scale (row norms -> sigma), oz_slice (scaled residues, int8,
+// K-major, one matrix per modulus), oz_gemm (tcgen05.mma kind::i8, TMA-fed,
+// TMEM accumulators, warp-specialised persistent kernel), oz_reconstruct (CRT +
+// scaling + alpha/beta + fill-mode tile skipping into C).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+#include "common.cuh"
 #include "ozaki.cuh"
+#include "ozaki_crt.cuh"
 
 namespace splab {
-size_t ozaki_workspace_bytes(const GemmProblem&, int) { return 0; }
-cudaError_t ozaki_gemm(const GemmProblem&, int, void*, size_t, cudaStream_t) {
-  return cudaErrorNotSupported;
+namespace oz {
+
+constexpr int BM = 128;       // rows of A per tile (TMEM lanes)
+constexpr int BN = 256;       // rows of B per tile (TMEM columns)
+constexpr int BKB = 128;      // k bytes per pipeline stage (one 128-byte swizzle atom)
+constexpr int STAGES = 4;
+constexpr int A_STAGE = BM * BKB;  // 16 KiB
+constexpr int B_STAGE = BN * BKB;  // 32 KiB
+constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
+constexpr int GEMM_THREADS = 192;  // warp 0: TMA, warp 1: MMA, warps 2-5: epilogue
+constexpr int GEMM_SMEM = STAGES * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*alignment*/;
+// Max k (bytes) per INT32 accumulation: 127/128 * 128 * 128 * chunk < 2^31.
+constexpr int kChunkBlocks = 976;  // 976 * 128 = 124928
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any wait
+
+// --------------------------------------------------------------------------
+// device helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Wait for the phase of `bar` with parity `parity` to complete. Bounded: gives
+// up after kWaitLimitNs or when another role raised *abort, and returns false.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort,
+                                          unsigned long long limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 0) {
+      if (*abort) return false;
+      if (globaltimer() - t0 > limit_ns) {
+        *abort = 1;
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major operand in the 128-byte swizzle
+// layout written by TMA (8-row atoms of 128 B, atoms 1024 B apart).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= uint64_t((saddr >> 4) & 0x3FFFu);  // start address
+  d |= uint64_t(1) << 16;                  // leading byte offset (unused for SW128 K-major)
+  d |= uint64_t(1024 >> 4) << 32;          // stride byte offset: 8 rows x 128 B
+  d |= uint64_t(1) << 46;                  // descriptor version (sm_100)
+  d |= uint64_t(2) << 61;                  // layout: 128-byte swizzle
+  return d;
+}
+
+// Instruction descriptor of tcgen05.mma kind::i8: S32 accumulate, signed int8
+// A and B, both K-major, M = 128, N = 256.
+constexpr uint32_t kIdescI8 = (2u << 4)              // D format S32
+                              | (1u << 7)            // A format: signed int8
+                              | (1u << 10)           // B format: signed int8
+                              | (uint32_t(BN >> 3) << 17)  // N / 8
+                              | (uint32_t(BM >> 4) << 24); // M / 16
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdescI8), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+        "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+        "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// --------------------------------------------------------------------------
+// 1. row scale exponents
+
+// One block per row: sigma = Q - e where ||row||_2 = f 2^e, f in [0.5, 1).
+// Rows of zeros get sigma = 0.
+__global__ void oz_row_scale(const double* __restrict__ X, int64_t ld_doubles, int64_t len,
+                             int rows, int q_bits, int* __restrict__ sigma) {
+  const int row = blockIdx.x;
+  if (row >= rows) return;
+  const double* x = X + int64_t(row) * ld_doubles;
+  double s = 0.0;
+  for (int64_t l = threadIdx.x; l < len; l += blockDim.x) s = fma(x[l], x[l], s);
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) {
+      int e = 0;
+      if (s > 0.0) frexp(sqrt(s), &e);
+      sigma[row] = s > 0.0 ? q_bits - e : 0;
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// 2. residues
+
+struct SliceConsts {
+  int n;
+  int p[kMaxModuli];
+  double inv_p[kMaxModuli];
+};
+
+// Symmetric residue of an integer-valued double x (|x| < 2^62) modulo p, as
+// int8: x - p * rint(x / p) is exact (|result| < 2p), then folded into
+// [-p/2, p/2) (for p = 256: [-128, 127]).
+__device__ __forceinline__ int sym_residue(double x, double p, double inv_p) {
+  const double q = rint(x * inv_p);
+  double r = fma(-q, p, x);
+  const double half = 0.5 * p;
+  if (r >= half) r -= p;
+  if (r < -half) r += p;
+  if (r >= half) r -= p;
+  if (r < -half) r += p;
+  return int(r);
+}
+
+// Residues of one operand, written K-major: res[t][row][l] (row stride kp).
+// Each thread handles 16 consecutive reals of one row.
+// mode 0: plain rows (A rows, or B rows of a real product): out row = row.
+// mode 1: complex B rows -> u row `row` and v row `row + rows` with sign s:
+//         u = (br, -s*bi), v = (bi, s*br) interleaved.
+__global__ void oz_slice(const double* __restrict__ X, int64_t ld_doubles, int64_t len, int rows,
+                         int64_t kp, const int* __restrict__ sigma, int mode, int s_sign,
+                         int8_t* __restrict__ res, int64_t res_mod_stride, SliceConsts sc) {
+  const int64_t groups = kp / 16;
+  const int64_t gid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int row = int(gid / groups);
+  if (row >= rows) return;
+  const int64_t l0 = (gid % groups) * 16;
+  const double* x = X + int64_t(row) * ld_doubles;
+  const int sg = sigma[row];
+  double v[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int64_t l = l0 + i;
+    v[i] = l < len ? rint(ldexp(x[l], sg)) : 0.0;
+  }
+  for (int t = 0; t < sc.n; ++t) {
+    const double p = double(sc.p[t]), ip = sc.inv_p[t];
+    int r[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) r[i] = sym_residue(v[i], p, ip);
+    int8_t* out = res + t * res_mod_stride;
+    if (mode == 0) {
+      uint32_t w[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        w[q] = (uint32_t(uint8_t(r[4 * q])) | (uint32_t(uint8_t(r[4 * q + 1])) << 8) |
+                (uint32_t(uint8_t(r[4 * q + 2])) << 16) | (uint32_t(uint8_t(r[4 * q + 3])) << 24));
+      *reinterpret_cast<uint4*>(out + int64_t(row) * kp + l0) = make_uint4(w[0], w[1], w[2], w[3]);
+    } else {
+      uint32_t wu[4], wv[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        // pairs (re, im) at positions 4q, 4q+1 and 4q+2, 4q+3
+        const int br0 = r[4 * q], bi0 = r[4 * q + 1], br1 = r[4 * q + 2], bi1 = r[4 * q + 3];
+        const int u0 = br0, u1 = -s_sign * bi0, u2 = br1, u3 = -s_sign * bi1;
+        const int v0 = bi0, v1 = s_sign * br0, v2 = bi1, v3 = s_sign * br1;
+        wu[q] = uint32_t(uint8_t(u0)) | (uint32_t(uint8_t(u1)) << 8) |
+                (uint32_t(uint8_t(u2)) << 16) | (uint32_t(uint8_t(u3)) << 24);
+        wv[q] = uint32_t(uint8_t(v0)) | (uint32_t(uint8_t(v1)) << 8) |
+                (uint32_t(uint8_t(v2)) << 16) | (uint32_t(uint8_t(v3)) << 24);
+      }
+      *reinterpret_cast<uint4*>(out + int64_t(row) * kp + l0) =
+          make_uint4(wu[0], wu[1], wu[2], wu[3]);
+      *reinterpret_cast<uint4*>(out + int64_t(row + rows) * kp + l0) =
+          make_uint4(wv[0], wv[1], wv[2], wv[3]);
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// 3. INT8 residue GEMM on tcgen05
+
+struct GemmParams {
+  int m;             // rows of A per modulus
+  int nb;            // rows of B per modulus
+  int kblocks;       // kp / 128
+  int nchunks;       // ceil(kblocks / kChunkBlocks)
+  int nmod;
+  int tiles_m, tiles_n;
+  int total_units;   // nmod * nchunks * tiles_m * tiles_n
+  int* R;            // accumulated residues [nmod][nb][m] (int32)
+  int* status;       // set to 1 when a bounded wait gave up
+  unsigned long long wait_limit_ns;  // bound on every barrier wait
+  int stall_test;    // 1: the producer issues no copies (exercises the bounded waits)
+  int p[kMaxModuli];
+};
+
+struct Unit {
+  int t, c, tm, tn;
+};
+
+__device__ __forceinline__ Unit decode_unit(int u, const GemmParams& g) {
+  Unit r;
+  const int tiles = g.tiles_m * g.tiles_n;
+  const int tile = u % tiles;
+  const int rest = u / tiles;
+  r.tm = tile % g.tiles_m;
+  r.tn = tile / g.tiles_m;
+  r.c = rest % g.nchunks;
+  r.t = rest / g.nchunks;
+  return r;
+}
+
+__global__ void __launch_bounds__(GEMM_THREADS, 1)
+    oz_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+            const __grid_constant__ GemmParams g) {
+  extern __shared__ unsigned char smem_raw[];
+  // 1024-byte aligned base for the 128-byte swizzle atoms
+  const uint32_t raw_addr = smem_u32(smem_raw);
+  const uint32_t base = (raw_addr + 1023u) & ~1023u;
+  unsigned char* base_ptr = smem_raw + (base - raw_addr);
+  const uint32_t bar_base = base + STAGES * STAGE_BYTES;
+  auto full_bar = [&](int s) { return bar_base + 8u * s; };
+  auto empty_bar = [&](int s) { return bar_base + 8u * (STAGES + s); };
+  auto accf_bar = [&](int b) { return bar_base + 8u * (2 * STAGES + b); };
+  auto acce_bar = [&](int b) { return bar_base + 8u * (2 * STAGES + 2 + b); };
+  const uint32_t drain_bar = bar_base + 8u * (2 * STAGES + 4);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base_ptr + STAGES * STAGE_BYTES + 256);
+  volatile int* abort = reinterpret_cast<volatile int*>(base_ptr + STAGES * STAGE_BYTES + 264);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf_bar(b), 1);
+      mbar_init(acce_bar(b), 128);
+    }
+    mbar_init(drain_bar, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                     smem_u32(tmem_slot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer
+    int stage = 0;
+    uint32_t phase = 0;
+    bool ok = g.stall_test == 0;
+    for (int u = blockIdx.x; u < g.total_units && ok; u += gridDim.x) {
+      const Unit w = decode_unit(u, g);
+      const int kb0 = w.c * kChunkBlocks;
+      const int kb1 = min(g.kblocks, kb0 + kChunkBlocks);
+      const int arow = w.t * g.m + w.tm * BM;
+      const int brow = w.t * g.nb + w.tn * BN;
+      for (int kb = kb0; kb < kb1; ++kb) {
+        if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort, g.wait_limit_ns)) {
+          ok = false;
+          break;
+        }
+        mbar_arrive_expect_tx(full_bar(stage), STAGE_BYTES);
+        const uint32_t sa = base + stage * STAGE_BYTES;
+        tma_load_2d(sa, &tmA, kb * BKB, arow, full_bar(stage));
+        tma_load_2d(sa + A_STAGE, &tmB, kb * BKB, brow, full_bar(stage));
+        if (++stage == STAGES) {
+          stage = 0;
+          phase ^= 1u;
+        }
+      }
+    }
+    if (!ok && g.stall_test == 0) {
+      // let the copies already issued land before the shared memory goes away
+      for (int s = 0; s < STAGES; ++s) {
+        const unsigned long long t0 = globaltimer();
+        while (!mbar_try_wait(full_bar(s), 0) && !mbar_try_wait(full_bar(s), 1) &&
+               globaltimer() - t0 < 1000000ull) {
+        }
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer
+    int stage = 0;
+    uint32_t phase = 0;
+    uint32_t acc_phase[2] = {0, 0};
+    int accb = 0;
+    bool ok = true;
+    for (int u = blockIdx.x; u < g.total_units && ok; u += gridDim.x) {
+      const Unit w = decode_unit(u, g);
+      const int kb0 = w.c * kChunkBlocks;
+      const int kb1 = min(g.kblocks, kb0 + kChunkBlocks);
+      if (!mbar_wait(acce_bar(accb), acc_phase[accb] ^ 1u, abort, g.wait_limit_ns)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t d = tmem_base + uint32_t(accb * BN);
+      for (int kb = kb0; kb < kb1; ++kb) {
+        if (!mbar_wait(full_bar(stage), phase, abort, g.wait_limit_ns)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = base + stage * STAGE_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BKB / 32; ++kk) {
+          const uint64_t ad = umma_desc_sw128(sa + kk * 32);
+          const uint64_t bd = umma_desc_sw128(sa + A_STAGE + kk * 32);
+          umma_i8(d, ad, bd, (kb > kb0 || kk > 0) ? 1u : 0u);
+        }
+        umma_commit(empty_bar(stage));
+        if (++stage == STAGES) {
+          stage = 0;
+          phase ^= 1u;
+        }
+      }
+      if (!ok) break;
+      umma_commit(accf_bar(accb));
+      acc_phase[accb] ^= 1u;
+      accb ^= 1;
+    }
+    if (!ok) {
+      // MMAs may still be in flight: wait (bounded) until they retire
+      umma_commit(drain_bar);
+      const unsigned long long t0 = globaltimer();
+      while (!mbar_try_wait(drain_bar, 0) && globaltimer() - t0 < 1000000ull) {
+      }
+    }
+  } else if (warp >= 2) {
+    // ---- epilogue: TMEM -> registers -> mod p -> accumulate into R
+    const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
+    const int row = quarter * 32 + lane;
+    uint32_t acc_phase[2] = {0, 0};
+    int accb = 0;
+    for (int u = blockIdx.x; u < g.total_units; u += gridDim.x) {
+      const Unit w = decode_unit(u, g);
+      if (!mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)) break;
+      tc_fence_after();
+      const int p = g.p[w.t];
+      const int i = w.tm * BM + row;
+      const int j0 = w.tn * BN;
+      int* Rt = g.R + int64_t(w.t) * g.nb * g.m;
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(accb * BN + c0), v);
+        if (i < g.m) {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) {
+            const int j = j0 + c0 + c;
+            if (j < g.nb) {
+              int r = int(v[c]) % p;
+              if (r < 0) r += p;
+              atomicAdd(Rt + int64_t(j) * g.m + i, r);
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(acce_bar(accb));
+      acc_phase[accb] ^= 1u;
+      accb ^= 1;
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (*abort && threadIdx.x == 0) atomicExch(g.status, 1);
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base)
+                 : "memory");
+  }
+}
+
+// --------------------------------------------------------------------------
+// 4. reconstruction
+
+// C(i, j) <- alpha * 2^(-sigma_i - tau_j) * X + beta * C(i, j); complex: real
+// part from R row j, imaginary part from R row n + j.
+template <bool CPLX>
+__global__ void oz_reconstruct(const int* __restrict__ R, int m, int n, int nb,
+                               const int* __restrict__ sigA, const int* __restrict__ sigB,
+                               void* C, int64_t ldc, double alr, double ali, double ber,
+                               double bei, int fill, int64_t ro, int64_t co, int tile_m, int tile_n,
+                               ReconParams rp) {
+  const int64_t total = int64_t(m) * n;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int i = int(idx % m), j = int(idx / m);
+    if (fill != 0) {
+      const int64_t ti = (i / tile_m) * int64_t(tile_m), tj = (j / tile_n) * int64_t(tile_n);
+      if (!tile_is_active(fill, ti, tj, ::min((int64_t)tile_m, (int64_t)m - ti), ::min((int64_t)tile_n, (int64_t)n - tj),
+                          ro, co))
+        continue;
+    }
+    int r[kMaxModuli];
+    const int64_t plane = int64_t(nb) * m;
+    for (int t = 0; t < rp.n; ++t) {
+      const int v = R[t * plane + int64_t(j) * m + i];
+      r[t] = v % rp.p[t];
+    }
+    const int e = -(sigA[i] + sigB[j]);
+    const double xr = ldexp(crt_value(r, rp), e);
+    double xi = 0.0;
+    if (CPLX) {
+      for (int t = 0; t < rp.n; ++t) {
+        const int v = R[t * plane + int64_t(n + j) * m + i];
+        r[t] = v % rp.p[t];
+      }
+      xi = ldexp(crt_value(r, rp), e);
+    }
+    double outr = alr * xr - ali * xi, outi = alr * xi + ali * xr;
+    const bool read_c = (ber != 0.0 || bei != 0.0);
+    if (CPLX) {
+      double2* c = static_cast<double2*>(C) + i + int64_t(j) * ldc;
+      if (read_c) {
+        const double2 old = *c;
+        outr += ber * old.x - bei * old.y;
+        outi += ber * old.y + bei * old.x;
+      }
+      *c = make_double2(outr, outi);
+    } else {
+      double* c = static_cast<double*>(C) + i + int64_t(j) * ldc;
+      *c = read_c ? fma(ber, *c, outr) : outr;
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// host orchestration
+
+struct Layout {
+  int nmod;
+  int64_t K2, kp;          // real depth, padded to 128
+  int rowsA, rowsB, nb;    // A rows, B source rows, B residue rows
+  size_t off_sigA, off_sigB, off_resA, off_resB, off_R, off_status, total;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+Layout layout_of(const GemmProblem& p, int moduli) {
+  Layout L{};
+  L.nmod = moduli > 0 ? std::min(moduli, kMaxModuli) : kDefaultModuli;
+  const bool cplx = p.dtype == kC64;
+  L.K2 = cplx ? 2 * p.k : p.k;
+  L.kp = (L.K2 + BKB - 1) / BKB * BKB;
+  L.rowsA = int(p.m);
+  L.rowsB = int(p.n);
+  L.nb = cplx ? int(2 * p.n) : int(p.n);
+  size_t off = 0;
+  L.off_sigA = off;
+  off = align256(off + sizeof(int) * L.rowsA);
+  L.off_sigB = off;
+  off = align256(off + sizeof(int) * L.rowsB);
+  L.off_resA = off;
+  off = align256(off + size_t(L.nmod) * L.rowsA * L.kp);
+  L.off_resB = off;
+  off = align256(off + size_t(L.nmod) * L.nb * L.kp);
+  L.off_R = off;
+  off = align256(off + sizeof(int) * size_t(L.nmod) * L.nb * L.rowsA);
+  L.off_status = off;
+  off = align256(off + 256);
+  L.total = off;
+  return L;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* f = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+bool make_map(CUtensorMap* map, void* base, int64_t kp, int64_t rows, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {cuuint64_t(kp), cuuint64_t(rows)};
+  cuuint64_t strides[1] = {cuuint64_t(kp)};
+  cuuint32_t box[2] = {cuuint32_t(BKB), cuuint32_t(box_rows)};
+  cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+int sm_count() {
+  int dev = 0, v = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+  return v;
+}
+
+}  // namespace oz
+
+size_t ozaki_workspace_bytes(const GemmProblem& p, int moduli) {
+  if (p.m <= 0 || p.n <= 0) return 0;
+  return oz::layout_of(p, moduli).total;
+}
+
+bool ozaki_supported(const GemmProblem& p) {
+  return (p.dtype == kR64 || p.dtype == kC64) && p.opA != 0 && p.opB == 0 &&
+         p.m <= (1 << 24) && p.n <= (1 << 23);
+}
+
+cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_bytes,
+                       cudaStream_t st) {
+  using namespace oz;
+  if (!ozaki_supported(p)) return cudaErrorNotSupported;
+  if (p.m <= 0 || p.n <= 0) return cudaSuccess;
+  const Layout L = layout_of(p, moduli);
+  if (ws_bytes < L.total || !ws) return cudaErrorInvalidValue;
+  const Crt crt = make_crt(L.nmod);
+  const bool cplx = p.dtype == kC64;
+  char* w = static_cast<char*>(ws);
+  int* sigA = reinterpret_cast<int*>(w + L.off_sigA);
+  int* sigB = reinterpret_cast<int*>(w + L.off_sigB);
+  int8_t* resA = reinterpret_cast<int8_t*>(w + L.off_resA);
+  int8_t* resB = reinterpret_cast<int8_t*>(w + L.off_resB);
+  int* R = reinterpret_cast<int*>(w + L.off_R);
+  int* status = reinterpret_cast<int*>(w + L.off_status);
+  const double* A = static_cast<const double*>(p.A);
+  const double* B = static_cast<const double*>(p.B);
+  const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in doubles
+  const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
+
+  cudaError_t e;
+  phase_mark(0, false, st);
+  if (p.k > 0) {
+    oz_row_scale<<<L.rowsA, 256, 0, st>>>(A, ldA, L.K2, L.rowsA, crt.q_bits, sigA);
+    oz_row_scale<<<L.rowsB, 256, 0, st>>>(B, ldB, L.K2, L.rowsB, crt.q_bits, sigB);
+    SliceConsts sc{};
+    sc.n = L.nmod;
+    for (int t = 0; t < L.nmod; ++t) {
+      sc.p[t] = crt.p[t];
+      sc.inv_p[t] = crt.inv_p[t];
+    }
+    const int64_t groups = L.kp / 16;
+    const int threads = 256;
+    oz_slice<<<unsigned((int64_t(L.rowsA) * groups + threads - 1) / threads), threads, 0, st>>>(
+        A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA, int64_t(L.rowsA) * L.kp, sc);
+    const int s_sign = p.opA == 2 ? -1 : 1;
+    oz_slice<<<unsigned((int64_t(L.rowsB) * groups + threads - 1) / threads), threads, 0, st>>>(
+        B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0, s_sign, resB, int64_t(L.nb) * L.kp, sc);
+  } else {
+    cudaMemsetAsync(sigA, 0, sizeof(int) * L.rowsA, st);
+    cudaMemsetAsync(sigB, 0, sizeof(int) * L.rowsB, st);
+  }
+  cudaMemsetAsync(R, 0, sizeof(int) * size_t(L.nmod) * L.nb * L.rowsA, st);
+  cudaMemsetAsync(status, 0, sizeof(int), st);
+  phase_mark(0, true, st);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+
+  phase_mark(1, false, st);
+  if (p.k > 0) {
+    CUtensorMap mapA, mapB;
+    if (!make_map(&mapA, resA, L.kp, int64_t(L.nmod) * L.rowsA, BM) ||
+        !make_map(&mapB, resB, L.kp, int64_t(L.nmod) * L.nb, BN))
+      return cudaErrorNotSupported;
+    GemmParams g{};
+    g.m = L.rowsA;
+    g.nb = L.nb;
+    g.kblocks = int(L.kp / BKB);
+    g.nchunks = (g.kblocks + kChunkBlocks - 1) / kChunkBlocks;
+    g.nmod = L.nmod;
+    g.tiles_m = (L.rowsA + BM - 1) / BM;
+    g.tiles_n = (L.nb + BN - 1) / BN;
+    g.total_units = g.nmod * g.nchunks * g.tiles_m * g.tiles_n;
+    g.R = R;
+    g.status = status;
+    g.wait_limit_ns = kWaitLimitNs;
+    g.stall_test = 0;
+    if (const char* v = std::getenv("SPLAB_OZAKI_STALL_TEST")) {
+      // test hook for the failure path: no copies are issued, every wait runs
+      // into a 50 ms bound, the kernel reports SPLAB_ERR_TIMEOUT and returns
+      if (v[0] == '1') {
+        g.stall_test = 1;
+        g.wait_limit_ns = 50000000ull;
+      }
+    }
+    for (int t = 0; t < L.nmod; ++t) g.p[t] = crt.p[t];
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
+      attr = true;
+    }
+    const int grid = std::min(g.total_units, sm_count());
+    oz_gemm<<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(mapA, mapB, g);
+  }
+  phase_mark(1, true, st);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+
+  phase_mark(2, false, st);
+  ReconParams rp{};
+  rp.n = L.nmod;
+  for (int t = 0; t < L.nmod; ++t) {
+    rp.p[t] = crt.p[t];
+    rp.w_lo[t] = crt.w_lo[t];
+    rp.w_hi[t] = crt.w_hi[t];
+  }
+  rp.P_lo = crt.P_lo;
+  rp.P_hi = crt.P_hi;
+  rp.P_d = crt.P_d;
+  const int64_t total = p.m * p.n;
+  const int threads = 256;
+  const unsigned blocks = unsigned(std::min<int64_t>((total + threads - 1) / threads, 148 * 32));
+  if (cplx)
+    oz_reconstruct<true><<<blocks, threads, 0, st>>>(
+        R, L.rowsA, int(p.n), L.nb, sigA, sigB, p.C, p.ldc, p.alpha[0], p.alpha[1], p.beta[0],
+        p.beta[1], p.fill_mode, p.fill_ro, p.fill_co, BM, BN / 2, rp);
+  else
+    oz_reconstruct<false><<<blocks, threads, 0, st>>>(
+        R, L.rowsA, int(p.n), L.nb, sigA, sigB, p.C, p.ldc, p.alpha[0], p.alpha[1], p.beta[0],
+        p.beta[1], p.fill_mode, p.fill_ro, p.fill_co, BM, BN, rp);
+  phase_mark(2, true, st);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+int ozaki_status(const GemmProblem& p, int moduli, void* ws, cudaStream_t st) {
+  const oz::Layout L = oz::layout_of(p, moduli);
+  int h = 0;
+  cudaMemcpyAsync(&h, static_cast<char*>(ws) + L.off_status, sizeof(int), cudaMemcpyDeviceToHost,
+                  st);
+  cudaStreamSynchronize(st);
+  return h;
+}
+
 }  // namespace splab

@@ -14,6 +14,14 @@ size_t ozaki_workspace_bytes(const GemmProblem& prob, int moduli);
 
 // C <- alpha * op(A) * op(B) + beta * C for double / complex double through
 // INT8 residue GEMMs on tcgen05 and Chinese-remainder reconstruction.
+// True when the Ozaki path handles this problem (double / complex double,
+// op(A) in {T, C}, op(B) = N).
+bool ozaki_supported(const GemmProblem& prob);
+
+// Status word of the last ozaki_gemm on this workspace (synchronises
+// `stream`): 0 = ok, 1 = a bounded device wait gave up.
+int ozaki_status(const GemmProblem& prob, int moduli, void* workspace, cudaStream_t stream);
+
 cudaError_t ozaki_gemm(const GemmProblem& prob, int moduli, void* workspace, size_t ws_bytes,
                        cudaStream_t stream);
 

@@ -1,0 +1,178 @@
+// Chinese-remainder constants and reconstruction of the Ozaki scheme II path
+// (host and device code). The reconstruction is exact integer arithmetic on
+// 64-bit limbs; see ozaki.cu for the method.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+namespace splab {
+namespace oz {
+
+inline constexpr int kMaxModuli = 20;
+// Pairwise coprime moduli <= 256, largest first (256 = 2^8, 255 = 3*5*17,
+// 253 = 11*23, 247 = 13*19, 217 = 7*31, the rest prime).
+inline constexpr int kModuli[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
+                                     223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
+inline constexpr int kDefaultModuli = 15;
+
+struct Crt {
+  int n;
+  int p[kMaxModuli];
+  double inv_p[kMaxModuli];
+  unsigned long long w_lo[kMaxModuli], w_hi[kMaxModuli];  // CRT weights W_t < P
+  unsigned long long P_lo, P_hi;
+  double P_d;
+  int q_bits;  // Q: scaled rows have 2-norm < 2^Q
+};
+
+// --------------------------------------------------------------------------
+// host: CRT constants
+
+inline Crt make_crt(int n) {
+  Crt c{};
+  c.n = n;
+  unsigned __int128 P = 1;
+  for (int t = 0; t < n; ++t) P *= (unsigned __int128)kModuli[t];
+  for (int t = 0; t < n; ++t) {
+    const int p = kModuli[t];
+    c.p[t] = p;
+    c.inv_p[t] = 1.0 / double(p);
+    const unsigned __int128 Mt = P / (unsigned __int128)p;
+    const int mt_mod = int(Mt % (unsigned __int128)p);
+    int y = 1;
+    while ((mt_mod * y) % p != 1) ++y;  // modular inverse, p <= 256
+    const unsigned __int128 W = Mt * (unsigned __int128)y;  // < P since y < p
+    c.w_lo[t] = (unsigned long long)W;
+    c.w_hi[t] = (unsigned long long)(W >> 64);
+  }
+  c.P_lo = (unsigned long long)P;
+  c.P_hi = (unsigned long long)(P >> 64);
+  c.P_d = double(c.P_hi) * 18446744073709551616.0 + double(c.P_lo);
+  // |X| <= (2^Q + sqrt(K)/2)^2 must stay below P/2: Q = floor((log2 P - 2) / 2).
+  const double lp = std::log2(c.P_d);
+  c.q_bits = int(std::floor((lp - 2.0) / 2.0));
+  return c;
+}
+
+struct ReconParams {
+  int n;
+  int p[kMaxModuli];
+  unsigned long long w_lo[kMaxModuli], w_hi[kMaxModuli];
+  unsigned long long P_lo, P_hi;
+  double P_d;
+};
+
+__host__ __device__ __forceinline__ unsigned long long mulhi64(unsigned long long a,
+                                                               unsigned long long b) {
+#ifdef __CUDA_ARCH__
+  return __umul64hi(a, b);
+#else
+  return (unsigned long long)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+
+// Correctly rounded conversion of the signed 128-bit value x1:x0 (two's
+// complement) to double: the magnitude's top 64 bits (with a sticky bit for
+// the rest) are converted once and scaled by a power of two.
+__host__ __device__ __forceinline__ double i128_to_double(unsigned long long x1,
+                                                           unsigned long long x0) {
+  const bool neg = (long long)x1 < 0;
+  if (neg) {  // negate: ~x + 1
+    x0 = ~x0 + 1ull;
+    x1 = ~x1 + (x0 == 0 ? 1ull : 0ull);
+  }
+  double mag;
+  if (x1 == 0) {
+    mag = double(x0);
+  } else {
+#ifdef __CUDA_ARCH__
+    const int lz = __clzll((long long)x1);
+#else
+    const int lz = __builtin_clzll(x1);
+#endif
+    const unsigned long long top = lz ? ((x1 << lz) | (x0 >> (64 - lz))) : x1;
+    const unsigned long long rest = lz ? (x0 << lz) : x0;
+    mag = ldexp(double(top | (rest != 0 ? 1ull : 0ull)), 64 - lz);
+  }
+  return neg ? -mag : mag;
+}
+
+// X = (sum_t W_t r_t) mod P as a signed value in (-P/2, P/2], converted to double.
+__host__ __device__ __forceinline__ double crt_value(const int* r, const ReconParams& rp) {
+  // 192-bit accumulation S = s2:s1:s0
+  unsigned long long s0 = 0, s1 = 0, s2 = 0;
+  for (int t = 0; t < rp.n; ++t) {
+    const unsigned long long rt = (unsigned long long)r[t];
+    const unsigned long long lo_lo = rp.w_lo[t] * rt, lo_hi = mulhi64(rp.w_lo[t], rt);
+    const unsigned long long hi_lo = rp.w_hi[t] * rt, hi_hi = mulhi64(rp.w_hi[t], rt);
+    // add lo part
+    unsigned long long a = s0 + lo_lo;
+    unsigned long long c = a < s0;
+    s0 = a;
+    unsigned long long b = s1 + lo_hi;
+    unsigned long long c2 = b < s1;
+    b += c;
+    c2 += (b < c);
+    s1 = b;
+    s2 += c2;
+    // add hi part at 2^64
+    a = s1 + hi_lo;
+    c = a < s1;
+    s1 = a;
+    s2 += hi_hi + c;
+  }
+  // q = floor(S / P) estimated in double (q < n * 256), then S - qP
+  const double S_d = double(s2) * 3.402823669209385e38 + double(s1) * 18446744073709551616.0 +
+                     double(s0);
+  unsigned long long q = (unsigned long long)floor(S_d / rp.P_d);
+  // qP (192-bit)
+  const unsigned long long qp0 = rp.P_lo * q, qp0h = mulhi64(rp.P_lo, q);
+  const unsigned long long qp1l = rp.P_hi * q, qp1h = mulhi64(rp.P_hi, q);
+  unsigned long long t1 = qp0h + qp1l;
+  unsigned long long t2 = qp1h + (t1 < qp0h);
+  // X = S - qP (192-bit two's complement)
+  unsigned long long x0 = s0 - qp0;
+  unsigned long long br = s0 < qp0;
+  unsigned long long x1 = s1 - t1 - br;
+  unsigned long long br1 = (s1 < t1) || (s1 - t1 < br);
+  unsigned long long x2 = s2 - t2 - br1;
+  // fix-up into [0, P)
+  for (int it = 0; it < 3; ++it) {
+    if ((long long)x2 < 0) {  // X < 0: X += P
+      unsigned long long n0 = x0 + rp.P_lo;
+      unsigned long long cy = n0 < x0;
+      unsigned long long n1 = x1 + rp.P_hi + cy;
+      unsigned long long cy1 = (n1 < x1) || (cy && n1 == x1);
+      x0 = n0;
+      x1 = n1;
+      x2 += cy1;
+    } else if (x2 > 0 || x1 > rp.P_hi || (x1 == rp.P_hi && x0 >= rp.P_lo)) {  // X >= P
+      unsigned long long n0 = x0 - rp.P_lo;
+      unsigned long long b0 = x0 < rp.P_lo;
+      unsigned long long n1 = x1 - rp.P_hi - b0;
+      unsigned long long b1 = (x1 < rp.P_hi) || (x1 - rp.P_hi < b0);
+      x0 = n0;
+      x1 = n1;
+      x2 -= b1;
+    }
+  }
+  // now 0 <= X < P (x2 == 0). Symmetric: X > P/2 -> X - P.
+  const unsigned long long hP_hi = rp.P_hi >> 1,
+                           hP_lo = (rp.P_lo >> 1) | (rp.P_hi << 63);
+  const bool upper = x1 > hP_hi || (x1 == hP_hi && x0 > hP_lo);
+  if (upper) {
+    const unsigned long long n0 = x0 - rp.P_lo;
+    const unsigned long long b0 = x0 < rp.P_lo;
+    const unsigned long long n1 = x1 - rp.P_hi - b0;
+    x0 = n0;
+    x1 = n1;  // now the top limb is negative (two's complement 128-bit)
+  }
+  return i128_to_double(x1, x0);
+}
+
+
+}  // namespace oz
+}  // namespace splab

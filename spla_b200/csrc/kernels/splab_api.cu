@@ -73,10 +73,16 @@ GemmProblem make_problem(int dtype, int opA, int opB, int64_t m, int64_t n, int6
   return p;
 }
 
-int use_ozaki(int dtype, int path) {
-  if (path == SPLAB_PATH_OZAKI) return 1;
-  (void)dtype;
-  return 0;
+constexpr bool kAutoUsesOzaki = false;
+
+// Ozaki when requested (or, for AUTO, when the problem is a large ssb-shaped
+// FP64 contraction) and the path supports the layout; DMMA otherwise.
+bool use_ozaki(const GemmProblem& p, int path) {
+  if (!ozaki_supported(p)) return false;
+  if (path == SPLAB_PATH_OZAKI) return true;
+  if (path == SPLAB_PATH_DMMA) return false;
+  const double flops = double(p.m) * p.n * p.k * (p.dtype == kC64 ? 8.0 : 2.0);
+  return kAutoUsesOzaki && p.m >= 256 && p.n >= 128 && p.k >= 8192 && flops >= 2e12;
 }
 
 __global__ void block_cyclic_info_kernel(int64_t rb, int64_t cb, int64_t gr, int64_t gc,
@@ -124,8 +130,8 @@ const char* splab_status_string(int status) {
 }
 
 size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t m, int64_t n,
-                                 int64_t k) {
-  if (dtype < 0 || dtype > 3 || m <= 0 || n <= 0 || k <= 0) return 0;
+                                 int64_t k, int ozakiModuli) {
+  if (dtype < 0 || dtype > 3 || m <= 0 || n <= 0 || k < 0) return 0;
   GemmProblem p{};
   p.dtype = dtype;
   p.opA = opA;
@@ -133,8 +139,23 @@ size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t 
   p.m = m;
   p.n = n;
   p.k = k;
-  if (use_ozaki(dtype, path)) return ozaki_workspace_bytes(p, 0);
+  if (use_ozaki(p, path)) return ozaki_workspace_bytes(p, ozakiModuli);
   return dmma_plan(p, num_sms()).workspace_bytes;
+}
+
+int splab_gemm_check(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int64_t k,
+                     int ozakiModuli, void* workspace, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  GemmProblem p{};
+  p.dtype = dtype;
+  p.opA = opA;
+  p.opB = opB;
+  p.m = m;
+  p.n = n;
+  p.k = k;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return SPLAB_ERR_LAUNCH;
+  if (m <= 0 || n <= 0 || !workspace || !use_ozaki(p, path)) return SPLAB_OK;
+  return ozaki_status(p, ozakiModuli, workspace, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
 }
 
 int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int64_t k,
@@ -149,8 +170,8 @@ int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int6
   GemmProblem p = make_problem(dtype, opA, opB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
                                fill, ro, co);
   cudaError_t err;
-  if (use_ozaki(dtype, path)) {
-    if (!dtype_is_double(dtype)) return SPLAB_ERR_UNSUPPORTED;
+  if (ozakiModuli != 0 && (ozakiModuli < 8 || ozakiModuli > 20)) return SPLAB_ERR_INVALID;
+  if (use_ozaki(p, path)) {
     const size_t need = ozaki_workspace_bytes(p, ozakiModuli);
     if (need > workspaceBytes || (need && !workspace)) return SPLAB_ERR_WORKSPACE;
     err = ozaki_gemm(p, ozakiModuli, workspace, workspaceBytes, st);

@@ -1,0 +1,69 @@
+// CPU check of the Ozaki path's Chinese-remainder reconstruction (the same
+// host/device code the reconstruction kernel runs): random integers X with
+// |X| < P/2 are reduced modulo every modulus, reconstructed, and compared with
+// X converted to double. Also checks the CRT weights: W_t = 1 mod p_t and
+// 0 mod p_s (s != t). Prints "OK <cases>" on success.
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+
+#include "../../spla_b200/csrc/kernels/ozaki_crt.cuh"
+
+using namespace splab::oz;
+typedef unsigned __int128 u128;
+typedef __int128 i128;
+
+static int mod_pos(i128 x, int p) {
+  i128 r = x % p;
+  if (r < 0) r += p;
+  return int(r);
+}
+
+int main() {
+  std::mt19937_64 rng(12345);
+  long cases = 0;
+  for (int n = 8; n <= 16; ++n) {
+    const Crt c = make_crt(n);
+    const u128 P = (u128(c.P_hi) << 64) | c.P_lo;
+    for (int t = 0; t < n; ++t) {
+      const u128 W = (u128(c.w_hi[t]) << 64) | c.w_lo[t];
+      if (W >= P) { printf("FAIL weight >= P\n"); return 1; }
+      for (int s = 0; s < n; ++s) {
+        const int r = int(W % u128(c.p[s]));
+        if (r != (s == t ? 1 : 0)) { printf("FAIL weight %d mod %d = %d\n", t, c.p[s], r); return 1; }
+      }
+    }
+    ReconParams rp{};
+    rp.n = n;
+    for (int t = 0; t < n; ++t) { rp.p[t] = c.p[t]; rp.w_lo[t] = c.w_lo[t]; rp.w_hi[t] = c.w_hi[t]; }
+    rp.P_lo = c.P_lo; rp.P_hi = c.P_hi; rp.P_d = c.P_d;
+    const i128 half = i128(P / 2);
+    for (int it = 0; it < 20000; ++it) {
+      i128 X;
+      const int kind = it % 5;
+      if (kind == 0) X = half - 1 - i128(rng() % 1000);
+      else if (kind == 1) X = -half + 1 + i128(rng() % 1000);
+      else if (kind == 2) X = i128(int64_t(rng() % 2000001) - 1000000);
+      else {
+        u128 v = (u128(rng()) << 64) | rng();
+        v %= P;
+        X = i128(v) - half;
+      }
+      int r[kMaxModuli];
+      for (int t = 0; t < n; ++t) r[t] = mod_pos(X, c.p[t]);
+      const double got = crt_value(r, rp);
+      const long long hi = (long long)(X >> 64);
+      const unsigned long long lo = (unsigned long long)X;
+      const double want = (double)((long double)hi * 18446744073709551616.0L + (long double)lo);
+      const double diff = got > want ? got - want : want - got;
+      const double tol = (want < 0 ? -want : want) * 2.3e-16 + 1e-300;
+      if (diff > tol) {
+        printf("FAIL n=%d it=%d got %.17g want %.17g\n", n, it, got, want);
+        return 1;
+      }
+      ++cases;
+    }
+  }
+  printf("OK %ld\n", cases);
+  return 0;
+}

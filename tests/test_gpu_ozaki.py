@@ -1,0 +1,132 @@
+"""Ozaki scheme II path (INT8 tcgen05) against the double-double oracle.
+
+Covers: complex A^H B and A^T B, real A^T B, partial tiles in both
+dimensions, several k-chunks (k*2 > 124928), alpha/beta with C offsets and
+ldc padding, k = 0, the modulus-count knob, the fill-mode tile skipping, and
+the failure path of the bounded device waits (no GPU fault: the producer
+issues no copies, every wait runs into a 50 ms bound)."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import oracle
+import spla_b200 as spla
+from inputs import buffer
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(x):
+    import torch
+    return torch.from_numpy(x).cuda()
+
+
+def run_ssb(dt, m, n, k, opA, alpha=1.0, beta=0.0, ro=0, co=0, pad=0, fill=0, moduli=0,
+            seed=1, dist="gauss_k", path=spla.PATH_OZAKI, cols=None):
+    A = buffer(dt, k + pad, m, seed, dist, k)
+    B = buffer(dt, k + pad, n, seed + 1, dist, k)
+    ldc = m + ro + pad
+    C = buffer(dt, ldc, n + co, seed + 2, "uniform11")
+    ctx = spla.Context(spla.PU_GPU)
+    ctx.set_fp64_path(path, moduli)
+    d = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128, 128)
+    dC = _dev(C)
+    spla.pgemm_ssbtr(m, n, k, opA, alpha, _dev(A), k + pad, _dev(B), k + pad, beta, dC, ldc, ro,
+                     co, fill, d, ctx)
+    got = dC.cpu().numpy()
+    ref = C.copy()
+    assert oracle.pgemm_ssb(m, n, k, opA, alpha, A, k + pad, B, k + pad, beta, ref, ldc, ro, co) == 0
+    return C, got, ref, ldc
+
+
+def block(x, ldc, m, n, ro, co):
+    return x.reshape(-1, ldc)[co:co + n, ro:ro + m]
+
+
+@pytest.mark.parametrize("opA", [2, 1])
+def test_complex_multi_chunk_partial_tiles(opA):
+    m, n, k = 300, 150, 150000  # 2k = 300000 -> 3 k-chunks; 3 x 2 tiles, partial
+    C0, got, ref, ldc = run_ssb(np.complex128, m, n, k, opA)
+    err = oracle.rel_fro(got, ref)
+    assert err <= 1e-14, err
+
+
+def test_real_double():
+    m, n, k = 200, 330, 70000
+    C0, got, ref, ldc = run_ssb(np.float64, m, n, k, 1, dist="uniform11")
+    assert oracle.rel_fro(got, ref) <= 1e-14
+
+
+def test_alpha_beta_offsets_padding():
+    m, n, k, ro, co = 70, 90, 20000, 3, 2
+    alpha, beta = 0.5 - 1.25j, 0.75 + 0.5j
+    C0, got, ref, ldc = run_ssb(np.complex128, m, n, k, 2, alpha, beta, ro, co, pad=5)
+    gb, rb = block(got, ldc, m, n, ro, co), block(ref, ldc, m, n, ro, co)
+    assert oracle.rel_fro(gb, rb) <= 1e-14
+    # everything outside the block is bit-unchanged
+    mask = np.ones((n + co, ldc), bool)
+    mask[co:co + n, ro:ro + m] = False
+    assert np.array_equal(got.reshape(-1, ldc)[mask], C0.reshape(-1, ldc)[mask])
+
+
+def test_k_zero_scales_c():
+    m, n = 40, 30
+    C0, got, ref, ldc = run_ssb(np.complex128, m, n, 0, 2, 1.0, 0.5 - 0.5j)
+    assert oracle.rel_fro(got, ref) <= 1e-15
+
+
+@pytest.mark.parametrize("moduli,bar", [(16, 1e-14), (20, 1e-14), (12, 1e-9)])
+def test_modulus_count(moduli, bar):
+    m, n, k = 130, 70, 30000
+    C0, got, ref, ldc = run_ssb(np.complex128, m, n, k, 2, moduli=moduli)
+    assert oracle.rel_fro(got, ref) <= bar
+
+
+def test_fill_lower_triangle():
+    m = n = 300
+    k = 6000
+    C0, got, ref, ldc = run_ssb(np.complex128, m, n, k, 2, fill=spla.FILL_MODE_LOWER)
+    g, r = got.reshape(n, ldc).T[:m], ref.reshape(n, ldc).T[:m]
+    c0 = C0.reshape(n, ldc).T[:m]
+    tri = np.tril(np.ones((m, n), bool))
+    assert oracle.rel_fro(g[tri], r[tri]) <= 1e-14
+    off = ~tri
+    ok = np.isclose(g[off], r[off], rtol=1e-12, atol=1e-14) | (g[off] == c0[off])
+    assert ok.all()
+
+
+def test_bounded_wait_failure_path():
+    """The INT8 GEMM's barrier waits are bounded: with the test hook the
+    producer issues no copies, the waits give up after 50 ms, the kernel frees
+    its tensor memory and returns, and the call reports SPLA_GPU_LAUNCH_ERROR
+    (SPLAB_ERR_TIMEOUT) without faulting; the context stays usable."""
+    code = r"""
+import sys, numpy as np, torch
+sys.path[:0] = [%r, %r]
+import spla_b200 as spla
+m, n, k = 64, 64, 4096
+A = torch.randn(m * k, dtype=torch.complex128, device='cuda')
+B = torch.randn(n * k, dtype=torch.complex128, device='cuda')
+C = torch.zeros(m * n, dtype=torch.complex128, device='cuda')
+ctx = spla.Context(spla.PU_GPU); ctx.set_fp64_path(spla.PATH_OZAKI)
+d = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, 'R', 1, 1, 64, 64)
+try:
+    spla.pgemm_ssb(m, n, k, 2, 1.0, A, k, B, k, 0.0, C, m, 0, 0, d, ctx)
+    print('NO_ERROR')
+except spla.GPULaunchError:
+    print('TIMEOUT_REPORTED')
+# the device is still usable afterwards
+ctx.set_fp64_path(spla.PATH_DMMA)
+spla.pgemm_ssb(m, n, k, 2, 1.0, A, k, B, k, 0.0, C, m, 0, 0, d, ctx)
+torch.cuda.synchronize()
+print('DEVICE_OK')
+""" % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+       os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, SPLAB_OZAKI_STALL_TEST="1")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                         timeout=300)
+    assert "TIMEOUT_REPORTED" in out.stdout, out.stdout + out.stderr
+    assert "DEVICE_OK" in out.stdout, out.stdout + out.stderr
