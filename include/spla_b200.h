@@ -13,7 +13,7 @@ extern "C" {
 /* Select the contraction path a context uses for double and complex double:
  * path 0 = automatic, 1 = FP64 tensor cores (DMMA), 2 = Ozaki scheme II on
  * INT8 tensor cores. moduli = number of CRT moduli for path 2 (0 = default,
- * sized for <= 1e-14 relative error); valid range 0..20. The environment
+ * sized for <= 1e-14 relative error); valid: 0 or 8..16. The environment
  * variables SPLA_B200_PATH (auto|dmma|ozaki) and SPLA_B200_OZAKI_MODULI set the
  * defaults of new contexts. */
 SPLA_EXPORT SplaError spla_b200_ctx_set_fp64_path(SplaContext ctx, int path, int moduli);

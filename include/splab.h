@@ -63,7 +63,7 @@ SPLAB_API size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB
  * pgemm_sbs (src/pgemm_sbs/pgemm_sbs_gpu.cpp:246-249, N,N) reduce to, plus the
  * fill-mode tile skipping of pgemm_ssbtr (src/block_generation/block.hpp:58-66).
  * ozakiModuli: number of CRT moduli for SPLAB_PATH_OZAKI (0 = default, 15, for
- * <= 1e-14 relative error; 8..20); ignored otherwise. A bounded device wait
+ * <= 1e-14 relative error; 8..16); ignored otherwise. A bounded device wait
  * that gives up makes the next splab_gemm_check() return SPLAB_ERR_TIMEOUT.
  */
 SPLAB_API int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int64_t k,

@@ -280,7 +280,8 @@ SplaError spla_ctx_set_alloc_gpu(SplaContext ctx, void* (*a)(size_t), void (*f)(
 // path of a context. path: 0 auto, 1 FP64 DMMA, 2 Ozaki INT8; moduli 0 = default.
 SPLA_EXPORT SplaError spla_b200_ctx_set_fp64_path(SplaContext ctx, int path, int moduli) {
   if (!ctx) return SPLA_INVALID_HANDLE_ERROR;
-  if (path < 0 || path > 2 || moduli < 0 || moduli > 20) return SPLA_INVALID_PARAMETER_ERROR;
+  if (path < 0 || path > 2 || moduli < 0 || moduli > 16 || (moduli > 0 && moduli < 8))
+    return SPLA_INVALID_PARAMETER_ERROR;
   return guarded([&] {
     auto& c = spla::detail::Access::ctx(as_ctx(ctx));
     c.set_fp64_path(path);

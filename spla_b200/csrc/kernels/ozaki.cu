@@ -559,7 +559,7 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 Layout layout_of(const GemmProblem& p, int moduli) {
   Layout L{};
-  L.nmod = moduli > 0 ? std::min(moduli, kMaxModuli) : kDefaultModuli;
+  L.nmod = moduli > 0 ? std::min(moduli, kMaxUsableModuli) : kDefaultModuli;
   const bool cplx = p.dtype == kC64;
   L.K2 = cplx ? 2 * p.k : p.k;
   L.kp = (L.K2 + BKB - 1) / BKB * BKB;

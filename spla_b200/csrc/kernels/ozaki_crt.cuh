@@ -10,7 +10,9 @@
 namespace splab {
 namespace oz {
 
-inline constexpr int kMaxModuli = 20;
+inline constexpr int kMaxModuli = 20;  // table size
+// The product of the moduli must fit 128 bits: at most 16 (2^124.4).
+inline constexpr int kMaxUsableModuli = 16;
 // Pairwise coprime moduli <= 256, largest first (256 = 2^8, 255 = 3*5*17,
 // 253 = 11*23, 247 = 13*19, 217 = 7*31, the rest prime).
 inline constexpr int kModuli[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,

@@ -170,7 +170,7 @@ int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int6
   GemmProblem p = make_problem(dtype, opA, opB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
                                fill, ro, co);
   cudaError_t err;
-  if (ozakiModuli != 0 && (ozakiModuli < 8 || ozakiModuli > 20)) return SPLAB_ERR_INVALID;
+  if (ozakiModuli != 0 && (ozakiModuli < 8 || ozakiModuli > 16)) return SPLAB_ERR_INVALID;
   if (use_ozaki(p, path)) {
     const size_t need = ozaki_workspace_bytes(p, ozakiModuli);
     if (need > workspaceBytes || (need && !workspace)) return SPLAB_ERR_WORKSPACE;

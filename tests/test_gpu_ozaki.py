@@ -78,11 +78,19 @@ def test_k_zero_scales_c():
     assert oracle.rel_fro(got, ref) <= 1e-15
 
 
-@pytest.mark.parametrize("moduli,bar", [(16, 1e-14), (20, 1e-14), (12, 1e-9)])
+@pytest.mark.parametrize("moduli,bar", [(16, 1e-14), (14, 1e-13), (12, 1e-9)])
 def test_modulus_count(moduli, bar):
     m, n, k = 130, 70, 30000
     C0, got, ref, ldc = run_ssb(np.complex128, m, n, k, 2, moduli=moduli)
     assert oracle.rel_fro(got, ref) <= bar
+
+
+def test_modulus_count_out_of_range_rejected():
+    ctx = spla.Context(spla.PU_GPU)
+    with pytest.raises(spla.InvalidParameterError):
+        ctx.set_fp64_path(spla.PATH_OZAKI, 17)
+    with pytest.raises(spla.InvalidParameterError):
+        ctx.set_fp64_path(spla.PATH_OZAKI, 5)
 
 
 def test_fill_lower_triangle():
