@@ -79,6 +79,33 @@ SPLAB_API int splab_gemm_check(int dtype, int path, int opA, int opB, int64_t m,
                                int64_t k, int ozakiModuli, void *workspace, void *stream);
 
 /*
+ * Allocation-free FP64 contraction (no counterpart in the reference library).
+ *
+ * Same operation and arguments as splab_gemm on the DMMA path (FP64 tensor
+ * cores), minus the workspace: for callers that cannot allocate device
+ * memory - applications whose device memory belongs to a framework allocator
+ * that must account for every byte, processes under a hard device-memory
+ * cap, and latency-critical loops that cannot take the device synchronisation
+ * of cudaMalloc / cudaFree. It allocates nothing: the split-K partials live
+ * in one static device array of SPLAB_NOALLOC_SCRATCH_BYTES (64 MiB) that
+ * every GPU loading the library holds until exit. Problems with
+ * m * n * e > 32 MiB (e = 16 bytes for complex, 8 for real dtypes: one FP64
+ * partial of C; two must fit) are rejected with SPLAB_ERR_WORKSPACE; the
+ * others use fewer k-splits than splab_gemm when the partials would not fit.
+ * The first call on a device looks up the array's device address (with that
+ * device current); make that first call before any stream capture. All calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller. Inputs and outputs are passed by the caller as for
+ * splab_gemm; alpha/beta are host pointers.
+ */
+#define SPLAB_NOALLOC_SCRATCH_BYTES (64u << 20)
+SPLAB_API int splab_gemm_dmma_noalloc(int dtype, int opA, int opB, int64_t m, int64_t n, int64_t k,
+                                      const void *alpha, const void *A, int64_t lda,
+                                      const void *B, int64_t ldb, const void *beta, void *C,
+                                      int64_t ldc, int fill, int64_t ro, int64_t co,
+                                      void *stream);
+
+/*
  * Block-cyclic index map on the device: for each of `count` block indices in
  * blockIdx (device, column-major block order) write 9 int64 values to out
  * (device): global row, global col, global sub-row, global sub-col, local row,

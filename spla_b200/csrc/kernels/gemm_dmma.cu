@@ -23,8 +23,10 @@
 // skipped (C left unchanged), with the reference's block predicate
 // (src/block_generation/block.hpp:58-66) applied per tile.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
+#include "../../../include/splab.h"
 #include "gemm_dmma.cuh"
 
 namespace splab {
@@ -505,4 +507,64 @@ cudaError_t reduce_partials(const GemmProblem& pr, const void* P, int splits, in
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the FP64 contraction.
+//
+// For callers that must not allocate device memory themselves or through
+// this library: applications whose device memory is owned by a framework
+// allocator that has to account for every byte, processes running against a
+// hard device-memory cap, and latency-critical loops that cannot afford the
+// implicit device synchronisation of cudaMalloc / cudaFree. The split-K
+// partials live in one file-scope device array of SPLAB_NOALLOC_SCRATCH_BYTES
+// that every GPU loading this library holds until the process exits.
+//
+// The array's host-side symbol is only a stand-in: its device address is
+// looked up with cudaGetSymbolAddress, once per device, by the first call on
+// that device (with that device current). Make that first call before any
+// stream capture. All calls share the array and it keeps the last call's
+// contents; nothing in it has to start at zero (every split overwrites its
+// partial tile before the reduction reads it). Calls whose execution overlaps
+// on the GPU (different streams, or different host threads) race on the
+// array and must be serialised by the caller.
+
+static __device__ __align__(256) unsigned char noalloc_scratch[SPLAB_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex noalloc_mutex;
+void* noalloc_ptr[64] = {nullptr};
+
+cudaError_t noalloc_scratch_address(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(noalloc_mutex);
+  if (!noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    noalloc_ptr[dev] = p;
+  }
+  *out = noalloc_ptr[dev];
+  return cudaSuccess;
+}
+}  // namespace
+
+int dmma_gemm_noalloc(const GemmProblem& pr, int num_sms, cudaStream_t st) {
+  if (pr.m <= 0 || pr.n <= 0) return 0;
+  // one k-split's partials are m * n FP64 (complex: pairs); two must fit
+  const size_t per_split = size_t(pr.m) * size_t(pr.n) * (dtype_is_complex(pr.dtype) ? 16 : 8);
+  if (2 * per_split > SPLAB_NOALLOC_SCRATCH_BYTES) return 2;
+  DmmaPlan plan = dmma_plan(pr, num_sms);
+  if (plan.workspace_bytes > SPLAB_NOALLOC_SCRATCH_BYTES) {
+    // fewer k-splits so that the partials fit the static array
+    const int fit = int(size_t(SPLAB_NOALLOC_SCRATCH_BYTES) / per_split);
+    plan = dmma_plan(pr, num_sms, fit);
+    if (plan.workspace_bytes > SPLAB_NOALLOC_SCRATCH_BYTES) return 2;
+  }
+  void* scratch = nullptr;
+  if (plan.workspace_bytes > 0 && noalloc_scratch_address(&scratch) != cudaSuccess) return 3;
+  return dmma_gemm(pr, plan, scratch, st) == cudaSuccess ? 0 : 3;
+}
 }  // namespace splab

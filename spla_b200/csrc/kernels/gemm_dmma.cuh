@@ -44,6 +44,11 @@ DmmaPlan dmma_plan(const GemmProblem& prob, int num_sms, int force_splits = 0);
 cudaError_t dmma_gemm(const GemmProblem& prob, const DmmaPlan& plan, void* workspace,
                       cudaStream_t stream);
 
+// The DMMA contraction with its split-K partials in a static device array
+// (no allocation). Returns 0, 2 when the problem needs more scratch than the
+// array holds, 3 on a CUDA error.
+int dmma_gemm_noalloc(const GemmProblem& prob, int num_sms, cudaStream_t stream);
+
 // Sum `splits` FP64 partial tiles in order and apply alpha/beta into C.
 cudaError_t reduce_partials(const GemmProblem& prob, const void* partials, int splits, int tile_m,
                             int tile_n, cudaStream_t stream);

@@ -188,6 +188,21 @@ int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int6
   return err == cudaSuccess ? SPLAB_OK : SPLAB_ERR_LAUNCH;
 }
 
+int splab_gemm_dmma_noalloc(int dtype, int opA, int opB, int64_t m, int64_t n, int64_t k,
+                            const void* alpha, const void* A, int64_t lda, const void* B,
+                            int64_t ldb, const void* beta, void* C, int64_t ldc, int fill,
+                            int64_t ro, int64_t co, void* stream) {
+  if (!valid_problem(dtype, opA, opB, m, n, k, lda, ldb, ldc)) return SPLAB_ERR_INVALID;
+  if (fill < 0 || fill > 2 || !alpha || !beta) return SPLAB_ERR_INVALID;
+  if (m == 0 || n == 0) return SPLAB_OK;
+  if (!C || (k > 0 && (!A || !B))) return SPLAB_ERR_INVALID;
+  GemmProblem p = make_problem(dtype, opA, opB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                               fill, ro, co);
+  const int rc = dmma_gemm_noalloc(p, num_sms(), static_cast<cudaStream_t>(stream));
+  if (rc == 2) return SPLAB_ERR_WORKSPACE;
+  return rc == 0 ? SPLAB_OK : SPLAB_ERR_LAUNCH;
+}
+
 int splab_set_phase_events(void** events, int count) {
   PhaseEvents& pe = phase_events();
   pe.ev = reinterpret_cast<cudaEvent_t*>(events);
