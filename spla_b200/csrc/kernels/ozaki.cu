@@ -211,22 +211,45 @@ __global__ void oz_row_scale(const double* __restrict__ X, int64_t ld_doubles, i
 
 struct SliceConsts {
   int n;
-  int p[kMaxModuli];
-  double inv_p[kMaxModuli];
+  float p[kMaxModuli];
+  float inv_p[kMaxModuli];
+  // 2^(13 i) mod p in symmetric form, i = 1..4 (digit weights)
+  float c[kMaxModuli][4];
 };
 
-// Symmetric residue of an integer-valued double x (|x| < 2^62) modulo p, as
-// int8: x - p * rint(x / p) is exact (|result| < 2p), then folded into
-// [-p/2, p/2) (for p = 256: [-128, 127]).
-__device__ __forceinline__ int sym_residue(double x, double p, double inv_p) {
-  const double q = rint(x * inv_p);
-  double r = fma(-q, p, x);
-  const double half = 0.5 * p;
-  if (r >= half) r -= p;
-  if (r < -half) r += p;
-  if (r >= half) r -= p;
-  if (r < -half) r += p;
-  return int(r);
+// Residues are computed on the FP32 pipe from five balanced base-2^13 digits
+// of the scaled integer x (|x| < 2^62), which are extracted exactly with FP64
+// operations:  x = sum_i d_i 2^(13 i), |d_i| <= 4096 (|d_4| <= 1024). For a
+// modulus p the digit sum s = d_0 + sum_i c_i d_i (|c_i| <= p/2) is below
+// 2^22 in magnitude and exact in FP32; r = s - p * nearest(s / p) lies in
+// [-(p-1)/2, (p-1)/2] for odd p. For p = 256 the weights vanish and r is the
+// low byte of d_0. Each residue is produced as the float MAGIC + r, whose low
+// byte is r in two's complement: the int8 value without a conversion.
+__device__ __forceinline__ void digits13(double x, float (&d)[5]) {
+  const double b = 8192.0, ib = 1.0 / 8192.0;
+  double q1 = rint(x * ib);
+  d[0] = float(fma(q1, -b, x));
+  double q2 = rint(q1 * ib);
+  d[1] = float(fma(q2, -b, q1));
+  double q3 = rint(q2 * ib);
+  d[2] = float(fma(q3, -b, q2));
+  double q4 = rint(q3 * ib);
+  d[3] = float(fma(q4, -b, q3));
+  d[4] = float(q4);
+}
+
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: ulp 1, low mantissa bits hold r
+
+__device__ __forceinline__ uint32_t pack4(float a, float b, float c, float d) {
+  const uint32_t t0 = __byte_perm(__float_as_uint(a), __float_as_uint(b), 0x0040);
+  const uint32_t t1 = __byte_perm(__float_as_uint(c), __float_as_uint(d), 0x0040);
+  return __byte_perm(t0, t1, 0x5410);
+}
+
+// negate the int8 residues in bytes 1 and 3 of a packed word (mod 2^8, which
+// keeps every residue class, including -128 for p = 256)
+__device__ __forceinline__ uint32_t neg_odd_bytes(uint32_t w) {
+  return (w & 0x00FF00FFu) | (__vsub4(0u, w) & 0xFF00FF00u);
 }
 
 // Residues of one operand, written K-major: res[t][row][l] (row stride kp).
@@ -234,47 +257,72 @@ __device__ __forceinline__ int sym_residue(double x, double p, double inv_p) {
 // mode 0: plain rows (A rows, or B rows of a real product): out row = row.
 // mode 1: complex B rows -> u row `row` and v row `row + rows` with sign s:
 //         u = (br, -s*bi), v = (bi, s*br) interleaved.
-__global__ void oz_slice(const double* __restrict__ X, int64_t ld_doubles, int64_t len, int rows,
-                         int64_t kp, const int* __restrict__ sigma, int mode, int s_sign,
-                         int8_t* __restrict__ res, int64_t res_mod_stride, SliceConsts sc) {
+template <bool VEC>
+__global__ void __launch_bounds__(256) oz_slice(const double* __restrict__ X, int64_t ld_doubles,
+                                                int64_t len, int rows, int64_t kp,
+                                                const int* __restrict__ sigma, int mode,
+                                                int s_sign, int8_t* __restrict__ res,
+                                                int64_t res_mod_stride, SliceConsts sc) {
   const int64_t groups = kp / 16;
   const int64_t gid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   const int row = int(gid / groups);
   if (row >= rows) return;
   const int64_t l0 = (gid % groups) * 16;
-  const double* x = X + int64_t(row) * ld_doubles;
+  const double* x = X + int64_t(row) * ld_doubles + l0;
   const int sg = sigma[row];
+  // 2^sg as a double when representable, else ldexp per element
+  const bool direct = sg > -1000 && sg < 1000;
+  const double scale = direct ? __longlong_as_double((long long)(sg + 1023) << 52) : 1.0;
   double v[16];
+  if (VEC && l0 + 16 <= len) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const double2 t = __ldg(reinterpret_cast<const double2*>(x) + i);
+      v[2 * i] = t.x;
+      v[2 * i + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = (l0 + i < len) ? x[i] : 0.0;
+  }
+  float d[16][5];
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
-    const int64_t l = l0 + i;
-    v[i] = l < len ? rint(ldexp(x[l], sg)) : 0.0;
+    const double xi = rint(direct ? v[i] * scale : ldexp(v[i], sg));
+    digits13(xi, d[i]);
   }
   for (int t = 0; t < sc.n; ++t) {
-    const double p = double(sc.p[t]), ip = sc.inv_p[t];
-    int r[16];
+    float r[16];
+    if (t == 0 && sc.p[0] == 256.0f) {
 #pragma unroll
-    for (int i = 0; i < 16; ++i) r[i] = sym_residue(v[i], p, ip);
+      for (int i = 0; i < 16; ++i) r[i] = d[i][0] + kMagic;
+    } else {
+      const float p = sc.p[t], ip = sc.inv_p[t];
+      const float c1 = sc.c[t][0], c2 = sc.c[t][1], c3 = sc.c[t][2], c4 = sc.c[t][3];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        float s = fmaf(c1, d[i][1], d[i][0]);
+        s = fmaf(c2, d[i][2], s);
+        s = fmaf(c3, d[i][3], s);
+        s = fmaf(c4, d[i][4], s);
+        const float q = fmaf(s, ip, kMagic) - kMagic;
+        r[i] = fmaf(-q, p, s + kMagic);
+      }
+    }
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[q] = pack4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
     int8_t* out = res + t * res_mod_stride;
     if (mode == 0) {
-      uint32_t w[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        w[q] = (uint32_t(uint8_t(r[4 * q])) | (uint32_t(uint8_t(r[4 * q + 1])) << 8) |
-                (uint32_t(uint8_t(r[4 * q + 2])) << 16) | (uint32_t(uint8_t(r[4 * q + 3])) << 24));
       *reinterpret_cast<uint4*>(out + int64_t(row) * kp + l0) = make_uint4(w[0], w[1], w[2], w[3]);
     } else {
+      // w = [br0, bi0, br1, bi1]; u = [br, -s bi], v = [bi, s br]
       uint32_t wu[4], wv[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        // pairs (re, im) at positions 4q, 4q+1 and 4q+2, 4q+3
-        const int br0 = r[4 * q], bi0 = r[4 * q + 1], br1 = r[4 * q + 2], bi1 = r[4 * q + 3];
-        const int u0 = br0, u1 = -s_sign * bi0, u2 = br1, u3 = -s_sign * bi1;
-        const int v0 = bi0, v1 = s_sign * br0, v2 = bi1, v3 = s_sign * br1;
-        wu[q] = uint32_t(uint8_t(u0)) | (uint32_t(uint8_t(u1)) << 8) |
-                (uint32_t(uint8_t(u2)) << 16) | (uint32_t(uint8_t(u3)) << 24);
-        wv[q] = uint32_t(uint8_t(v0)) | (uint32_t(uint8_t(v1)) << 8) |
-                (uint32_t(uint8_t(v2)) << 16) | (uint32_t(uint8_t(v3)) << 24);
+        const uint32_t sw = __byte_perm(w[q], 0u, 0x2301);  // [bi0, br0, bi1, br1]
+        wu[q] = s_sign > 0 ? neg_odd_bytes(w[q]) : w[q];
+        wv[q] = s_sign > 0 ? sw : neg_odd_bytes(sw);
       }
       *reinterpret_cast<uint4*>(out + int64_t(row) * kp + l0) =
           make_uint4(wu[0], wu[1], wu[2], wu[3]);
@@ -658,16 +706,35 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
     SliceConsts sc{};
     sc.n = L.nmod;
     for (int t = 0; t < L.nmod; ++t) {
-      sc.p[t] = crt.p[t];
-      sc.inv_p[t] = crt.inv_p[t];
+      const int pt = crt.p[t];
+      sc.p[t] = float(pt);
+      sc.inv_p[t] = 1.0f / float(pt);
+      long long w = 1;
+      for (int i = 0; i < 4; ++i) {
+        w = (w * 8192) % pt;  // 2^(13 (i+1)) mod p
+        const long long c = w > pt / 2 ? w - pt : w;
+        sc.c[t][i] = float(c);
+      }
     }
     const int64_t groups = L.kp / 16;
     const int threads = 256;
-    oz_slice<<<unsigned((int64_t(L.rowsA) * groups + threads - 1) / threads), threads, 0, st>>>(
-        A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA, int64_t(L.rowsA) * L.kp, sc);
+    const unsigned gridA = unsigned((int64_t(L.rowsA) * groups + threads - 1) / threads);
+    const unsigned gridB = unsigned((int64_t(L.rowsB) * groups + threads - 1) / threads);
+    const bool vecA = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (ldA % 2 == 0);
+    const bool vecB = (reinterpret_cast<uintptr_t>(B) % 16 == 0) && (ldB % 2 == 0);
     const int s_sign = p.opA == 2 ? -1 : 1;
-    oz_slice<<<unsigned((int64_t(L.rowsB) * groups + threads - 1) / threads), threads, 0, st>>>(
-        B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0, s_sign, resB, int64_t(L.nb) * L.kp, sc);
+    if (vecA)
+      oz_slice<true><<<gridA, threads, 0, st>>>(A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA,
+                                                int64_t(L.rowsA) * L.kp, sc);
+    else
+      oz_slice<false><<<gridA, threads, 0, st>>>(A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA,
+                                                 int64_t(L.rowsA) * L.kp, sc);
+    if (vecB)
+      oz_slice<true><<<gridB, threads, 0, st>>>(B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0,
+                                                s_sign, resB, int64_t(L.nb) * L.kp, sc);
+    else
+      oz_slice<false><<<gridB, threads, 0, st>>>(B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0,
+                                                 s_sign, resB, int64_t(L.nb) * L.kp, sc);
   } else {
     cudaMemsetAsync(sigA, 0, sizeof(int) * L.rowsA, st);
     cudaMemsetAsync(sigB, 0, sizeof(int) * L.rowsB, st);
