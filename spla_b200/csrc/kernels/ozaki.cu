@@ -540,6 +540,255 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 }
 
 // --------------------------------------------------------------------------
+// 3b. the same GEMM on CTA pairs (tcgen05 cta_group::2)
+//
+// A cluster of two CTAs computes a 256 x 256 tile: each CTA stages 128 rows of
+// A and 128 rows of B per k-block (TMA, no multicast), the even CTA issues
+// tcgen05.mma.cta_group::2 (M = 256, N = 256, K = 32) reading both CTAs'
+// shared memory, and each CTA's TMEM receives its 128 rows of the tile. Per
+// SM this halves the shared-memory operand traffic of the 1-CTA form and
+// runs the tensor pipe at its full int8 rate.
+//   full[s]  (even CTA): TMA bytes of both CTAs + the even producer's arrival
+//   empty[s] (both):     commit of the MMAs, multicast to the pair
+//   accf[b]  (both):     commit after a tile's last k-block, multicast
+//   acce[b]  (even CTA): 256 epilogue threads of both CTAs, remote arrivals
+constexpr int STAGES2 = 6;
+constexpr int A_STAGE2 = 128 * BKB;  // 16 KiB per CTA
+constexpr int B_STAGE2 = 128 * BKB;  // 16 KiB per CTA
+constexpr int STAGE2_BYTES = A_STAGE2 + B_STAGE2;
+constexpr int GEMM2_SMEM = STAGES2 * STAGE2_BYTES + 1024 + 1024;
+constexpr uint32_t kIdescI8Pair = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(256 >> 3) << 17) |
+                                  (uint32_t(256 >> 4) << 24);
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t map_to_rank(uint32_t saddr, uint32_t rank) {
+  uint32_t out;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(saddr), "r"(rank));
+  return out;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                                 uint32_t bar_cluster) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar_cluster)
+      : "memory");
+}
+__device__ __forceinline__ void umma_i8_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                             uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdescI8Pair), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit_pair(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(bar),
+      "h"((unsigned short)0x3)
+      : "memory");
+}
+
+__global__ void __launch_bounds__(GEMM_THREADS, 1)
+    oz_gemm_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                 const __grid_constant__ GemmParams g) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw_addr = smem_u32(smem_raw);
+  const uint32_t base = (raw_addr + 1023u) & ~1023u;
+  unsigned char* base_ptr = smem_raw + (base - raw_addr);
+  const uint32_t bar_base = base + STAGES2 * STAGE2_BYTES;
+  auto full_bar = [&](int s) { return bar_base + 8u * s; };
+  auto empty_bar = [&](int s) { return bar_base + 8u * (STAGES2 + s); };
+  auto accf_bar = [&](int b) { return bar_base + 8u * (2 * STAGES2 + b); };
+  auto acce_bar = [&](int b) { return bar_base + 8u * (2 * STAGES2 + 2 + b); };
+  const uint32_t drain_bar = bar_base + 8u * (2 * STAGES2 + 4);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(base_ptr + STAGES2 * STAGE2_BYTES + 256);
+  volatile int* abort = reinterpret_cast<volatile int*>(base_ptr + STAGES2 * STAGE2_BYTES + 264);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();  // 0: issues the MMAs
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  const int tiles = g.tiles_m * g.tiles_n;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES2; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf_bar(b), 1);
+      mbar_init(acce_bar(b), 256);
+    }
+    mbar_init(drain_bar, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                     smem_u32(tmem_slot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  cluster_sync_all();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  auto unit_of = [&](int u, int& t, int& c, int& tm, int& tn) {
+    const int tile = u % tiles, rest = u / tiles;
+    tm = tile % g.tiles_m;
+    tn = tile / g.tiles_m;
+    c = rest % g.nchunks;
+    t = rest / g.nchunks;
+  };
+
+  bool aborted = false;
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer (both CTAs): 128 rows of A and of B per k-block
+    int stage = 0;
+    uint32_t phase = 0;
+    bool ok = g.stall_test == 0;
+    for (int u = pair; u < g.total_units && ok; u += npairs) {
+      int t, c, tm, tn;
+      unit_of(u, t, c, tm, tn);
+      const int kb0 = c * kChunkBlocks, kb1 = min(g.kblocks, kb0 + kChunkBlocks);
+      const int arow = t * g.m + tm * 256 + int(rank) * 128;
+      const int brow = t * g.nb + tn * 256 + int(rank) * 128;
+      for (int kb = kb0; kb < kb1; ++kb) {
+        if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort, g.wait_limit_ns)) {
+          ok = false;
+          break;
+        }
+        const uint32_t fb = map_to_rank(full_bar(stage), 0);
+        if (rank == 0) mbar_arrive_expect_tx(full_bar(stage), 2 * STAGE2_BYTES);
+        const uint32_t sa = base + stage * STAGE2_BYTES;
+        tma_load_2d_pair(sa, &tmA, kb * BKB, arow, fb);
+        tma_load_2d_pair(sa + A_STAGE2, &tmB, kb * BKB, brow, fb);
+        if (++stage == STAGES2) {
+          stage = 0;
+          phase ^= 1u;
+        }
+      }
+    }
+    aborted = !ok && g.stall_test == 0;
+  } else if (warp == 1 && lane == 0 && rank == 0) {
+    // ---- MMA issuer (even CTA)
+    int stage = 0;
+    uint32_t phase = 0;
+    uint32_t acc_phase[2] = {0, 0};
+    int accb = 0;
+    bool ok = true;
+    for (int u = pair; u < g.total_units && ok; u += npairs) {
+      int t, c, tm, tn;
+      unit_of(u, t, c, tm, tn);
+      const int kb0 = c * kChunkBlocks, kb1 = min(g.kblocks, kb0 + kChunkBlocks);
+      if (!mbar_wait(acce_bar(accb), acc_phase[accb] ^ 1u, abort, g.wait_limit_ns)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t d = tmem_base + uint32_t(accb * 256);
+      for (int kb = kb0; kb < kb1; ++kb) {
+        if (!mbar_wait(full_bar(stage), phase, abort, g.wait_limit_ns)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = base + stage * STAGE2_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BKB / 32; ++kk)
+          umma_i8_pair(d, umma_desc_sw128(sa + kk * 32), umma_desc_sw128(sa + A_STAGE2 + kk * 32),
+                       (kb > kb0 || kk > 0) ? 1u : 0u);
+        umma_commit_pair(empty_bar(stage));
+        if (++stage == STAGES2) {
+          stage = 0;
+          phase ^= 1u;
+        }
+      }
+      if (!ok) break;
+      umma_commit_pair(accf_bar(accb));
+      acc_phase[accb] ^= 1u;
+      accb ^= 1;
+    }
+    if (!ok) {
+      asm volatile(
+          "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              drain_bar)
+          : "memory");
+      const unsigned long long t0 = globaltimer();
+      while (!mbar_try_wait(drain_bar, 0) && globaltimer() - t0 < 1000000ull) {
+      }
+    }
+  } else if (warp >= 2) {
+    // ---- epilogue (both CTAs): own TMEM rows -> mod p -> R
+    const int quarter = warp & 3;
+    const int row = int(rank) * 128 + quarter * 32 + lane;
+    uint32_t acc_phase[2] = {0, 0};
+    int accb = 0;
+    for (int u = pair; u < g.total_units; u += npairs) {
+      int t, c, tm, tn;
+      unit_of(u, t, c, tm, tn);
+      if (!mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)) break;
+      tc_fence_after();
+      const int p = g.p[t];
+      const int i = tm * 256 + row;
+      const int j0 = tn * 256;
+      int* Rt = g.R + int64_t(t) * g.nb * g.m;
+      for (int c0 = 0; c0 < 256; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(accb * 256 + c0), v);
+        if (i < g.m) {
+#pragma unroll
+          for (int cc = 0; cc < 32; ++cc) {
+            const int j = j0 + c0 + cc;
+            if (j < g.nb) {
+              int r = int(v[cc]) % p;
+              if (r < 0) r += p;
+              atomicAdd(Rt + int64_t(j) * g.m + i, r);
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive_cluster(map_to_rank(acce_bar(accb), 0));
+      acc_phase[accb] ^= 1u;
+      accb ^= 1;
+    }
+  }
+
+  if (aborted) {
+    // copies issued by this CTA may still be landing in shared memory
+    const unsigned long long t0 = globaltimer();
+    while (globaltimer() - t0 < 2000000ull) {
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (*abort && threadIdx.x == 0) atomicExch(g.status, 1);
+  cluster_sync_all();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, 512;" ::"r"(tmem_base)
+                 : "memory");
+  }
+}
+
+// --------------------------------------------------------------------------
 // 4. reconstruction
 
 // C(i, j) <- alpha * 2^(-sigma_i - tau_j) * X + beta * C(i, j); complex: real
@@ -772,13 +1021,46 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
       }
     }
     for (int t = 0; t < L.nmod; ++t) g.p[t] = crt.p[t];
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
-      attr = true;
+    const char* gk = std::getenv("SPLAB_OZAKI_GEMM");
+    const bool pair = !(gk && gk[0] == '1');  // "1sm" selects the single-CTA kernel
+    if (pair) {
+      g.tiles_m = (L.rowsA + 255) / 256;
+      g.tiles_n = (L.nb + 255) / 256;
+      g.total_units = g.nmod * g.nchunks * g.tiles_m * g.tiles_n;
+      static bool attr2 = false;
+      if (!attr2) {
+        cudaFuncSetAttribute(oz_gemm_pair, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             GEMM2_SMEM);
+        attr2 = true;
+      }
+      CUtensorMap mapA2, mapB2;
+      if (!make_map(&mapA2, resA, L.kp, int64_t(L.nmod) * L.rowsA, 128) ||
+          !make_map(&mapB2, resB, L.kp, int64_t(L.nmod) * L.nb, 128))
+        return cudaErrorNotSupported;
+      const int pairs = std::max(1, std::min(g.total_units, sm_count() / 2));
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(unsigned(2 * pairs));
+      cfg.blockDim = dim3(GEMM_THREADS);
+      cfg.dynamicSmemBytes = GEMM2_SMEM;
+      cfg.stream = st;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 2;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      e = cudaLaunchKernelEx(&cfg, oz_gemm_pair, mapA2, mapB2, g);
+      if (e != cudaSuccess) return e;
+    } else {
+      static bool attr = false;
+      if (!attr) {
+        cudaFuncSetAttribute(oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
+        attr = true;
+      }
+      const int grid = std::min(g.total_units, sm_count());
+      oz_gemm<<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(mapA, mapB, g);
     }
-    const int grid = std::min(g.total_units, sm_count());
-    oz_gemm<<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(mapA, mapB, g);
   }
   phase_mark(1, true, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
