@@ -106,6 +106,43 @@ SPLAB_API int splab_gemm_dmma_noalloc(int dtype, int opA, int opB, int64_t m, in
                                       void *stream);
 
 /*
+ * Batched grouped contraction (the many-instance form of splab_gemm): all
+ * problems share dtype and op(A)/op(B); each has its own sizes, pointers,
+ * alpha and beta (as (re, im) doubles; im ignored for real dtypes). One
+ * persistent launch walks every (problem, tile, k-chunk) work item, one
+ * grouped launch reduces the split-K partials; the pair is captured in a CUDA
+ * graph on the first run and replayed afterwards. The k-chunk size is chosen
+ * by measuring the candidates on the first run (autotune != 0; C is not
+ * written while measuring) or by a model otherwise. FP64 tensor-core path
+ * (float inputs accumulate in FP64). No counterpart in the reference library
+ * (a batch there is a loop of pgemm_ssb calls).
+ */
+typedef struct splab_problem {
+  int opA, opB;
+  int64_t m, n, k;
+  const void *A;
+  int64_t lda;
+  const void *B;
+  int64_t ldb;
+  void *C;
+  int64_t ldc;
+  double alpha[2], beta[2];
+} splab_problem;
+
+SPLAB_API int splab_batch_create(int dtype, int count, const splab_problem *problems,
+                                 void **plan, size_t *workspaceBytes);
+/* Run (and on the first call tune + capture) the batch on `stream`; workspace
+ * must hold workspaceBytes of device memory and stay the same between runs
+ * (a different pointer triggers a new capture). */
+SPLAB_API int splab_batch_run(void *plan, void *workspace, size_t workspaceBytes, int autotune,
+                              void *stream);
+/* Chosen k-chunk, and the measured time (ms) of each candidate k-chunk when
+ * tuned; arrays of at least 32 entries. */
+SPLAB_API int splab_batch_info(void *plan, int64_t *kChunk, int *nCandidates, int64_t *candidates,
+                               double *tuningMs);
+SPLAB_API int splab_batch_destroy(void *plan);
+
+/*
  * Block-cyclic index map on the device: for each of `count` block indices in
  * blockIdx (device, column-major block order) write 9 int64 values to out
  * (device): global row, global col, global sub-row, global sub-col, local row,

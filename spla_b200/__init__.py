@@ -379,3 +379,69 @@ def splab_gemm_workspace_size(dtype, path, opA, opB, m, n, k, moduli=0):
 def splab_gemm_check(dtype, path, opA, opB, m, n, k, moduli=0, workspace=None, stream=0):
     return lib().splab_gemm_check(_dtype_of(dtype=dtype), path, opA, opB, m, n, k, moduli,
                                   _addr(workspace)[0], stream)
+
+
+# ---------------------------------------------------------------------------
+# batched grouped contraction (splab_batch_*)
+
+
+class _Problem(ct.Structure):
+    _fields_ = [("opA", ct.c_int), ("opB", ct.c_int), ("m", ct.c_int64), ("n", ct.c_int64),
+                ("k", ct.c_int64), ("A", ct.c_void_p), ("lda", ct.c_int64), ("B", ct.c_void_p),
+                ("ldb", ct.c_int64), ("C", ct.c_void_p), ("ldc", ct.c_int64),
+                ("alpha", ct.c_double * 2), ("beta", ct.c_double * 2)]
+
+
+class Batch:
+    """A batch of independent local GEMMs of one dtype and op pair, run as one
+    persistent grouped launch replayed from a CUDA graph (splab_batch_*).
+
+    problems: list of dicts with keys opA, opB, m, n, k, A, lda, B, ldb, C, ldc,
+    alpha, beta (buffers as device tensors or integer addresses)."""
+
+    def __init__(self, dtype, problems):
+        L = lib()
+        L.splab_batch_create.argtypes = [ct.c_int, ct.c_int, ct.c_void_p, ct.POINTER(ct.c_void_p),
+                                         ct.POINTER(ct.c_size_t)]
+        L.splab_batch_run.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_size_t, ct.c_int,
+                                      ct.c_void_p]
+        L.splab_batch_info.argtypes = [ct.c_void_p, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int),
+                                       ct.c_void_p, ct.c_void_p]
+        L.splab_batch_destroy.argtypes = [ct.c_void_p]
+        self.dtype = _dtype_of(dtype=dtype)
+        arr = (_Problem * len(problems))()
+        for i, p in enumerate(problems):
+            a, b = complex(p.get("alpha", 1.0)), complex(p.get("beta", 0.0))
+            arr[i] = _Problem(p["opA"], p["opB"], p["m"], p["n"], p["k"], _addr(p["A"])[0],
+                              p["lda"], _addr(p["B"])[0], p["ldb"], _addr(p["C"])[0], p["ldc"],
+                              (ct.c_double * 2)(a.real, a.imag), (ct.c_double * 2)(b.real, b.imag))
+        self._arr = arr
+        self._plan = ct.c_void_p()
+        ws = ct.c_size_t()
+        rc = L.splab_batch_create(self.dtype, len(problems), ct.cast(arr, ct.c_void_p),
+                                  ct.byref(self._plan), ct.byref(ws))
+        if rc != 0:
+            raise InvalidParameterError(f"splab_batch_create: {L.splab_status_string(rc)}")
+        self.workspace_bytes = ws.value
+
+    def run(self, workspace, stream=0, autotune=True):
+        rc = lib().splab_batch_run(self._plan, _addr(workspace)[0], self.workspace_bytes,
+                                   int(bool(autotune)), stream)
+        if rc != 0:
+            raise GPULaunchError(f"splab_batch_run: {lib().splab_status_string(rc).decode()}")
+
+    def info(self):
+        kc, nc = ct.c_int64(), ct.c_int()
+        cands = (ct.c_int64 * 32)()
+        ms = (ct.c_double * 32)()
+        lib().splab_batch_info(self._plan, ct.byref(kc), ct.byref(nc), ct.cast(cands, ct.c_void_p),
+                               ct.cast(ms, ct.c_void_p))
+        return {"k_chunk": kc.value, "candidates": list(cands[:nc.value]),
+                "tuning_ms": list(ms[:nc.value])}
+
+    def __del__(self):
+        try:
+            if self._plan:
+                lib().splab_batch_destroy(self._plan)
+        except Exception:
+            pass

@@ -23,7 +23,9 @@
 // skipped (C left unchanged), with the reference's block predicate
 // (src/block_generation/block.hpp:58-66) applied per tile.
 #include <algorithm>
+#include <climits>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "../../../include/splab.h"
@@ -176,24 +178,26 @@ __device__ __forceinline__ void store_alpha_beta_impl(void* C, int64_t idx, doub
   }
 }
 
+// One CTA tile (tile index -> (tm, tn), column of tiles fastest) over the
+// k-range of split `split`.
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS) dmma_gemm_kernel(DmmaParams p) {
+__device__ __forceinline__ void dmma_tile(const DmmaParams& p, int64_t tile, int split,
+                                          unsigned char* smem_raw) {
   using S = typename Cfg::S;
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, WM = Cfg::WM, WN = Cfg::WN;
   constexpr int FM = WM / 8, FN = WN / 8, STAGES = Cfg::STAGES;
   constexpr bool CPLX = Cfg::CPLX;
 
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   S* smem = reinterpret_cast<S*>(smem_raw);
 
   const int64_t tiles_m = (p.m + BM - 1) / BM;
-  const int64_t tm = blockIdx.x % tiles_m, tn = blockIdx.x / tiles_m;
+  const int64_t tm = tile % tiles_m, tn = tile / tiles_m;
   const int64_t m0 = tm * BM, n0 = tn * BN;
   if (!tile_is_active(p.fill_mode, m0, n0, ::min((int64_t)BM, p.m - m0),
                       ::min((int64_t)BN, p.n - n0), p.fill_ro, p.fill_co))
     return;
 
-  const int64_t kbeg = static_cast<int64_t>(blockIdx.y) * p.k_per_split;
+  const int64_t kbeg = static_cast<int64_t>(split) * p.k_per_split;
   const int64_t kend = min(p.k, kbeg + p.k_per_split);
   const int nkt = kend > kbeg ? static_cast<int>((kend - kbeg + BK - 1) / BK) : 0;
 
@@ -288,7 +292,7 @@ __global__ void __launch_bounds__(Cfg::THREADS) dmma_gemm_kernel(DmmaParams p) {
         const double xr = accr[fi][fj][e];
         const double xi = CPLX ? acci[CPLX ? fi : 0][CPLX ? fj : 0][e] : 0.0;
         if (p.partial) {
-          const int64_t idx = static_cast<int64_t>(blockIdx.y) * p.m * p.n + j * p.m + i;
+          const int64_t idx = static_cast<int64_t>(split) * p.m * p.n + j * p.m + i;
           if constexpr (CPLX) {
             reinterpret_cast<double2*>(p.P)[idx] = make_double2(xr, xi);
           } else {
@@ -300,6 +304,27 @@ __global__ void __launch_bounds__(Cfg::THREADS) dmma_gemm_kernel(DmmaParams p) {
         }
       }
     }
+  }
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS) dmma_gemm_kernel(DmmaParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  dmma_tile<Cfg>(p, blockIdx.x, int(blockIdx.y), smem_raw);
+}
+
+// Persistent grouped form: CTAs walk a list of (instance, tile, split) work
+// items of many independent problems of one configuration (one launch for a
+// whole batch). Items are pre-sorted by the host (longest first).
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS)
+    dmma_gemm_grouped_kernel(const DmmaParams* __restrict__ params, const int4* __restrict__ items,
+                             int n_items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const int4 w = items[it];
+    __syncthreads();  // the previous item's fragments are no longer read
+    dmma_tile<Cfg>(params[w.x], w.y, w.z, smem_raw);
   }
 }
 
@@ -567,4 +592,311 @@ int dmma_gemm_noalloc(const GemmProblem& pr, int num_sms, cudaStream_t st) {
   if (plan.workspace_bytes > 0 && noalloc_scratch_address(&scratch) != cudaSuccess) return 3;
   return dmma_gemm(pr, plan, scratch, st) == cudaSuccess ? 0 : 3;
 }
+
+// ---------------------------------------------------------------------------
+// Batched grouped contraction: many independent problems of one dtype and
+// operand layout in one persistent launch (plus one grouped reduction),
+// captured in a CUDA graph, with the k-chunk size picked by measurement.
+
+// Grouped reduction: blockIdx.y = problem, x covers its elements.
+template <int DT>
+__global__ void reduce_partials_grouped_kernel(const DmmaParams* __restrict__ params,
+                                               const int* __restrict__ splits, int tile_m,
+                                               int tile_n) {
+  const DmmaParams& p = params[blockIdx.y];
+  const int ns = splits[blockIdx.y];
+  const int64_t total = p.m * p.n;
+  constexpr bool CPLX = dtype_is_complex(DT);
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = idx % p.m, j = idx / p.m;
+    if (p.fill_mode != 0) {
+      const int64_t ti = (i / tile_m) * tile_m, tj = (j / tile_n) * tile_n;
+      if (!tile_is_active(p.fill_mode, ti, tj, ::min((int64_t)tile_m, p.m - ti),
+                          ::min((int64_t)tile_n, p.n - tj), p.fill_ro, p.fill_co))
+        continue;
+    }
+    double sr = 0.0, si = 0.0;
+    if constexpr (CPLX) {
+      const double2* q = static_cast<const double2*>(p.P) + idx;
+      for (int s = 0; s < ns; ++s) {
+        const double2 v = q[s * total];
+        sr += v.x;
+        si += v.y;
+      }
+    } else {
+      const double* q = static_cast<const double*>(p.P) + idx;
+      for (int s = 0; s < ns; ++s) sr += q[s * total];
+    }
+    store_alpha_beta_impl<DT>(p.C, i + j * p.ldc, sr, si, p.alpha_r, p.alpha_i, p.beta_r,
+                              p.beta_i);
+  }
+}
+
+namespace {
+
+template <class Cfg>
+int grouped_occupancy() {
+  static int occ = -1;
+  if (occ < 0) {
+    cudaFuncSetAttribute(dmma_gemm_grouped_kernel<Cfg>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES);
+    int o = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, dmma_gemm_grouped_kernel<Cfg>,
+                                                      Cfg::THREADS, Cfg::SMEM_BYTES) !=
+            cudaSuccess ||
+        o < 1)
+      o = 1;
+    occ = o;
+  }
+  return occ;
+}
+
+}  // namespace
+
+struct BatchPlanImpl {
+  int dtype = 0, opA = 0, opB = 0, count = 0;
+  int bm = 0, bn = 0, bk = 0;
+  std::vector<GemmProblem> probs;
+  int64_t kc = 0;  // k per split (multiple of BK)
+  std::vector<int64_t> candidates;
+  bool tuned = false;
+  std::vector<double> tuning_ms;
+  // device-side tables (allocated by the caller's workspace)
+  size_t off_params = 0, off_items = 0, off_splits = 0, off_partials = 0, total = 0;
+  int n_items = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  void* graph_ws = nullptr;
+  cudaStream_t graph_stream = nullptr;
+};
+
+namespace {
+
+size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <class Cfg>
+void batch_geometry(BatchPlanImpl& b) {
+  b.bm = Cfg::BM;
+  b.bn = Cfg::BN;
+  b.bk = Cfg::BK;
+  int64_t kmin = INT64_MAX, kmax = 0;
+  for (auto& p : b.probs) {
+    kmin = std::min<int64_t>(kmin, p.k);
+    kmax = std::max<int64_t>(kmax, p.k);
+  }
+  // candidate k-chunks: powers of two between 16 BK and the smallest k / 2,
+  // so that every problem has at least two splits (partials only, C untouched
+  // while tuning)
+  b.candidates.clear();
+  for (int64_t c = 16 * Cfg::BK; c <= std::max<int64_t>(16 * Cfg::BK, kmin / 2); c *= 2)
+    b.candidates.push_back(c);
+  // workspace: tables + partials for the smallest candidate (most splits)
+  const int64_t cmin = b.candidates.front();
+  size_t partial_bytes = 0, items = 0;
+  const size_t esz = Cfg::CPLX ? 16 : 8;
+  for (auto& p : b.probs) {
+    const int64_t sp = std::max<int64_t>(1, (p.k + cmin - 1) / cmin);
+    partial_bytes += al256(size_t(sp) * p.m * p.n * esz);
+    items += size_t(sp) * ((p.m + Cfg::BM - 1) / Cfg::BM) * ((p.n + Cfg::BN - 1) / Cfg::BN);
+  }
+  b.off_params = 0;
+  b.off_splits = al256(sizeof(DmmaParams) * b.count);
+  b.off_items = b.off_splits + al256(sizeof(int) * b.count);
+  b.off_partials = b.off_items + al256(sizeof(int4) * items);
+  b.total = b.off_partials + partial_bytes;
+}
+
+// Build the parameter and item tables for k-chunk kc and upload them.
+template <class Cfg>
+cudaError_t batch_tables(BatchPlanImpl& b, int64_t kc, char* ws, cudaStream_t st) {
+  std::vector<DmmaParams> prm(b.count);
+  std::vector<int> splits(b.count);
+  std::vector<std::pair<int64_t, int4>> items;
+  size_t poff = b.off_partials;
+  const size_t esz = Cfg::CPLX ? 16 : 8;
+  for (int i = 0; i < b.count; ++i) {
+    const GemmProblem& pr = b.probs[i];
+    DmmaParams p{};
+    p.A = pr.A;
+    p.B = pr.B;
+    p.C = pr.C;
+    p.lda = pr.lda;
+    p.ldb = pr.ldb;
+    p.ldc = pr.ldc;
+    p.m = pr.m;
+    p.n = pr.n;
+    p.k = pr.k;
+    const int sp = int(std::max<int64_t>(1, (pr.k + kc - 1) / kc));
+    p.k_per_split = kc;
+    p.alpha_r = pr.alpha[0];
+    p.alpha_i = pr.alpha[1];
+    p.beta_r = pr.beta[0];
+    p.beta_i = pr.beta[1];
+    p.conj_a = pr.opA == 2;
+    p.conj_b = pr.opB == 2;
+    p.partial = 1;
+    p.fill_mode = pr.fill_mode;
+    p.fill_ro = pr.fill_ro;
+    p.fill_co = pr.fill_co;
+    p.P = ws + poff;
+    poff += al256(size_t(sp) * pr.m * pr.n * esz);
+    prm[i] = p;
+    splits[i] = sp;
+    const int64_t tiles = ((pr.m + Cfg::BM - 1) / Cfg::BM) * ((pr.n + Cfg::BN - 1) / Cfg::BN);
+    for (int s = 0; s < sp; ++s) {
+      const int64_t klen = std::min<int64_t>(kc, pr.k - int64_t(s) * kc);
+      for (int64_t t = 0; t < tiles; ++t)
+        items.push_back({klen, make_int4(i, int(t), s, 0)});
+    }
+  }
+  if (poff > b.total) return cudaErrorInvalidValue;
+  // longest items first so the persistent CTAs finish together
+  std::stable_sort(items.begin(), items.end(),
+                   [](const auto& a, const auto& c) { return a.first > c.first; });
+  std::vector<int4> flat(items.size());
+  for (size_t i = 0; i < items.size(); ++i) flat[i] = items[i].second;
+  b.n_items = int(flat.size());
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(ws + b.off_params, prm.data(), sizeof(DmmaParams) * b.count,
+                           cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemcpyAsync(ws + b.off_splits, splits.data(), sizeof(int) * b.count,
+                           cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemcpyAsync(ws + b.off_items, flat.data(), sizeof(int4) * flat.size(),
+                           cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return e;
+  return cudaStreamSynchronize(st);  // host tables go out of scope
+}
+
+template <class Cfg>
+cudaError_t batch_launch_gemm(BatchPlanImpl& b, char* ws, cudaStream_t st) {
+  const int slots = grouped_occupancy<Cfg>() * [] {
+    int dev = 0, v = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v;
+  }();
+  const int grid = std::max(1, std::min(b.n_items, slots));
+  dmma_gemm_grouped_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(
+      reinterpret_cast<const DmmaParams*>(ws + b.off_params),
+      reinterpret_cast<const int4*>(ws + b.off_items), b.n_items);
+  return cudaGetLastError();
+}
+
+template <class Cfg>
+cudaError_t batch_launch_reduce(BatchPlanImpl& b, char* ws, cudaStream_t st) {
+  int64_t maxel = 0;
+  for (auto& p : b.probs) maxel = std::max<int64_t>(maxel, p.m * p.n);
+  const int threads = 256;
+  const unsigned bx = unsigned(std::min<int64_t>((maxel + threads - 1) / threads, 256));
+  reduce_partials_grouped_kernel<Cfg::DT><<<dim3(bx, unsigned(b.count)), threads, 0, st>>>(
+      reinterpret_cast<const DmmaParams*>(ws + b.off_params),
+      reinterpret_cast<const int*>(ws + b.off_splits), Cfg::BM, Cfg::BN);
+  return cudaGetLastError();
+}
+
+template <class Cfg>
+cudaError_t batch_run_cfg(BatchPlanImpl& b, char* ws, cudaStream_t st, bool autotune) {
+  cudaError_t e;
+  if (!b.tuned) {
+    if (autotune && b.candidates.size() > 1) {
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      double best = 1e30;
+      int64_t best_kc = b.candidates.front();
+      b.tuning_ms.clear();
+      for (int64_t kc : b.candidates) {
+        if ((e = batch_tables<Cfg>(b, kc, ws, st)) != cudaSuccess) return e;
+        if ((e = batch_launch_gemm<Cfg>(b, ws, st)) != cudaSuccess) return e;  // warm
+        cudaEventRecord(e0, st);
+        if ((e = batch_launch_gemm<Cfg>(b, ws, st)) != cudaSuccess) return e;
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        b.tuning_ms.push_back(ms);
+        if (ms < best) {
+          best = ms;
+          best_kc = kc;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      b.kc = best_kc;
+    } else {
+      // model choice: the candidate closest to 8 k-tiles per ... one wave multiple
+      b.kc = b.candidates.size() > 2 ? b.candidates[2] : b.candidates.back();
+    }
+    if ((e = batch_tables<Cfg>(b, b.kc, ws, st)) != cudaSuccess) return e;
+    b.tuned = true;
+  }
+  // capture once per (workspace, stream), then replay
+  if (!b.exec || b.graph_ws != ws || b.graph_stream != st) {
+    if (b.exec) cudaGraphExecDestroy(b.exec);
+    if (b.graph) cudaGraphDestroy(b.graph);
+    b.exec = nullptr;
+    b.graph = nullptr;
+    if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return e;
+    cudaError_t e1 = batch_launch_gemm<Cfg>(b, ws, st);
+    cudaError_t e2 = batch_launch_reduce<Cfg>(b, ws, st);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(st, &g);
+    if (e1 != cudaSuccess) return e1;
+    if (e2 != cudaSuccess) return e2;
+    if (e != cudaSuccess) return e;
+    b.graph = g;
+    if ((e = cudaGraphInstantiate(&b.exec, g, 0)) != cudaSuccess) return e;
+    b.graph_ws = ws;
+    b.graph_stream = st;
+  }
+  return cudaGraphLaunch(b.exec, st);
+}
+
+template <class F>
+auto batch_dispatch(const BatchPlanImpl& b, F&& f) {
+  GemmProblem pr{};
+  pr.dtype = b.dtype;
+  pr.opA = b.opA;
+  pr.opB = b.opB;
+  return dispatch(pr, f);
+}
+
+}  // namespace
+
+BatchPlanImpl* batch_create(int dtype, const std::vector<GemmProblem>& probs) {
+  auto* b = new BatchPlanImpl();
+  b->dtype = dtype;
+  b->opA = probs.front().opA;
+  b->opB = probs.front().opB;
+  b->count = int(probs.size());
+  b->probs = probs;
+  batch_dispatch(*b, [&](auto cfg) {
+    batch_geometry<decltype(cfg)>(*b);
+    return 0;
+  });
+  return b;
+}
+
+size_t batch_workspace(const BatchPlanImpl* b) { return b->total; }
+
+cudaError_t batch_run(BatchPlanImpl* b, void* ws, cudaStream_t st, bool autotune) {
+  return batch_dispatch(*b, [&](auto cfg) {
+    return batch_run_cfg<decltype(cfg)>(*b, static_cast<char*>(ws), st, autotune);
+  });
+}
+
+void batch_destroy(BatchPlanImpl* b) {
+  if (!b) return;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  delete b;
+}
+
+int64_t batch_kc(const BatchPlanImpl* b) { return b->kc; }
+const std::vector<double>& batch_tuning(const BatchPlanImpl* b) { return b->tuning_ms; }
+const std::vector<int64_t>& batch_candidates(const BatchPlanImpl* b) { return b->candidates; }
 }  // namespace splab

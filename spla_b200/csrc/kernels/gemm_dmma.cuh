@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace splab {
 
@@ -48,6 +49,18 @@ cudaError_t dmma_gemm(const GemmProblem& prob, const DmmaPlan& plan, void* works
 // (no allocation). Returns 0, 2 when the problem needs more scratch than the
 // array holds, 3 on a CUDA error.
 int dmma_gemm_noalloc(const GemmProblem& prob, int num_sms, cudaStream_t stream);
+
+// Batched grouped FP64 contraction (one dtype and operand layout per batch).
+struct BatchPlanImpl;
+BatchPlanImpl* batch_create(int dtype, const std::vector<GemmProblem>& probs);
+size_t batch_workspace(const BatchPlanImpl* plan);
+// First run measures the candidate k-chunk sizes (autotune) or takes the model
+// choice, then captures the grouped launch in a CUDA graph; later runs replay.
+cudaError_t batch_run(BatchPlanImpl* plan, void* workspace, cudaStream_t stream, bool autotune);
+void batch_destroy(BatchPlanImpl* plan);
+int64_t batch_kc(const BatchPlanImpl* plan);
+const std::vector<double>& batch_tuning(const BatchPlanImpl* plan);
+const std::vector<int64_t>& batch_candidates(const BatchPlanImpl* plan);
 
 // Sum `splits` FP64 partial tiles in order and apply alpha/beta into C.
 cudaError_t reduce_partials(const GemmProblem& prob, const void* partials, int splits, int tile_m,

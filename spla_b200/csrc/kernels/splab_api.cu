@@ -1,6 +1,7 @@
 // splab_* C ABI: argument checks and dispatch to the sm_100a kernels.
 #include <algorithm>
 #include <cstdio>
+#include <vector>
 #include <cstdlib>
 #include <cstring>
 
@@ -201,6 +202,76 @@ int splab_gemm_dmma_noalloc(int dtype, int opA, int opB, int64_t m, int64_t n, i
   const int rc = dmma_gemm_noalloc(p, num_sms(), static_cast<cudaStream_t>(stream));
   if (rc == 2) return SPLAB_ERR_WORKSPACE;
   return rc == 0 ? SPLAB_OK : SPLAB_ERR_LAUNCH;
+}
+
+int splab_batch_create(int dtype, int count, const splab_problem* problems, void** plan,
+                       size_t* workspaceBytes) {
+  if (dtype < 0 || dtype > 3 || count < 1 || !problems || !plan || !workspaceBytes)
+    return SPLAB_ERR_INVALID;
+  std::vector<GemmProblem> probs;
+  probs.reserve(count);
+  for (int i = 0; i < count; ++i) {
+    const splab_problem& q = problems[i];
+    if (q.opA != problems[0].opA || q.opB != problems[0].opB) return SPLAB_ERR_INVALID;
+    if (!valid_problem(dtype, q.opA, q.opB, q.m, q.n, q.k, q.lda, q.ldb, q.ldc))
+      return SPLAB_ERR_INVALID;
+    if (q.m > 0 && q.n > 0 && (!q.C || (q.k > 0 && (!q.A || !q.B)))) return SPLAB_ERR_INVALID;
+    GemmProblem p{};
+    p.dtype = dtype;
+    p.opA = q.opA;
+    p.opB = q.opB;
+    p.m = q.m;
+    p.n = q.n;
+    p.k = q.k;
+    p.A = q.A;
+    p.lda = q.lda;
+    p.B = q.B;
+    p.ldb = q.ldb;
+    p.C = q.C;
+    p.ldc = q.ldc;
+    const bool cplx = dtype_is_complex(dtype);
+    p.alpha[0] = q.alpha[0];
+    p.alpha[1] = cplx ? q.alpha[1] : 0.0;
+    p.beta[0] = q.beta[0];
+    p.beta[1] = cplx ? q.beta[1] : 0.0;
+    if (p.m > 0 && p.n > 0) probs.push_back(p);
+  }
+  if (probs.empty()) return SPLAB_ERR_INVALID;
+  BatchPlanImpl* b = batch_create(dtype, probs);
+  *plan = b;
+  *workspaceBytes = batch_workspace(b);
+  return SPLAB_OK;
+}
+
+int splab_batch_run(void* plan, void* workspace, size_t workspaceBytes, int autotune,
+                    void* stream) {
+  if (!plan) return SPLAB_ERR_INVALID;
+  BatchPlanImpl* b = static_cast<BatchPlanImpl*>(plan);
+  if (!workspace || workspaceBytes < batch_workspace(b)) return SPLAB_ERR_WORKSPACE;
+  return batch_run(b, workspace, static_cast<cudaStream_t>(stream), autotune != 0) == cudaSuccess
+             ? SPLAB_OK
+             : SPLAB_ERR_LAUNCH;
+}
+
+int splab_batch_info(void* plan, int64_t* kChunk, int* nCandidates, int64_t* candidates,
+                     double* tuningMs) {
+  if (!plan) return SPLAB_ERR_INVALID;
+  const BatchPlanImpl* b = static_cast<const BatchPlanImpl*>(plan);
+  if (kChunk) *kChunk = batch_kc(b);
+  const auto& c = batch_candidates(b);
+  const auto& t = batch_tuning(b);
+  const int nc = int(std::min<size_t>(c.size(), 32));
+  if (nCandidates) *nCandidates = nc;
+  for (int i = 0; i < nc; ++i) {
+    if (candidates) candidates[i] = c[i];
+    if (tuningMs) tuningMs[i] = i < int(t.size()) ? t[i] : -1.0;
+  }
+  return SPLAB_OK;
+}
+
+int splab_batch_destroy(void* plan) {
+  batch_destroy(static_cast<BatchPlanImpl*>(plan));
+  return SPLAB_OK;
 }
 
 int splab_set_phase_events(void** events, int count) {
