@@ -668,7 +668,10 @@ struct BatchPlanImpl {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   void* graph_ws = nullptr;
-  cudaStream_t graph_stream = nullptr;
+  // private stream the graph is captured on and replayed on (the caller's
+  // stream may be the legacy default stream, which cannot be captured)
+  cudaStream_t own = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
 };
 
 namespace {
@@ -833,27 +836,37 @@ cudaError_t batch_run_cfg(BatchPlanImpl& b, char* ws, cudaStream_t st, bool auto
     if ((e = batch_tables<Cfg>(b, b.kc, ws, st)) != cudaSuccess) return e;
     b.tuned = true;
   }
-  // capture once per (workspace, stream), then replay
-  if (!b.exec || b.graph_ws != ws || b.graph_stream != st) {
+  // capture once per workspace on the plan's own stream, then replay there,
+  // ordered after / before the caller's stream with events
+  if (!b.own) {
+    if ((e = cudaStreamCreateWithFlags(&b.own, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&b.ev_in, cudaEventDisableTiming)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&b.ev_out, cudaEventDisableTiming)) != cudaSuccess) return e;
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;  // tables uploaded on st
+  if (!b.exec || b.graph_ws != ws) {
     if (b.exec) cudaGraphExecDestroy(b.exec);
     if (b.graph) cudaGraphDestroy(b.graph);
     b.exec = nullptr;
     b.graph = nullptr;
-    if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    if ((e = cudaStreamBeginCapture(b.own, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
       return e;
-    cudaError_t e1 = batch_launch_gemm<Cfg>(b, ws, st);
-    cudaError_t e2 = batch_launch_reduce<Cfg>(b, ws, st);
+    cudaError_t e1 = batch_launch_gemm<Cfg>(b, ws, b.own);
+    cudaError_t e2 = batch_launch_reduce<Cfg>(b, ws, b.own);
     cudaGraph_t g = nullptr;
-    e = cudaStreamEndCapture(st, &g);
+    e = cudaStreamEndCapture(b.own, &g);
     if (e1 != cudaSuccess) return e1;
     if (e2 != cudaSuccess) return e2;
     if (e != cudaSuccess) return e;
     b.graph = g;
     if ((e = cudaGraphInstantiate(&b.exec, g, 0)) != cudaSuccess) return e;
     b.graph_ws = ws;
-    b.graph_stream = st;
   }
-  return cudaGraphLaunch(b.exec, st);
+  if ((e = cudaEventRecord(b.ev_in, st)) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(b.own, b.ev_in, 0)) != cudaSuccess) return e;
+  if ((e = cudaGraphLaunch(b.exec, b.own)) != cudaSuccess) return e;
+  if ((e = cudaEventRecord(b.ev_out, b.own)) != cudaSuccess) return e;
+  return cudaStreamWaitEvent(st, b.ev_out, 0);
 }
 
 template <class F>
@@ -891,8 +904,12 @@ cudaError_t batch_run(BatchPlanImpl* b, void* ws, cudaStream_t st, bool autotune
 
 void batch_destroy(BatchPlanImpl* b) {
   if (!b) return;
+  if (b->own) cudaStreamSynchronize(b->own);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->ev_in) cudaEventDestroy(b->ev_in);
+  if (b->ev_out) cudaEventDestroy(b->ev_out);
+  if (b->own) cudaStreamDestroy(b->own);
   delete b;
 }
 
