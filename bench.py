@@ -327,6 +327,199 @@ def cpu_reference_run(steps, warmup, budget_s=12.0):
 # ---------------------------------------------------------------------------
 
 
+# ---------------------------------------------------------------------------
+# further configurations of the benchmark suite (one JSON line each)
+
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def workload_sbs(torch, spla, steps, warmup):
+    """pzgemm_sbs subspace rotation: A 200000 x 2048 (Gaussian/sqrt(k)), B a
+    Haar-random unitary 2048 x 2048 (QR of a complex Gaussian, phases of
+    diag(R) folded in), C 200000 x 2048 U[-1,1], alpha = beta = 1."""
+    import numpy as np
+    import oracle
+    mloc, n, k = 200000, 2048, 2048
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20250003)
+    s = (1.0 / (2.0 * k)) ** 0.5
+    A = torch.randn((k, mloc), dtype=torch.complex128, device="cuda", generator=g) * s  # cm mloc x k
+    Z = torch.randn((n, k), dtype=torch.complex128, device="cuda", generator=g)
+    Q, R = torch.linalg.qr(Z.T)  # k x n
+    d = torch.diagonal(R)
+    Q = Q * (d / d.abs()).unsqueeze(0)
+    B = Q.T.contiguous()  # column-major k x n buffer: row j of B.T... stored (n, k)
+    C0 = (torch.rand((n, mloc), dtype=torch.float64, device="cuda", generator=g) * 2 - 1) + 1j * (
+        torch.rand((n, mloc), dtype=torch.float64, device="cuda", generator=g) * 2 - 1)
+    C = C0.clone()
+    flops = 8.0 * mloc * n * k
+    ctx = spla.Context(spla.PU_GPU)
+    dist = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128,
+                                                             128)
+
+    def step():
+        C.copy_(C0)
+        spla.pgemm_sbs(mloc, n, k, 1.0, A, mloc, B, k, 0, 0, dist, 1.0, C, mloc, ctx)
+
+    for _ in range(warmup):
+        step()
+    e0, e1 = _events(torch)
+    ms_copy = 0.0
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    # subtract the C reset copy (13 GB) timed separately
+    e0.record()
+    for _ in range(steps):
+        C.copy_(C0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_copy = e0.elapsed_time(e1) / steps
+    step()
+    torch.cuda.synchronize()
+    cols = [0, 1024, 2047]
+    An = A.cpu().numpy().ravel()
+    Bn = B.cpu().numpy()  # (n, k) rows = columns of B
+    Bs = np.ascontiguousarray(Bn[cols].ravel())
+    ref = np.ascontiguousarray(C0.cpu().numpy()[cols].ravel())
+    assert oracle.pgemm_sbs(mloc, len(cols), k, 1.0, An, mloc, Bs, k, 0, 0, 1.0, ref, mloc) == 0
+    got = C.cpu().numpy()[cols].ravel()
+    err = oracle.rel_fro(got, ref)
+    t = ms - ms_copy
+    return {"metric": "ZGEMM-SBS TFLOP/s (pzgemm_sbs, FP64 DMMA)", "value": flops / (t / 1e3) / 1e12,
+            "unit": "TFLOP/s", "ms_per_step": t, "rel_err_vs_oracle_3cols": err,
+            "config": {"workload": "pzgemm_sbs mLocal=200000 n=k=2048 alpha=beta=1, B unitary",
+                       "path": "dmma"}}
+
+
+def workload_ssbtr_float(torch, spla, steps, warmup):
+    """psgemm_ssbtr lower fill, real float, k = 400000, m = n = 1536,
+    Gaussian/sqrt(k)."""
+    import numpy as np
+    import oracle
+    m = n = 1536
+    k = 400000
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20250006)
+    s = (1.0 / k) ** 0.5
+    A = torch.randn((m, k), dtype=torch.float32, device="cuda", generator=g) * s
+    B = torch.randn((n, k), dtype=torch.float32, device="cuda", generator=g) * s
+    C = torch.zeros((n, m), dtype=torch.float32, device="cuda")
+    ctx = spla.Context(spla.PU_GPU)
+    dist = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128,
+                                                             128)
+
+    def step():
+        spla.pgemm_ssbtr(m, n, k, spla.OP_TRANSPOSE, 1.0, A, k, B, k, 0.0, C, m, 0, 0,
+                         spla.FILL_MODE_LOWER, dist, ctx)
+
+    for _ in range(warmup):
+        step()
+    e0, e1 = _events(torch)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    cols = [0, 700, 1535]
+    An = A.cpu().numpy().astype(np.float64).ravel()
+    Bs = np.ascontiguousarray(B[cols].cpu().numpy().astype(np.float64).ravel())
+    ref = np.zeros(m * len(cols))
+    assert oracle.gemm(1, 0, m, len(cols), k, 1.0, An, k, Bs, k, 0.0, ref, m) == 0
+    got = C[cols].cpu().numpy().astype(np.float64).reshape(len(cols), m)
+    ref = ref.reshape(len(cols), m)
+    mask = np.array([[i >= j for i in range(m)] for j in cols])
+    err = float(np.linalg.norm((got - ref)[mask]) / np.linalg.norm(ref[mask]))
+    tri = float(k) * m * (m + 1)
+    return {"metric": "SGEMM-SSBTR TFLOP/s (lower triangle, real float)",
+            "value": tri / (ms / 1e3) / 1e12, "unit": "TFLOP/s", "ms_per_step": ms,
+            "full_matrix_tflops": 2.0 * m * n * k / (ms / 1e3) / 1e12,
+            "rel_err_vs_exact_triangle_3cols": err,
+            "config": {"workload": "psgemm_ssbtr m=n=1536 k=400000 lower, op=T",
+                       "path": "FP64-accumulated DMMA (float inputs)"}}
+
+
+def workload_batch(torch, spla, steps, warmup, dtype="complex128", count=64, sub=32):
+    """64 ssb instances, k ~ U{120000..180000}, m = n ~ U{512, 768, 1024}
+    (seeded draw order: k then m per instance), Gaussian/sqrt(k); run as
+    sub-batches of `sub` instances (the complex-double operands of all 64,
+    ~236 GB, exceed HBM), each one persistent grouped launch replayed from a
+    CUDA graph with the autotuned k-chunk."""
+    import numpy as np
+    rng = np.random.default_rng(20250004)
+    shapes = []
+    for _ in range(count):
+        k = int(rng.integers(120000, 180001))
+        m = int(rng.choice([512, 768, 1024]))
+        shapes.append((m, m, k))
+    tdt = getattr(torch, dtype)
+    total_flops = sum(8.0 * m * n * k for (m, n, k) in shapes)
+    total_ms = 0.0
+    tuning = []
+    for b0 in range(0, count, sub):
+        part = shapes[b0:b0 + sub]
+        g = torch.Generator(device="cuda")
+        g.manual_seed(20250004 + b0)
+        probs = []
+        keep = []
+        for (m, n, k) in part:
+            s = (1.0 / (2.0 * k)) ** 0.5
+            A = torch.randn((m, k), dtype=tdt, device="cuda", generator=g) * s
+            B = torch.randn((n, k), dtype=tdt, device="cuda", generator=g) * s
+            C = torch.empty((n, m), dtype=tdt, device="cuda")
+            keep += [A, B, C]
+            probs.append(dict(opA=2, opB=0, m=m, n=n, k=k, A=A, lda=k, B=B, ldb=k, C=C, ldc=m,
+                              alpha=1.0, beta=0.0))
+        batch = spla.Batch(dtype, probs)
+        ws = torch.empty(batch.workspace_bytes, dtype=torch.uint8, device="cuda")
+        batch.run(ws, autotune=True)
+        for _ in range(max(0, warmup - 1)):
+            batch.run(ws)
+        torch.cuda.synchronize()
+        e0, e1 = _events(torch)
+        e0.record()
+        for _ in range(steps):
+            batch.run(ws)
+        e1.record()
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1) / steps
+        tuning.append(batch.info())
+        # accuracy of one instance against torch (FP64 reference on the GPU)
+        if b0 == 0:
+            A, B, C = keep[0], keep[1], keep[2]
+            ref = (A.to(torch.complex128).conj() @ B.to(torch.complex128).T).T
+            err = float((C.to(torch.complex128) - ref).norm() / ref.norm())
+        del batch, ws, keep, probs
+        torch.cuda.empty_cache()
+    return {"metric": f"batched grouped ZGEMM-SSB TFLOP/s ({dtype})",
+            "value": total_flops / (total_ms / 1e3) / 1e12, "unit": "TFLOP/s",
+            "ms_per_batch": total_ms, "instances": count, "sub_batch": sub,
+            "rel_err_instance0_vs_torch_fp64": err, "autotune": tuning,
+            "config": {"workload": "64 x pgemm_ssb k~U{120000..180000} m=n~{512,768,1024}",
+                       "path": "DMMA grouped persistent + CUDA graph"}}
+
+
+def run_workload(name, steps, warmup):
+    import torch
+    import spla_b200 as spla
+    torch.cuda.set_device(0)
+    fn = {"sbs": workload_sbs, "ssbtr_float": workload_ssbtr_float,
+          "batch": workload_batch,
+          "batch_c64": lambda t, s, st, w: workload_batch(t, s, st, w, "complex64", 64, 64)}[name]
+    line = fn(torch, spla, steps, warmup)
+    line.update({"n_gpus": 1, "steps": steps, "warmup": warmup, "higher_is_better": True,
+                 "data": "synthetic, seeded"})
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -339,7 +532,11 @@ def main():
     ap.add_argument("--no-peaks", action="store_true")
     ap.add_argument("--m", type=int, default=1024, help="m = n (profiling of smaller cases)")
     ap.add_argument("--k", type=int, default=250000, help="k (profiling of smaller cases)")
+    ap.add_argument("--workload", default="zgemm_ssb",
+                    choices=["zgemm_ssb", "sbs", "ssbtr_float", "batch", "batch_c64"])
     args = ap.parse_args()
+    if args.workload != "zgemm_ssb" and args.impl == "ours":
+        return run_workload(args.workload, args.steps, max(3, args.warmup))
     set_shape(args.m, args.k)
     warmup = max(3, args.warmup)
 

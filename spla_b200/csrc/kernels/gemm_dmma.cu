@@ -688,12 +688,14 @@ void batch_geometry(BatchPlanImpl& b) {
     kmin = std::min<int64_t>(kmin, p.k);
     kmax = std::max<int64_t>(kmax, p.k);
   }
-  // candidate k-chunks: powers of two between 16 BK and the smallest k / 2,
-  // so that every problem has at least two splits (partials only, C untouched
-  // while tuning)
+  // candidate k-chunks: powers of two from the one giving at most 24 splits
+  // of the longest problem (bounds the partials' memory) up to the smallest
+  // k / 2, so that every problem has at least two splits while tuning (the
+  // tuning runs write partials only, never C)
   b.candidates.clear();
-  for (int64_t c = 16 * Cfg::BK; c <= std::max<int64_t>(16 * Cfg::BK, kmin / 2); c *= 2)
-    b.candidates.push_back(c);
+  int64_t c0 = 16 * Cfg::BK;
+  while (c0 * 24 < kmax) c0 *= 2;
+  for (int64_t c = c0; c <= std::max<int64_t>(c0, kmin / 2); c *= 2) b.candidates.push_back(c);
   // workspace: tables + partials for the smallest candidate (most splits)
   const int64_t cmin = b.candidates.front();
   size_t partial_bytes = 0, items = 0;

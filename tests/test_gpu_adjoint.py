@@ -9,9 +9,11 @@ Checks:
   * central finite differences, h = 1e-6, on 16 random unit-norm directions
     and 32 single coordinates (stepped along the gradient component, so real
     and imaginary parts both enter) per operand agree with Re<grad, dX> to
-    <= 1e-6 relative, dX = (X + hV) - (X - hV) as evaluated. The loss is evaluated as
-    m + sum|C|^2 - 2 Re tr C with an exactly rounded host sum (math.fsum), so
-    the O(m) constant cancels exactly between L(+h) and L(-h);
+    <= 1e-6 relative (dX = (X + hV) - (X - hV) as evaluated), the difference
+    quotient being evaluated in the cancellation-free form of the quadratic
+    loss (see _fd_check); the plain two-evaluation difference, whose accuracy
+    at h = 1e-6 is bounded by the FP64 rounding of the forwards, agrees to
+    <= 2e-3;
   * the Ozaki path's gradient equals the FP64 DMMA path's.
 """
 import math
@@ -73,15 +75,23 @@ def test_gradient_matches_torch_autograd(setup):
 
 
 def _fd_check(torch, spla, A, B, ctx, which, gA, gB):
-    """Central differences L(X + hV) - L(X - hV) against Re<grad, X+ - X->,
-    X+ and X- being the rounded perturbed inputs actually evaluated (for a
-    random unit direction a per-element step h|V_e| ~ 1e-10 is far below the
-    ulp-relative precision of X, so the realised step is what is measured)."""
+    """Central differences at h = 1e-6 along V, compared with Re<grad, dX>,
+    dX = X+ - X- the realised step (X+- = X +- hV as rounded).
+
+    For the quadratic loss, L(X+) - L(X-) = Re<C+ + C- - 2I, C+ - C->
+    exactly, and C+ - C- = forward(dX) by linearity. Two estimates:
+      stable: that identity with three forward evaluations - no cancellation;
+      raw:    L(X+) - L(X-) from two forward evaluations and exact host sums.
+    At h = 1e-6 the raw form is limited by the FP64 rounding of the two
+    forwards (~1e-5 relative here; the same holds for torch.matmul through
+    cuBLAS, which gives the identical value). Returns the worst relative
+    discrepancy of each estimate."""
     from spla_b200.autograd import ssb
     rng = np.random.default_rng(17 if which == "A" else 18)
     X = A if which == "A" else B
     grad = gA if which == "A" else gB
-    worst = 0.0
+    eye = torch.eye(M, N, dtype=X.dtype, device=X.device)
+    worst_stable = worst_raw = 0.0
     dirs = []
     for _ in range(16):
         V = torch.from_numpy(rng.standard_normal(X.shape) + 1j * rng.standard_normal(X.shape)).to(
@@ -93,30 +103,29 @@ def _fd_check(torch, spla, A, B, ctx, which, gA, gB):
         gi = complex(grad[idx].item())
         V[idx] = gi / abs(gi)  # unit step along the gradient component: real and imaginary parts
         dirs.append(V)
+
+    def fwd(Xv):
+        return ssb(Xv, B, ctx) if which == "A" else ssb(A, Xv, ctx)
+
     for V in dirs:
         Xp, Xm = X + H * V, X - H * V
-        if which == "A":
-            Lp, Lm = loss_exact(ssb(Xp, B, ctx)), loss_exact(ssb(Xm, B, ctx))
-        else:
-            Lp, Lm = loss_exact(ssb(A, Xp, ctx)), loss_exact(ssb(A, Xm, ctx))
-        fd = Lp - Lm
-        an = float((grad.conj() * (Xp - Xm)).sum().real)
-        worst = max(worst, abs(fd - an) / abs(an))
-    return worst
+        dX = Xp - Xm
+        Cp, Cm, dC = fwd(Xp), fwd(Xm), fwd(dX)
+        an = float((grad.conj() * dX).sum().real)
+        stable = float(((Cp + Cm - 2 * eye).conj() * dC).sum().real)
+        raw = loss_exact(Cp) - loss_exact(Cm)
+        worst_stable = max(worst_stable, abs(stable - an) / abs(an))
+        worst_raw = max(worst_raw, abs(raw - an) / abs(an))
+    return worst_stable, worst_raw
 
 
-def test_finite_differences_A(setup):
+@pytest.mark.parametrize("which", ["A", "B"])
+def test_finite_differences(setup, which):
     torch, spla, A, B, ctx = setup
     gA, gB = grads(torch, spla, A, B, ctx)
-    worst = _fd_check(torch, spla, A, B, ctx, "A", gA, gB)
-    assert worst <= 1e-6, worst
-
-
-def test_finite_differences_B(setup):
-    torch, spla, A, B, ctx = setup
-    gA, gB = grads(torch, spla, A, B, ctx)
-    worst = _fd_check(torch, spla, A, B, ctx, "B", gA, gB)
-    assert worst <= 1e-6, worst
+    stable, raw = _fd_check(torch, spla, A, B, ctx, which, gA, gB)
+    assert stable <= 1e-6, stable
+    assert raw <= 2e-3, raw
 
 
 def test_ozaki_forward_gradient_matches_dmma(setup):
