@@ -50,6 +50,12 @@ extern "C" {
 
 SPLAB_API const char *splab_status_string(int status);
 
+/* The concrete path (SPLAB_PATH_DMMA or SPLAB_PATH_OZAKI) `path` resolves to
+ * for this problem; SPLAB_PATH_AUTO looks at the shape and the free device
+ * memory, so resolve once and pass the result to the calls below. */
+SPLAB_API int splab_gemm_path(int dtype, int path, int opA, int opB, int64_t m, int64_t n,
+                              int64_t k);
+
 /* Bytes of device scratch splab_gemm needs for this problem (0 if none);
  * ozakiModuli as for splab_gemm. */
 SPLAB_API size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t m,

@@ -88,6 +88,8 @@ def _declare(L):
                              i64, i, vp, sz, vp]
     L.splab_gemm.restype = i
     L.splab_gemm_workspace_size.argtypes = [i, i, i, i, i64, i64, i64, i]
+    L.splab_gemm_path.argtypes = [i, i, i, i, i64, i64, i64]
+    L.splab_gemm_path.restype = i
     L.splab_gemm_check.argtypes = [i, i, i, i, i64, i64, i64, i, vp, vp]
     L.splab_gemm_check.restype = i
     L.splab_set_phase_events.argtypes = [vp, i]

@@ -98,7 +98,7 @@ void local_gemm(ContextInternal& ctx, SplaOperation opA, SplaOperation opB, int 
   if (lda < 1) lda = 1;
   if (ldb < 1) ldb = 1;
   if (ldc < m) throw InvalidParameterError();  // the reference hands this to BLAS unchecked
-  const int path = path_for(ctx, dtype);
+  const int path_pref = path_for(ctx, dtype);
   const int moduli = ctx.ozaki_moduli();
   cudaStream_t cs = ctx.compute_stream();
 
@@ -119,6 +119,7 @@ void local_gemm(ContextInternal& ctx, SplaOperation opA, SplaOperation opB, int 
   }
 
   if (devA && devB) {
+    const int path = splab_gemm_path(dtype, path_pref, opA, opB, m, n, k);
     const size_t ws = splab_gemm_workspace_size(dtype, path, opA, opB, m, n, k, moduli);
     void* w = ws ? ctx.device_pool().get(1, ws) : nullptr;
     check_splab(splab_gemm(dtype, path, opA, opB, m, n, k, &alpha, A, lda, B, ldb, &beta, dC,
@@ -144,6 +145,7 @@ void local_gemm(ContextInternal& ctx, SplaOperation opA, SplaOperation opB, int 
       if (!devB) bufB[b] = static_cast<T*>(ctx.device_pool().get(4 + b, bbytes));
     }
     const int64_t klast = k - (chunks - 1) * kc;
+    const int path = splab_gemm_path(dtype, path_pref, opA, opB, m, n, kc);
     const size_t ws =
         std::max(splab_gemm_workspace_size(dtype, path, opA, opB, m, n, kc, moduli),
                  splab_gemm_workspace_size(dtype, path, opA, opB, m, n, klast, moduli));

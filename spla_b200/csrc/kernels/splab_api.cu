@@ -74,16 +74,22 @@ GemmProblem make_problem(int dtype, int opA, int opB, int64_t m, int64_t n, int6
   return p;
 }
 
-constexpr bool kAutoUsesOzaki = false;
-
-// Ozaki when requested (or, for AUTO, when the problem is a large ssb-shaped
-// FP64 contraction) and the path supports the layout; DMMA otherwise.
+// Ozaki when requested, or, for AUTO, when the problem is a large ssb-shaped
+// FP64 contraction (where it measured faster than the FP64 tensor cores) whose
+// residue workspace is at most a quarter of the free device memory; DMMA
+// otherwise and whenever the layout is not supported.
 bool use_ozaki(const GemmProblem& p, int path) {
   if (!ozaki_supported(p)) return false;
   if (path == SPLAB_PATH_OZAKI) return true;
   if (path == SPLAB_PATH_DMMA) return false;
   const double flops = double(p.m) * p.n * p.k * (p.dtype == kC64 ? 8.0 : 2.0);
-  return kAutoUsesOzaki && p.m >= 256 && p.n >= 128 && p.k >= 8192 && flops >= 2e12;
+  if (!(p.m >= 256 && p.n >= 128 && p.k >= 8192 && flops >= 1e13)) return false;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return ozaki_workspace_bytes(p, 0) <= free_b / 4;
 }
 
 __global__ void block_cyclic_info_kernel(int64_t rb, int64_t cb, int64_t gr, int64_t gc,
@@ -128,6 +134,18 @@ const char* splab_status_string(int status) {
     case SPLAB_ERR_TIMEOUT: return "bounded device wait timed out";
     default: return "unknown status";
   }
+}
+
+int splab_gemm_path(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int64_t k) {
+  GemmProblem p{};
+  p.dtype = dtype;
+  p.opA = opA;
+  p.opB = opB;
+  p.m = m;
+  p.n = n;
+  p.k = k;
+  if (dtype < 0 || dtype > 3 || m <= 0 || n <= 0 || k < 0) return SPLAB_PATH_DMMA;
+  return use_ozaki(p, path) ? SPLAB_PATH_OZAKI : SPLAB_PATH_DMMA;
 }
 
 size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t m, int64_t n,

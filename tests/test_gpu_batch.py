@@ -35,7 +35,7 @@ def test_batch_matches_oracle(dt, tol, autotune):
     import torch
     import spla_b200 as spla
     shapes = [(130, 70, 9000), (64, 256, 4000), (200, 200, 12345), (17, 300, 2048),
-              (256, 128, 30000), (96, 96, 777)]
+              (256, 128, 30000), (96, 96, 777), (40, 40, 70000)]
     probs, host = _problems(torch, dt, shapes, 100)
     batch = spla.Batch(np.dtype(dt).name, probs)
     ws = torch.empty(batch.workspace_bytes, dtype=torch.uint8, device="cuda")
@@ -43,7 +43,7 @@ def test_batch_matches_oracle(dt, tol, autotune):
     torch.cuda.synchronize()
     info = batch.info()
     assert info["k_chunk"] in info["candidates"]
-    if autotune:
+    if autotune and len(info["candidates"]) > 1:
         assert all(t > 0 for t in info["tuning_ms"])
     for p, (A, B, C, alpha, beta) in zip(probs, host):
         ref = C.copy()
