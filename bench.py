@@ -53,6 +53,19 @@ def set_shape(m, k):
 OZAKI_MODULI = 15  # default modulus count of the library (<= 1e-14 at this k)
 
 
+def max_over_ranks(torch, ms, device):
+    """The step time of the slowest rank (all ranks take part in the reduction)."""
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if torch.distributed.is_initialized() and torch.distributed.get_world_size() > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_tflops(flops_per_rank, world, ms_max):
+    """Replicas: every rank did flops_per_rank in the slowest rank's time."""
+    return flops_per_rank * world / (ms_max / 1e3) / 1e12
+
+
 def cpu_env():
     """Thread count and an explicit OpenBLAS core type (must precede loading BLAS)."""
     n = os.cpu_count() or 1
@@ -582,33 +595,32 @@ def main():
             except RuntimeError as ex:
                 results[pname] = {"error": str(ex)}
                 continue
-            t = torch.tensor([ms], device=device)
-            if world > 1:
-                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
-            results[pname] = {"ms_per_step": ms, "tflops": FLOPS * world / (ms / 1e3) / 1e12,
+            ms = max_over_ranks(torch, ms, device)
+            results[pname] = {"ms_per_step": ms, "tflops": whole_job_tflops(FLOPS, world, ms),
                               "phase_ms": phases, "dC": dC}
     clocks = clk.summary()
     for pname, r in results.items():
         if "dC" in r:
             r["rel_err_vs_oracle"] = rel_err_sampled(r.pop("dC"), A, B) if rank == 0 else None
 
-    # headline: Ozaki if it ran and met the accuracy bar, else DMMA
+    # headline: Ozaki if it ran and met the accuracy bar (checked on rank 0 and
+    # broadcast, so that every rank takes the same steps), else DMMA
     head = "dmma"
     oz = results.get("ozaki", {})
     if "tflops" in oz and oz.get("rel_err_vs_oracle") is not None and oz["rel_err_vs_oracle"] <= 1e-14:
         head = "ozaki"
+    if world > 1:
+        flag = torch.tensor([1 if head == "ozaki" else 0], device=device)
+        torch.distributed.broadcast(flag, 0)
+        head = "ozaki" if int(flag.item()) else "dmma"
     hr = results[head]
     head_path = names[head]
 
     e2e = None
     if not args.no_e2e:
         ms_e2e, _ = e2e_public_api(torch, spla, head_path, A, B, max(1, min(args.steps, 3)), 1)
-        t = torch.tensor([ms_e2e], device=device)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-        e2e = {"value": FLOPS * world / (ms_e2e / 1e3) / 1e12, "unit": "TFLOP/s",
+        ms_e2e = max_over_ranks(torch, ms_e2e, device)
+        e2e = {"value": whole_job_tflops(FLOPS, world, ms_e2e), "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(16 * K * (M + N)), "d2h_bytes_per_step": int(16 * M * N),
                "ms_per_step": ms_e2e, "operands": "pinned host memory, streamed in k-chunks"}
 
