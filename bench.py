@@ -411,7 +411,7 @@ def workload_sbs(torch, spla, steps, warmup):
                        "path": "dmma"}}
 
 
-def workload_ssbtr_float(torch, spla, steps, warmup):
+def workload_ssbtr_float(torch, spla, steps, warmup, path=None):
     """psgemm_ssbtr lower fill, real float, k = 400000, m = n = 1536,
     Gaussian/sqrt(k)."""
     import numpy as np
@@ -425,6 +425,8 @@ def workload_ssbtr_float(torch, spla, steps, warmup):
     B = torch.randn((n, k), dtype=torch.float32, device="cuda", generator=g) * s
     C = torch.zeros((n, m), dtype=torch.float32, device="cuda")
     ctx = spla.Context(spla.PU_GPU)
+    if path is not None:
+        ctx.set_fp64_path(path)
     dist = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128,
                                                              128)
 
@@ -457,7 +459,7 @@ def workload_ssbtr_float(torch, spla, steps, warmup):
             "full_matrix_tflops": 2.0 * m * n * k / (ms / 1e3) / 1e12,
             "rel_err_vs_exact_triangle_3cols": err,
             "config": {"workload": "psgemm_ssbtr m=n=1536 k=400000 lower, op=T",
-                       "path": "FP64-accumulated DMMA (float inputs)"}}
+                       "path": {None: "auto", 1: "FP64-accumulated DMMA", 2: "Ozaki INT8"}[path]}}
 
 
 def workload_batch(torch, spla, steps, warmup, dtype="complex128", count=64, sub=32):
@@ -525,6 +527,8 @@ def run_workload(name, steps, warmup):
     import spla_b200 as spla
     torch.cuda.set_device(0)
     fn = {"sbs": workload_sbs, "ssbtr_float": workload_ssbtr_float,
+          "ssbtr_float_dmma": lambda t, s, st, w: workload_ssbtr_float(t, s, st, w, 1),
+          "ssbtr_float_ozaki": lambda t, s, st, w: workload_ssbtr_float(t, s, st, w, 2),
           "batch": workload_batch,
           "batch_c64": lambda t, s, st, w: workload_batch(t, s, st, w, "complex64", 64, 64)}[name]
     line = fn(torch, spla, steps, warmup)
@@ -546,7 +550,8 @@ def main():
     ap.add_argument("--m", type=int, default=1024, help="m = n (profiling of smaller cases)")
     ap.add_argument("--k", type=int, default=250000, help="k (profiling of smaller cases)")
     ap.add_argument("--workload", default="zgemm_ssb",
-                    choices=["zgemm_ssb", "sbs", "ssbtr_float", "batch", "batch_c64"])
+                    choices=["zgemm_ssb", "sbs", "ssbtr_float", "ssbtr_float_dmma",
+                             "ssbtr_float_ozaki", "batch", "batch_c64"])
     args = ap.parse_args()
     if args.workload != "zgemm_ssb" and args.impl == "ours":
         return run_workload(args.workload, args.steps, max(3, args.warmup))

@@ -36,9 +36,9 @@ extern "C" {
 #define SPLAB_C64 3
 
 /* Compute paths for the contraction. */
-#define SPLAB_PATH_AUTO 0  /* Ozaki for large double/complex-double ssb shapes, else DMMA */
+#define SPLAB_PATH_AUTO 0  /* Ozaki for large ssb-shaped problems, else DMMA */
 #define SPLAB_PATH_DMMA 1  /* FP64 tensor cores (mma.sync f64); float inputs accumulate in FP64 */
-#define SPLAB_PATH_OZAKI 2 /* Ozaki scheme II on INT8 tcgen05 for double / complex double with
+#define SPLAB_PATH_OZAKI 2 /* Ozaki scheme II on INT8 tcgen05 (all four dtypes) with
                               op(A) in {T, C}, op(B) = N; other problems use DMMA */
 
 #define SPLAB_OK 0
@@ -68,8 +68,9 @@ SPLAB_API size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB
  * (src/pgemm_ssb/pgemm_ssb_gpu.cpp:259-262, opA in {T,C}, opB = N) and
  * pgemm_sbs (src/pgemm_sbs/pgemm_sbs_gpu.cpp:246-249, N,N) reduce to, plus the
  * fill-mode tile skipping of pgemm_ssbtr (src/block_generation/block.hpp:58-66).
- * ozakiModuli: number of CRT moduli for SPLAB_PATH_OZAKI (0 = default, 15, for
- * <= 1e-14 relative error; 8..16); ignored otherwise. A bounded device wait
+ * ozakiModuli: number of CRT moduli for SPLAB_PATH_OZAKI (0 = default: 15 for
+ * double, <= 1e-14 relative error; 9 for float, ~1e-8; range 8..16); ignored
+ * otherwise. A bounded device wait
  * that gives up makes the next splab_gemm_check() return SPLAB_ERR_TIMEOUT.
  */
 SPLAB_API int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int64_t k,

@@ -61,10 +61,7 @@ struct DeviceGuard {
   ~DeviceGuard() { cudaSetDevice(prev); }
 };
 
-int path_for(const ContextInternal& ctx, int dtype) {
-  if (dtype == SPLAB_R64 || dtype == SPLAB_C64) return ctx.fp64_path();
-  return SPLAB_PATH_DMMA;
-}
+int path_for(const ContextInternal& ctx, int) { return ctx.fp64_path(); }
 
 // Copy the k-range [k0, k0 + kc) of an operand into a dense device buffer.
 // `kmajor` operands have k as their contiguous (row) dimension: element

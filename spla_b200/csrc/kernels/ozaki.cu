@@ -184,13 +184,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 
 // One block per row: sigma = Q - e where ||row||_2 = f 2^e, f in [0.5, 1).
 // Rows of zeros get sigma = 0.
-__global__ void oz_row_scale(const double* __restrict__ X, int64_t ld_doubles, int64_t len,
-                             int rows, int q_bits, int* __restrict__ sigma) {
+template <typename TIn>
+__global__ void oz_row_scale(const TIn* __restrict__ X, int64_t ld_elems, int64_t len, int rows,
+                             int q_bits, int* __restrict__ sigma) {
   const int row = blockIdx.x;
   if (row >= rows) return;
-  const double* x = X + int64_t(row) * ld_doubles;
+  const TIn* x = X + int64_t(row) * ld_elems;
   double s = 0.0;
-  for (int64_t l = threadIdx.x; l < len; l += blockDim.x) s = fma(x[l], x[l], s);
+  for (int64_t l = threadIdx.x; l < len; l += blockDim.x) {
+    const double v = double(x[l]);
+    s = fma(v, v, s);
+  }
   __shared__ double red[32];
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -225,17 +229,19 @@ struct SliceConsts {
 // [-(p-1)/2, (p-1)/2] for odd p. For p = 256 the weights vanish and r is the
 // low byte of d_0. Each residue is produced as the float MAGIC + r, whose low
 // byte is r in two's complement: the int8 value without a conversion.
+template <int NDIG>
 __device__ __forceinline__ void digits13(double x, float (&d)[5]) {
   const double b = 8192.0, ib = 1.0 / 8192.0;
-  double q1 = rint(x * ib);
-  d[0] = float(fma(q1, -b, x));
-  double q2 = rint(q1 * ib);
-  d[1] = float(fma(q2, -b, q1));
-  double q3 = rint(q2 * ib);
-  d[2] = float(fma(q3, -b, q2));
-  double q4 = rint(q3 * ib);
-  d[3] = float(fma(q4, -b, q3));
-  d[4] = float(q4);
+  double q = x;
+#pragma unroll
+  for (int i = 0; i < NDIG - 1; ++i) {
+    const double qn = rint(q * ib);
+    d[i] = float(fma(qn, -b, q));
+    q = qn;
+  }
+  d[NDIG - 1] = float(q);
+#pragma unroll
+  for (int i = NDIG; i < 5; ++i) d[i] = 0.0f;
 }
 
 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: ulp 1, low mantissa bits hold r
@@ -257,8 +263,9 @@ __device__ __forceinline__ uint32_t neg_odd_bytes(uint32_t w) {
 // mode 0: plain rows (A rows, or B rows of a real product): out row = row.
 // mode 1: complex B rows -> u row `row` and v row `row + rows` with sign s:
 //         u = (br, -s*bi), v = (bi, s*br) interleaved.
-template <bool VEC>
-__global__ void __launch_bounds__(256) oz_slice(const double* __restrict__ X, int64_t ld_doubles,
+// TIn: double (|x| < 2^62, five digits) or float (|x| < 2^38, three digits).
+template <typename TIn, bool VEC, int NDIG>
+__global__ void __launch_bounds__(256) oz_slice(const TIn* __restrict__ X, int64_t ld_doubles,
                                                 int64_t len, int rows, int64_t kp,
                                                 const int* __restrict__ sigma, int mode,
                                                 int s_sign, int8_t* __restrict__ res,
@@ -268,28 +275,39 @@ __global__ void __launch_bounds__(256) oz_slice(const double* __restrict__ X, in
   const int row = int(gid / groups);
   if (row >= rows) return;
   const int64_t l0 = (gid % groups) * 16;
-  const double* x = X + int64_t(row) * ld_doubles + l0;
+  const TIn* x = X + int64_t(row) * ld_doubles + l0;
   const int sg = sigma[row];
   // 2^sg as a double when representable, else ldexp per element
   const bool direct = sg > -1000 && sg < 1000;
   const double scale = direct ? __longlong_as_double((long long)(sg + 1023) << 52) : 1.0;
   double v[16];
   if (VEC && l0 + 16 <= len) {
+    if constexpr (sizeof(TIn) == 8) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const double2 t = __ldg(reinterpret_cast<const double2*>(x) + i);
-      v[2 * i] = t.x;
-      v[2 * i + 1] = t.y;
+      for (int i = 0; i < 8; ++i) {
+        const double2 t = __ldg(reinterpret_cast<const double2*>(x) + i);
+        v[2 * i] = t.x;
+        v[2 * i + 1] = t.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(x) + i);
+        v[4 * i] = t.x;
+        v[4 * i + 1] = t.y;
+        v[4 * i + 2] = t.z;
+        v[4 * i + 3] = t.w;
+      }
     }
   } else {
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = (l0 + i < len) ? x[i] : 0.0;
+    for (int i = 0; i < 16; ++i) v[i] = (l0 + i < len) ? double(x[i]) : 0.0;
   }
   float d[16][5];
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     const double xi = rint(direct ? v[i] * scale : ldexp(v[i], sg));
-    digits13(xi, d[i]);
+    digits13<NDIG>(xi, d[i]);
   }
   for (int t = 0; t < sc.n; ++t) {
     float r[16];
@@ -302,9 +320,9 @@ __global__ void __launch_bounds__(256) oz_slice(const double* __restrict__ X, in
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         float s = fmaf(c1, d[i][1], d[i][0]);
-        s = fmaf(c2, d[i][2], s);
-        s = fmaf(c3, d[i][3], s);
-        s = fmaf(c4, d[i][4], s);
+        if (NDIG > 2) s = fmaf(c2, d[i][2], s);
+        if (NDIG > 3) s = fmaf(c3, d[i][3], s);
+        if (NDIG > 4) s = fmaf(c4, d[i][4], s);
         const float q = fmaf(s, ip, kMagic) - kMagic;
         r[i] = fmaf(-q, p, s + kMagic);
       }
@@ -793,12 +811,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 
 // C(i, j) <- alpha * 2^(-sigma_i - tau_j) * X + beta * C(i, j); complex: real
 // part from R row j, imaginary part from R row n + j.
-template <bool CPLX>
+template <int DT>
 __global__ void oz_reconstruct(const int* __restrict__ R, int m, int n, int nb,
                                const int* __restrict__ sigA, const int* __restrict__ sigB,
                                void* C, int64_t ldc, double alr, double ali, double ber,
                                double bei, int fill, int64_t ro, int64_t co, int tile_m, int tile_n,
                                ReconParams rp) {
+  constexpr bool CPLX = dtype_is_complex(DT);
   const int64_t total = int64_t(m) * n;
   for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
        idx += int64_t(gridDim.x) * blockDim.x) {
@@ -827,17 +846,29 @@ __global__ void oz_reconstruct(const int* __restrict__ R, int m, int n, int nb,
     }
     double outr = alr * xr - ali * xi, outi = alr * xi + ali * xr;
     const bool read_c = (ber != 0.0 || bei != 0.0);
-    if (CPLX) {
-      double2* c = static_cast<double2*>(C) + i + int64_t(j) * ldc;
+    const int64_t ci = i + int64_t(j) * ldc;
+    if constexpr (DT == kC64) {
+      double2* c = static_cast<double2*>(C) + ci;
       if (read_c) {
         const double2 old = *c;
         outr += ber * old.x - bei * old.y;
         outi += ber * old.y + bei * old.x;
       }
       *c = make_double2(outr, outi);
-    } else {
-      double* c = static_cast<double*>(C) + i + int64_t(j) * ldc;
+    } else if constexpr (DT == kC32) {
+      float2* c = static_cast<float2*>(C) + ci;
+      if (read_c) {
+        const float2 old = *c;
+        outr += ber * double(old.x) - bei * double(old.y);
+        outi += ber * double(old.y) + bei * double(old.x);
+      }
+      *c = make_float2(float(outr), float(outi));
+    } else if constexpr (DT == kR64) {
+      double* c = static_cast<double*>(C) + ci;
       *c = read_c ? fma(ber, *c, outr) : outr;
+    } else {
+      float* c = static_cast<float*>(C) + ci;
+      *c = float(read_c ? fma(ber, double(*c), outr) : outr);
     }
   }
 }
@@ -856,8 +887,9 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 Layout layout_of(const GemmProblem& p, int moduli) {
   Layout L{};
-  L.nmod = moduli > 0 ? std::min(moduli, kMaxUsableModuli) : kDefaultModuli;
-  const bool cplx = p.dtype == kC64;
+  L.nmod = moduli > 0 ? std::min(moduli, kMaxUsableModuli)
+                      : (dtype_is_double(p.dtype) ? kDefaultModuli : kDefaultModuliFloat);
+  const bool cplx = dtype_is_complex(p.dtype);
   L.K2 = cplx ? 2 * p.k : p.k;
   L.kp = (L.K2 + BKB - 1) / BKB * BKB;
   L.rowsA = int(p.m);
@@ -922,9 +954,72 @@ size_t ozaki_workspace_bytes(const GemmProblem& p, int moduli) {
 }
 
 bool ozaki_supported(const GemmProblem& p) {
-  return (p.dtype == kR64 || p.dtype == kC64) && p.opA != 0 && p.opB == 0 &&
-         p.m <= (1 << 24) && p.n <= (1 << 23);
+  return p.opA != 0 && p.opB == 0 && p.m <= (1 << 24) && p.n <= (1 << 23);
 }
+
+namespace {
+template <typename TIn, bool VEC>
+void launch_slice(int ndig, unsigned grid, cudaStream_t st, const TIn* X, int64_t ld, int64_t len,
+                  int rows, int64_t kp, const int* sig, int mode, int s_sign, int8_t* res,
+                  int64_t stride, const oz::SliceConsts& sc) {
+  using namespace oz;
+  if (ndig <= 3)
+    oz_slice<TIn, VEC, 3><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
+                                                 stride, sc);
+  else if (ndig == 4)
+    oz_slice<TIn, VEC, 4><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
+                                                 stride, sc);
+  else
+    oz_slice<TIn, VEC, 5><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
+                                                 stride, sc);
+}
+
+template <typename TIn>
+void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
+                    int* sigA, int* sigB, int8_t* resA, int8_t* resB, cudaStream_t st) {
+  using namespace oz;
+  const TIn* A = static_cast<const TIn*>(p.A);
+  const TIn* B = static_cast<const TIn*>(p.B);
+  const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in real elements
+  const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
+  oz_row_scale<TIn><<<L.rowsA, 256, 0, st>>>(A, ldA, L.K2, L.rowsA, crt.q_bits, sigA);
+  oz_row_scale<TIn><<<L.rowsB, 256, 0, st>>>(B, ldB, L.K2, L.rowsB, crt.q_bits, sigB);
+  SliceConsts sc{};
+  sc.n = L.nmod;
+  for (int t = 0; t < L.nmod; ++t) {
+    const int pt = crt.p[t];
+    sc.p[t] = float(pt);
+    sc.inv_p[t] = 1.0f / float(pt);
+    long long w = 1;
+    for (int i = 0; i < 4; ++i) {
+      w = (w * 8192) % pt;  // 2^(13 (i+1)) mod p
+      const long long c = w > pt / 2 ? w - pt : w;
+      sc.c[t][i] = float(c);
+    }
+  }
+  // digits of 13 bits covering |x| < 2^(Q+1)
+  const int ndig = crt.q_bits + 1 <= 39 ? 3 : (crt.q_bits + 1 <= 52 ? 4 : 5);
+  const int64_t groups = L.kp / 16;
+  const unsigned gridA = unsigned((int64_t(L.rowsA) * groups + 255) / 256);
+  const unsigned gridB = unsigned((int64_t(L.rowsB) * groups + 255) / 256);
+  const int vec_elems = 16 / int(sizeof(TIn));
+  const bool vecA = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (ldA % vec_elems == 0);
+  const bool vecB = (reinterpret_cast<uintptr_t>(B) % 16 == 0) && (ldB % vec_elems == 0);
+  const int s_sign = p.opA == 2 ? -1 : 1;
+  if (vecA)
+    launch_slice<TIn, true>(ndig, gridA, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA,
+                            int64_t(L.rowsA) * L.kp, sc);
+  else
+    launch_slice<TIn, false>(ndig, gridA, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA,
+                             int64_t(L.rowsA) * L.kp, sc);
+  if (vecB)
+    launch_slice<TIn, true>(ndig, gridB, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0,
+                            s_sign, resB, int64_t(L.nb) * L.kp, sc);
+  else
+    launch_slice<TIn, false>(ndig, gridB, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0,
+                             s_sign, resB, int64_t(L.nb) * L.kp, sc);
+}
+}  // namespace
 
 cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_bytes,
                        cudaStream_t st) {
@@ -934,7 +1029,7 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
   const Layout L = layout_of(p, moduli);
   if (ws_bytes < L.total || !ws) return cudaErrorInvalidValue;
   const Crt crt = make_crt(L.nmod);
-  const bool cplx = p.dtype == kC64;
+  const bool cplx = dtype_is_complex(p.dtype);
   char* w = static_cast<char*>(ws);
   int* sigA = reinterpret_cast<int*>(w + L.off_sigA);
   int* sigB = reinterpret_cast<int*>(w + L.off_sigB);
@@ -942,48 +1037,14 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
   int8_t* resB = reinterpret_cast<int8_t*>(w + L.off_resB);
   int* R = reinterpret_cast<int*>(w + L.off_R);
   int* status = reinterpret_cast<int*>(w + L.off_status);
-  const double* A = static_cast<const double*>(p.A);
-  const double* B = static_cast<const double*>(p.B);
-  const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in doubles
-  const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
 
   cudaError_t e;
   phase_mark(0, false, st);
   if (p.k > 0) {
-    oz_row_scale<<<L.rowsA, 256, 0, st>>>(A, ldA, L.K2, L.rowsA, crt.q_bits, sigA);
-    oz_row_scale<<<L.rowsB, 256, 0, st>>>(B, ldB, L.K2, L.rowsB, crt.q_bits, sigB);
-    SliceConsts sc{};
-    sc.n = L.nmod;
-    for (int t = 0; t < L.nmod; ++t) {
-      const int pt = crt.p[t];
-      sc.p[t] = float(pt);
-      sc.inv_p[t] = 1.0f / float(pt);
-      long long w = 1;
-      for (int i = 0; i < 4; ++i) {
-        w = (w * 8192) % pt;  // 2^(13 (i+1)) mod p
-        const long long c = w > pt / 2 ? w - pt : w;
-        sc.c[t][i] = float(c);
-      }
-    }
-    const int64_t groups = L.kp / 16;
-    const int threads = 256;
-    const unsigned gridA = unsigned((int64_t(L.rowsA) * groups + threads - 1) / threads);
-    const unsigned gridB = unsigned((int64_t(L.rowsB) * groups + threads - 1) / threads);
-    const bool vecA = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (ldA % 2 == 0);
-    const bool vecB = (reinterpret_cast<uintptr_t>(B) % 16 == 0) && (ldB % 2 == 0);
-    const int s_sign = p.opA == 2 ? -1 : 1;
-    if (vecA)
-      oz_slice<true><<<gridA, threads, 0, st>>>(A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA,
-                                                int64_t(L.rowsA) * L.kp, sc);
+    if (dtype_is_double(p.dtype))
+      slice_operands<double>(L, crt, p, cplx, sigA, sigB, resA, resB, st);
     else
-      oz_slice<false><<<gridA, threads, 0, st>>>(A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA,
-                                                 int64_t(L.rowsA) * L.kp, sc);
-    if (vecB)
-      oz_slice<true><<<gridB, threads, 0, st>>>(B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0,
-                                                s_sign, resB, int64_t(L.nb) * L.kp, sc);
-    else
-      oz_slice<false><<<gridB, threads, 0, st>>>(B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0,
-                                                 s_sign, resB, int64_t(L.nb) * L.kp, sc);
+      slice_operands<float>(L, crt, p, cplx, sigA, sigB, resA, resB, st);
   } else {
     cudaMemsetAsync(sigA, 0, sizeof(int) * L.rowsA, st);
     cudaMemsetAsync(sigB, 0, sizeof(int) * L.rowsB, st);
@@ -1079,14 +1140,17 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
   const int64_t total = p.m * p.n;
   const int threads = 256;
   const unsigned blocks = unsigned(std::min<int64_t>((total + threads - 1) / threads, 148 * 32));
-  if (cplx)
-    oz_reconstruct<true><<<blocks, threads, 0, st>>>(
-        R, L.rowsA, int(p.n), L.nb, sigA, sigB, p.C, p.ldc, p.alpha[0], p.alpha[1], p.beta[0],
-        p.beta[1], p.fill_mode, p.fill_ro, p.fill_co, BM, BN / 2, rp);
-  else
-    oz_reconstruct<false><<<blocks, threads, 0, st>>>(
-        R, L.rowsA, int(p.n), L.nb, sigA, sigB, p.C, p.ldc, p.alpha[0], p.alpha[1], p.beta[0],
-        p.beta[1], p.fill_mode, p.fill_ro, p.fill_co, BM, BN, rp);
+  auto recon = [&](auto kern) {
+    kern<<<blocks, threads, 0, st>>>(R, L.rowsA, int(p.n), L.nb, sigA, sigB, p.C, p.ldc,
+                                     p.alpha[0], p.alpha[1], p.beta[0], p.beta[1], p.fill_mode,
+                                     p.fill_ro, p.fill_co, BM, cplx ? BN / 2 : BN, rp);
+  };
+  switch (p.dtype) {
+    case kC64: recon(oz_reconstruct<kC64>); break;
+    case kC32: recon(oz_reconstruct<kC32>); break;
+    case kR64: recon(oz_reconstruct<kR64>); break;
+    default: recon(oz_reconstruct<kR32>); break;
+  }
   phase_mark(2, true, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return cudaSuccess;

@@ -17,7 +17,8 @@ inline constexpr int kMaxUsableModuli = 16;
 // 253 = 11*23, 247 = 13*19, 217 = 7*31, the rest prime).
 inline constexpr int kModuli[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
                                      223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
-inline constexpr int kDefaultModuli = 15;
+inline constexpr int kDefaultModuli = 15;       // double: Q = 57
+inline constexpr int kDefaultModuliFloat = 9;   // float: Q = 34
 
 struct Crt {
   int n;

@@ -84,6 +84,7 @@ bool use_ozaki(const GemmProblem& p, int path) {
   if (path == SPLAB_PATH_DMMA) return false;
   const double flops = double(p.m) * p.n * p.k * (p.dtype == kC64 ? 8.0 : 2.0);
   if (!(p.m >= 256 && p.n >= 128 && p.k >= 8192 && flops >= 1e13)) return false;
+  if (!dtype_is_double(p.dtype) && flops < 4e13) return false;
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
     cudaGetLastError();

@@ -54,6 +54,16 @@ def test_complex_multi_chunk_partial_tiles(opA):
     assert err <= 1e-14, err
 
 
+@pytest.mark.parametrize("dt,opA", [(np.complex64, 2), (np.complex64, 1), (np.float32, 1)])
+def test_float_dtypes(dt, opA):
+    """Float inputs through the Ozaki path (9 moduli by default): the float
+    result is within 1e-6 of the double-double oracle rounded to float."""
+    m, n, k = 260, 140, 90000
+    C0, got, ref, ldc = run_ssb(dt, m, n, k, opA, 0.5 + 0.25j if np.dtype(dt).kind == "c" else 0.5,
+                                -1.0, dist="gauss_k")
+    assert oracle.rel_fro(got, ref) <= 1e-6
+
+
 def test_real_double():
     m, n, k = 200, 330, 70000
     C0, got, ref, ldc = run_ssb(np.float64, m, n, k, 1, dist="uniform11")
