@@ -459,7 +459,58 @@ def workload_ssbtr_float(torch, spla, steps, warmup, path=None):
             "full_matrix_tflops": 2.0 * m * n * k / (ms / 1e3) / 1e12,
             "rel_err_vs_exact_triangle_3cols": err,
             "config": {"workload": "psgemm_ssbtr m=n=1536 k=400000 lower, op=T",
-                       "path": {None: "auto", 1: "FP64-accumulated DMMA", 2: "Ozaki INT8"}[path]}}
+                       "path": {None: "auto", 1: "FP64-accumulated DMMA", 2: "Ozaki INT8",
+                                3: "3xTF32"}[path]}}
+
+
+def workload_cgemm_ssb(torch, spla, steps, warmup, path=None):
+    """pcgemm_ssb complex float, A^H B, k = 250000, m = n = 1024, complex
+    Gaussian/sqrt(k) (the complex-double ssb configuration in single
+    precision), full C, beta = 0."""
+    import numpy as np
+    import oracle
+    m = n = 1024
+    k = 250000
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20250007)
+    s = (1.0 / (2 * k)) ** 0.5
+    A = (torch.randn((m, k), dtype=torch.complex64, device="cuda", generator=g) * s).contiguous()
+    B = (torch.randn((n, k), dtype=torch.complex64, device="cuda", generator=g) * s).contiguous()
+    C = torch.zeros((n, m), dtype=torch.complex64, device="cuda")
+    ctx = spla.Context(spla.PU_GPU)
+    if path is not None:
+        ctx.set_fp64_path(path)
+    dist = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128,
+                                                             128)
+
+    def step():
+        spla.pgemm_ssb(m, n, k, spla.OP_CONJ_TRANSPOSE, 1.0, A, k, B, k, 0.0, C, m, 0, 0, dist,
+                       ctx)
+
+    for _ in range(warmup):
+        step()
+    e0, e1 = _events(torch)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    cols = [0, 511, 1023]
+    An = A.cpu().numpy().astype(np.complex128).ravel()
+    Bs = np.ascontiguousarray(B[cols].cpu().numpy().astype(np.complex128).ravel())
+    ref = np.zeros(m * len(cols), np.complex128)
+    assert oracle.gemm(2, 0, m, len(cols), k, 1.0, An, k, Bs, k, 0.0, ref, m) == 0
+    got = C[cols].cpu().numpy().astype(np.complex128).ravel()
+    err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    flops = 8.0 * m * n * k
+    return {"metric": "CGEMM-SSB TFLOP/s (complex float, A^H B)",
+            "value": flops / (ms / 1e3) / 1e12, "unit": "TFLOP/s", "ms_per_step": ms,
+            "rel_err_vs_oracle_3cols": err,
+            "config": {"workload": "pcgemm_ssb m=n=1024 k=250000 op=C",
+                       "path": {None: "auto", 1: "FP64-accumulated DMMA", 2: "Ozaki INT8",
+                                3: "3xTF32"}[path]}}
 
 
 def workload_batch(torch, spla, steps, warmup, dtype="complex128", count=64, sub=32):
@@ -529,6 +580,10 @@ def run_workload(name, steps, warmup):
     fn = {"sbs": workload_sbs, "ssbtr_float": workload_ssbtr_float,
           "ssbtr_float_dmma": lambda t, s, st, w: workload_ssbtr_float(t, s, st, w, 1),
           "ssbtr_float_ozaki": lambda t, s, st, w: workload_ssbtr_float(t, s, st, w, 2),
+          "ssbtr_float_tf32x3": lambda t, s, st, w: workload_ssbtr_float(t, s, st, w, 3),
+          "cgemm_ssb_dmma": lambda t, s, st, w: workload_cgemm_ssb(t, s, st, w, 1),
+          "cgemm_ssb_ozaki": lambda t, s, st, w: workload_cgemm_ssb(t, s, st, w, 2),
+          "cgemm_ssb_tf32x3": lambda t, s, st, w: workload_cgemm_ssb(t, s, st, w, 3),
           "batch": workload_batch,
           "batch_c64": lambda t, s, st, w: workload_batch(t, s, st, w, "complex64", 64, 64)}[name]
     line = fn(torch, spla, steps, warmup)
@@ -551,7 +606,8 @@ def main():
     ap.add_argument("--k", type=int, default=250000, help="k (profiling of smaller cases)")
     ap.add_argument("--workload", default="zgemm_ssb",
                     choices=["zgemm_ssb", "sbs", "ssbtr_float", "ssbtr_float_dmma",
-                             "ssbtr_float_ozaki", "batch", "batch_c64"])
+                             "ssbtr_float_ozaki", "ssbtr_float_tf32x3", "cgemm_ssb_dmma",
+                             "cgemm_ssb_ozaki", "cgemm_ssb_tf32x3", "batch", "batch_c64"])
     args = ap.parse_args()
     if args.workload != "zgemm_ssb" and args.impl == "ours":
         return run_workload(args.workload, args.steps, max(3, args.warmup))

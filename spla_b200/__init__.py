@@ -27,8 +27,8 @@ OP_NONE, OP_TRANSPOSE, OP_CONJ_TRANSPOSE = 0, 1, 2
 FILL_MODE_FULL, FILL_MODE_UPPER, FILL_MODE_LOWER = 0, 1, 2
 # single-rank communicators (MPICH handle encoding, as the library's stand-in)
 MPI_COMM_WORLD, MPI_COMM_SELF = 0x44000000, 0x44000001
-# contraction paths for double / complex double
-PATH_AUTO, PATH_DMMA, PATH_OZAKI = 0, 1, 2
+# contraction paths (PATH_TF32X3: float and complex float only)
+PATH_AUTO, PATH_DMMA, PATH_OZAKI, PATH_TF32X3 = 0, 1, 2, 3
 
 
 class GenericError(RuntimeError):
@@ -226,7 +226,7 @@ class Context:
         check(lib().spla_ctx_set_op_threshold_gpu(self._h, int(v)))
 
     def set_fp64_path(self, path: int, moduli: int = 0):
-        """Library extension: FP64 contraction path (PATH_AUTO / PATH_DMMA / PATH_OZAKI)."""
+        """Library extension: contraction path (PATH_AUTO / PATH_DMMA / PATH_OZAKI / PATH_TF32X3)."""
         check(lib().spla_b200_ctx_set_fp64_path(self._h, int(path), int(moduli)))
 
     def close(self):

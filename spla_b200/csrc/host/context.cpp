@@ -88,6 +88,7 @@ int path_from_env() {
   if (!v) return SPLAB_PATH_AUTO;
   if (!std::strcmp(v, "dmma")) return SPLAB_PATH_DMMA;
   if (!std::strcmp(v, "ozaki")) return SPLAB_PATH_OZAKI;
+  if (!std::strcmp(v, "tf32x3")) return SPLAB_PATH_TF32X3;
   return SPLAB_PATH_AUTO;
 }
 }  // namespace
@@ -277,10 +278,11 @@ SplaError spla_ctx_set_alloc_gpu(SplaContext ctx, void* (*a)(size_t), void (*f)(
 }
 
 // Library extensions (no reference counterpart): select the FP64 contraction
-// path of a context. path: 0 auto, 1 FP64 DMMA, 2 Ozaki INT8; moduli 0 = default.
+// path of a context. path: 0 auto, 1 FP64 DMMA, 2 Ozaki INT8, 3 3xTF32 (float
+// dtypes); moduli 0 = default.
 SPLA_EXPORT SplaError spla_b200_ctx_set_fp64_path(SplaContext ctx, int path, int moduli) {
   if (!ctx) return SPLA_INVALID_HANDLE_ERROR;
-  if (path < 0 || path > 2 || moduli < 0 || moduli > 16 || (moduli > 0 && moduli < 8))
+  if (path < 0 || path > 3 || moduli < 0 || moduli > 16 || (moduli > 0 && moduli < 8))
     return SPLA_INVALID_PARAMETER_ERROR;
   return guarded([&] {
     auto& c = spla::detail::Access::ctx(as_ctx(ctx));

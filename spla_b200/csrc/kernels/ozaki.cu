@@ -38,13 +38,16 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "ozaki.cuh"
 #include "ozaki_crt.cuh"
+#include "tcgen05_common.cuh"
 
 namespace splab {
 namespace oz {
+using namespace tc;
 
 constexpr int BM = 128;       // rows of A per tile (TMEM lanes)
 constexpr int BN = 256;       // rows of B per tile (TMEM columns)
@@ -61,77 +64,6 @@ constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any 
 
 // --------------------------------------------------------------------------
 // device helpers
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(done)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-
-// Wait for the phase of `bar` with parity `parity` to complete. Bounded: gives
-// up after kWaitLimitNs or when another role raised *abort, and returns false.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort,
-                                          unsigned long long limit_ns) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const unsigned long long t0 = globaltimer();
-  for (uint32_t it = 1;; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 0) {
-      if (*abort) return false;
-      if (globaltimer() - t0 > limit_ns) {
-        *abort = 1;
-        return false;
-      }
-    }
-  }
-}
-
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
-                                            uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-      : "memory");
-}
-
-// UMMA shared-memory descriptor: K-major operand in the 128-byte swizzle
-// layout written by TMA (8-row atoms of 128 B, atoms 1024 B apart).
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= uint64_t((saddr >> 4) & 0x3FFFu);  // start address
-  d |= uint64_t(1) << 16;                  // leading byte offset (unused for SW128 K-major)
-  d |= uint64_t(1024 >> 4) << 32;          // stride byte offset: 8 rows x 128 B
-  d |= uint64_t(1) << 46;                  // descriptor version (sm_100)
-  d |= uint64_t(2) << 61;                  // layout: 128-byte swizzle
-  return d;
-}
 
 // Instruction descriptor of tcgen05.mma kind::i8: S32 accumulate, signed int8
 // A and B, both K-major, M = 128, N = 256.
@@ -151,33 +83,6 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_
       : "memory");
 }
 
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-      : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-        "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
-        "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
-        "=r"(v[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
 
 // --------------------------------------------------------------------------
 // 1. row scale exponents
@@ -363,6 +268,8 @@ struct GemmParams {
   int total_units;   // nmod * nchunks * tiles_m * tiles_n
   int* R;            // accumulated residues [nmod][nb][m] (int32)
   int* status;       // set to 1 when a bounded wait gave up
+  const int* active; // CTA-pair kernel: list of tiles to compute (fill mode), or null = all
+  int n_active;
   unsigned long long wait_limit_ns;  // bound on every barrier wait
   int stall_test;    // 1: the producer issues no copies (exercises the bounded waits)
   int p[kMaxModuli];
@@ -578,32 +485,6 @@ constexpr int GEMM2_SMEM = STAGES2 * STAGE2_BYTES + 1024 + 1024;
 constexpr uint32_t kIdescI8Pair = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(256 >> 3) << 17) |
                                   (uint32_t(256 >> 4) << 24);
 
-__device__ __forceinline__ uint32_t cluster_rank() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t map_to_rank(uint32_t saddr, uint32_t rank) {
-  uint32_t out;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(saddr), "r"(rank));
-  return out;
-}
-__device__ __forceinline__ void cluster_sync_all() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
-                   : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
-               : "memory");
-}
-__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y,
-                                                 uint32_t bar_cluster) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar_cluster)
-      : "memory");
-}
 __device__ __forceinline__ void umma_i8_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
                                              uint32_t accumulate) {
   asm volatile(
@@ -613,14 +494,6 @@ __device__ __forceinline__ void umma_i8_pair(uint32_t tmem_d, uint64_t adesc, ui
       "l"(adesc), "l"(bdesc), "r"(kIdescI8Pair), "r"(accumulate)
       : "memory");
 }
-__device__ __forceinline__ void umma_commit_pair(uint32_t bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
-      " [%0], %1;" ::"r"(bar),
-      "h"((unsigned short)0x3)
-      : "memory");
-}
-
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     oz_gemm_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  const __grid_constant__ GemmParams g) {
@@ -666,8 +539,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
+  const int ntl = g.active ? g.n_active : tiles;
   auto unit_of = [&](int u, int& t, int& c, int& tm, int& tn) {
-    const int tile = u % tiles, rest = u / tiles;
+    const int tl = u % ntl, rest = u / ntl;
+    const int tile = g.active ? g.active[tl] : tl;
     tm = tile % g.tiles_m;
     tn = tile / g.tiles_m;
     c = rest % g.nchunks;
@@ -880,7 +755,7 @@ struct Layout {
   int nmod;
   int64_t K2, kp;          // real depth, padded to 128
   int rowsA, rowsB, nb;    // A rows, B source rows, B residue rows
-  size_t off_sigA, off_sigB, off_resA, off_resB, off_R, off_status, total;
+  size_t off_sigA, off_sigB, off_resA, off_resB, off_R, off_status, off_tiles, total;
 };
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -908,6 +783,8 @@ Layout layout_of(const GemmProblem& p, int moduli) {
   off = align256(off + sizeof(int) * size_t(L.nmod) * L.nb * L.rowsA);
   L.off_status = off;
   off = align256(off + 256);
+  L.off_tiles = off;
+  off = align256(off + sizeof(int) * size_t((L.rowsA + 255) / 256) * ((L.nb + 255) / 256));
   L.total = off;
   return L;
 }
@@ -1088,6 +965,49 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
       g.tiles_m = (L.rowsA + 255) / 256;
       g.tiles_n = (L.nb + 255) / 256;
       g.total_units = g.nmod * g.nchunks * g.tiles_m * g.tiles_n;
+      if (p.fill_mode != 0) {
+        // compute only the pair tiles that cover an element the reconstruction
+        // writes: its tiles are BM x (BN/2 complex | BN real) of C
+        const int rt_m = BM, rt_n = cplx ? BN / 2 : BN;
+        std::vector<int> act;
+        for (int tn = 0; tn < g.tiles_n; ++tn)
+          for (int tm = 0; tm < g.tiles_m; ++tm) {
+            const int64_t r0 = int64_t(tm) * 256, r1 = std::min<int64_t>(r0 + 256, L.rowsA);
+            const int64_t b0 = int64_t(tn) * 256, b1 = std::min<int64_t>(b0 + 256, L.nb);
+            // complex columns covered by the B rows (u rows j, v rows n + j)
+            int64_t cr[2][2] = {{0, 0}, {0, 0}};
+            int ncr = 0;
+            if (!cplx) {
+              cr[ncr][0] = b0;
+              cr[ncr++][1] = b1;
+            } else {
+              if (b0 < p.n) {
+                cr[ncr][0] = b0;
+                cr[ncr++][1] = std::min<int64_t>(b1, p.n);
+              }
+              if (b1 > p.n) {
+                cr[ncr][0] = std::max<int64_t>(b0, p.n) - p.n;
+                cr[ncr++][1] = b1 - p.n;
+              }
+            }
+            bool on = false;
+            for (int q = 0; q < ncr && !on; ++q)
+              for (int64_t ti = (r0 / rt_m) * rt_m; ti < r1 && !on; ti += rt_m)
+                for (int64_t tj = (cr[q][0] / rt_n) * rt_n; tj < cr[q][1] && !on; tj += rt_n)
+                  on = tile_is_active(p.fill_mode, ti, tj, std::min<int64_t>(rt_m, p.m - ti),
+                                      std::min<int64_t>(rt_n, p.n - tj), p.fill_ro, p.fill_co);
+            if (on) act.push_back(tm + tn * g.tiles_m);
+          }
+        if (act.empty()) act.push_back(0);  // keep the launch well formed
+        int* dtiles = reinterpret_cast<int*>(w + L.off_tiles);
+        if ((e = cudaMemcpyAsync(dtiles, act.data(), sizeof(int) * act.size(),
+                                 cudaMemcpyHostToDevice, st)) != cudaSuccess)
+          return e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;  // host list goes away
+        g.active = dtiles;
+        g.n_active = int(act.size());
+        g.total_units = g.nmod * g.nchunks * g.n_active;
+      }
       static bool attr2 = false;
       if (!attr2) {
         cudaFuncSetAttribute(oz_gemm_pair, cudaFuncAttributeMaxDynamicSharedMemorySize,

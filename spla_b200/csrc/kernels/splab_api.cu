@@ -9,6 +9,7 @@
 #include "common.cuh"
 #include "gemm_dmma.cuh"
 #include "ozaki.cuh"
+#include "tf32x3.cuh"
 
 namespace splab {
 
@@ -93,6 +94,11 @@ bool use_ozaki(const GemmProblem& p, int path) {
   return ozaki_workspace_bytes(p, 0) <= free_b / 4;
 }
 
+// 3xTF32 only when requested and the problem is a float ssb-shaped one.
+bool use_tf32x3(const GemmProblem& p, int path) {
+  return path == SPLAB_PATH_TF32X3 && tf32x3_supported(p);
+}
+
 __global__ void block_cyclic_info_kernel(int64_t rb, int64_t cb, int64_t gr, int64_t gc,
                                          int64_t nr, int64_t nc, int64_t ro, int64_t co,
                                          const int64_t* __restrict__ ids, int64_t count,
@@ -146,6 +152,7 @@ int splab_gemm_path(int dtype, int path, int opA, int opB, int64_t m, int64_t n,
   p.n = n;
   p.k = k;
   if (dtype < 0 || dtype > 3 || m <= 0 || n <= 0 || k < 0) return SPLAB_PATH_DMMA;
+  if (use_tf32x3(p, path)) return SPLAB_PATH_TF32X3;
   return use_ozaki(p, path) ? SPLAB_PATH_OZAKI : SPLAB_PATH_DMMA;
 }
 
@@ -159,6 +166,7 @@ size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t 
   p.m = m;
   p.n = n;
   p.k = k;
+  if (use_tf32x3(p, path)) return tf32x3_workspace_bytes(p);
   if (use_ozaki(p, path)) return ozaki_workspace_bytes(p, ozakiModuli);
   return dmma_plan(p, num_sms()).workspace_bytes;
 }
@@ -174,7 +182,9 @@ int splab_gemm_check(int dtype, int path, int opA, int opB, int64_t m, int64_t n
   p.n = n;
   p.k = k;
   if (cudaStreamSynchronize(st) != cudaSuccess) return SPLAB_ERR_LAUNCH;
-  if (m <= 0 || n <= 0 || !workspace || !use_ozaki(p, path)) return SPLAB_OK;
+  if (m <= 0 || n <= 0 || !workspace) return SPLAB_OK;
+  if (use_tf32x3(p, path)) return tf32x3_status(p, workspace, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
+  if (!use_ozaki(p, path)) return SPLAB_OK;
   return ozaki_status(p, ozakiModuli, workspace, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
 }
 
@@ -183,7 +193,7 @@ int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int6
                const void* beta, void* C, int64_t ldc, int fill, int64_t ro, int64_t co,
                int ozakiModuli, void* workspace, size_t workspaceBytes, void* stream) {
   if (!valid_problem(dtype, opA, opB, m, n, k, lda, ldb, ldc)) return SPLAB_ERR_INVALID;
-  if (path < 0 || path > 2 || fill < 0 || fill > 2 || !alpha || !beta) return SPLAB_ERR_INVALID;
+  if (path < 0 || path > 3 || fill < 0 || fill > 2 || !alpha || !beta) return SPLAB_ERR_INVALID;
   if (m == 0 || n == 0) return SPLAB_OK;
   if (!C || (k > 0 && (!A || !B))) return SPLAB_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -191,7 +201,11 @@ int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int6
                                fill, ro, co);
   cudaError_t err;
   if (ozakiModuli != 0 && (ozakiModuli < 8 || ozakiModuli > 16)) return SPLAB_ERR_INVALID;
-  if (use_ozaki(p, path)) {
+  if (use_tf32x3(p, path)) {
+    const size_t need = tf32x3_workspace_bytes(p);
+    if (need > workspaceBytes || (need && !workspace)) return SPLAB_ERR_WORKSPACE;
+    err = tf32x3_gemm(p, workspace, workspaceBytes, st);
+  } else if (use_ozaki(p, path)) {
     const size_t need = ozaki_workspace_bytes(p, ozakiModuli);
     if (need > workspaceBytes || (need && !workspace)) return SPLAB_ERR_WORKSPACE;
     err = ozaki_gemm(p, ozakiModuli, workspace, workspaceBytes, st);
