@@ -15,10 +15,10 @@
 // walked in windows of kWin k-blocks (64 reals); each window starts from a
 // zero accumulator, issues the small correction products (hi lo, lo hi) of
 // the whole window first and the hi hi products last, so only 8 MMAs add
-// into a large value. The epilogue folds each window's FP32 result into a
-// running double-float sum (hi + lo pair of FP32, error-free 2Sum) kept in
-// TMEM beside the double-buffered accumulator, and writes the FP64 value of
-// the sum once per work unit.
+// into a large value. The epilogue adds kFold window results in registers
+// (round to nearest), folds that sum into a running double-float sum (hi +
+// lo pair of FP32, error-free 2Sum) kept in TMEM beside the double-buffered
+// accumulator, and writes the FP64 value of the sum once per work unit.
 //
 // Tiles: a CTA pair computes 256 rows x 128 columns of the real-form result
 // (tcgen05.mma.cta_group::2.kind::tf32 M256 N128 K8). TMEM per CTA: columns
@@ -54,8 +54,9 @@ constexpr int B_PLANE = 64 * 128;       // bytes per B plane per CTA and stage (
 constexpr int STAGE_BYTES = 2 * A_PLANE + 2 * B_PLANE;  // A_hi, A_lo, B_hi, B_lo
 constexpr int STAGES = 4;
 constexpr int kWin = 2;                 // k-blocks per FP32 accumulation window
+constexpr int kFold = 4;                // windows per register sum before the 2Sum fold
 constexpr int kMinSuperBlocks = 64;     // smallest k extent of a work unit (2048 reals)
-constexpr int THREADS = 192;            // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int THREADS = 320;            // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 constexpr int SMEM = STAGES * STAGE_BYTES + 2048;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 constexpr uint32_t kIdesc = (1u << 4)                      // D: F32
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(accf_bar(b), 1);
-      mbar_init(acce_bar(b), 256);
+      mbar_init(acce_bar(b), 16);  // one arrival per epilogue warp of both CTAs
     }
     mbar_init(drain_bar, 1);
     *abort = 0;
@@ -294,8 +295,14 @@ __global__ void __launch_bounds__(THREADS, 1)
       }
     }
   } else if (warp >= 2) {
-    // ---- epilogue (both CTAs): window results -> double-float TMEM sums
+    // ---- epilogue (both CTAs). Warp w reads TMEM lanes 32 (w % 4) .. +31
+    // (its hardware lane quarter); warps 2-5 take columns 0-63 of the tile,
+    // warps 6-9 columns 64-127. Each window's FP32 result is loaded, the
+    // accumulator released at once, and the values added (round to nearest)
+    // to a register sum of kFold windows; every kFold windows that sum is
+    // folded into the double-float TMEM sum with 2Sum.
     const int quarter = warp & 3;
+    const int col_lo = ((warp - 2) >> 2) * (TN / 2);
     const int row = int(rank) * 128 + quarter * 32 + lane;
     const uint32_t lane_addr = tmem_base + (uint32_t(quarter * 32) << 16);
     uint32_t acc_phase[2] = {0, 0};
@@ -306,33 +313,55 @@ __global__ void __launch_bounds__(THREADS, 1)
       unit_of(u, sc, tm, tn);
       const int kb0 = sc * g.super_blocks, kb1 = min(g.kblocks, kb0 + g.super_blocks);
       const int i = tm * 256 + row;
-      for (int w0 = kb0; w0 < kb1; w0 += kWin) {
+      float mid[TN / 2];
+#pragma unroll
+      for (int c = 0; c < TN / 2; ++c) mid[c] = 0.0f;
+      bool first_fold = true;
+      int wi = 0;
+      for (int w0 = kb0; w0 < kb1; w0 += kWin, ++wi) {
         if (!mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const bool first = w0 == kb0, last = w0 + kWin >= kb1;
-#pragma unroll 1
-        for (int c0 = 0; c0 < TN; c0 += 32) {
-          uint32_t a[32], h[32], l[32];
-          tmem_ld32_nowait(lane_addr + uint32_t(accb * TN + c0), a);
-          if (!first) {
-            tmem_ld32_nowait(lane_addr + uint32_t(2 * TN + c0), h);
-            tmem_ld32_nowait(lane_addr + uint32_t(3 * TN + c0), l);
-          }
+#pragma unroll
+        for (int q = 0; q < TN / 64; ++q) {
+          uint32_t a[32];
+          tmem_ld32_nowait(lane_addr + uint32_t(accb * TN + col_lo + 32 * q), a);
           tmem_wait_ld();
 #pragma unroll
+          for (int cc = 0; cc < 32; ++cc)
+            mid[32 * q + cc] = __fadd_rn(mid[32 * q + cc], __uint_as_float(a[cc]));
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cluster(map_to_rank(acce_bar(accb), 0));
+        acc_phase[accb] ^= 1u;
+        accb ^= 1;
+
+        const bool last = w0 + kWin >= kb1;
+        if (!last && (wi % kFold) != kFold - 1) continue;
+#pragma unroll
+        for (int q = 0; q < TN / 64; ++q) {
+          const int c0 = col_lo + 32 * q;
+          uint32_t h[32], l[32];
+          if (!first_fold) {
+            tmem_ld32_nowait(lane_addr + uint32_t(2 * TN + c0), h);
+            tmem_ld32_nowait(lane_addr + uint32_t(3 * TN + c0), l);
+            tmem_wait_ld();
+          }
+#pragma unroll
           for (int cc = 0; cc < 32; ++cc) {
-            if (first) {
-              h[cc] = a[cc];
+            if (first_fold) {
+              h[cc] = __float_as_uint(mid[32 * q + cc]);
               l[cc] = 0u;
             } else {
               float t, e;
-              two_sum(__uint_as_float(h[cc]), __uint_as_float(a[cc]), t, e);
+              two_sum(__uint_as_float(h[cc]), mid[32 * q + cc], t, e);
               h[cc] = __float_as_uint(t);
               l[cc] = __float_as_uint(__fadd_rn(__uint_as_float(l[cc]), e));
             }
+            mid[32 * q + cc] = 0.0f;
           }
           if (last) {
             if (i < g.m) {
@@ -351,10 +380,7 @@ __global__ void __launch_bounds__(THREADS, 1)
           }
         }
         tmem_wait_st();
-        tc_fence_before();
-        mbar_arrive_cluster(map_to_rank(acce_bar(accb), 0));
-        acc_phase[accb] ^= 1u;
-        accb ^= 1;
+        first_fold = false;
       }
     }
   }
@@ -470,7 +496,11 @@ Layout layout_of(const GemmProblem& p) {
   L.nb = cplx ? int(2 * p.n) : int(p.n);
   const int64_t kblocks = L.kp / BKF;
   const int tiles = ((L.rowsA + 255) / 256) * ((L.nb + TN - 1) / TN);
-  const int s = choose_splits(kblocks, tiles, std::max(1, sm_count() / 2), L.rowsA, L.nb);
+  int s = choose_splits(kblocks, tiles, std::max(1, sm_count() / 2), L.rowsA, L.nb);
+  if (const char* v = std::getenv("SPLAB_TF32X3_SPLITS")) {  // tuning override
+    const int f = std::atoi(v);
+    if (f > 0) s = int(std::min<int64_t>(f, kblocks > 0 ? kblocks : 1));
+  }
   L.super_blocks = int(std::max<int64_t>(1, (kblocks + s - 1) / s));
   L.nsuper = int(std::max<int64_t>(1, (kblocks + L.super_blocks - 1) / L.super_blocks));
   size_t off = 0;
