@@ -118,38 +118,86 @@ __global__ void oz_row_scale(const TIn* __restrict__ X, int64_t ld_elems, int64_
 // --------------------------------------------------------------------------
 // 2. residues
 
+// Per-modulus constants of the slicer, each stored twice (both halves of an
+// f32x2 operand): -p, 1/p and the digit weights 2^(13 i) mod p in symmetric
+// form, i = 1..4.
 struct SliceConsts {
   int n;
-  float p[kMaxModuli];
-  float inv_p[kMaxModuli];
-  // 2^(13 i) mod p in symmetric form, i = 1..4 (digit weights)
-  float c[kMaxModuli][4];
+  float p0;  // first modulus (256: residue = low byte of the lowest digit)
+  unsigned long long neg_p[kMaxModuli];
+  unsigned long long inv_p[kMaxModuli];
+  unsigned long long c[kMaxModuli][4];
 };
 
-// Residues are computed on the FP32 pipe from five balanced base-2^13 digits
-// of the scaled integer x (|x| < 2^62), which are extracted exactly with FP64
-// operations:  x = sum_i d_i 2^(13 i), |d_i| <= 4096 (|d_4| <= 1024). For a
+// Residues are computed on the FP32 pipe from base-2^13 digits of the scaled
+// integer x = round(2^sigma y) (|x| < 2^62), x = sum_i d_i 2^(13 i), which are
+// extracted without conversion instructions: x = xh 2^26 + xl with
+// xh = round(y 2^-26) and |xl| <= 2^25, both read as integers from the bits of
+// (value + 1.5 2^52); then d_0 = xl mod 2^13 (0 .. 8191), d_1 = xl >> 13
+// (|d_1| <= 4096), and xh gives d_2.. the same way (top digit signed). For a
 // modulus p the digit sum s = d_0 + sum_i c_i d_i (|c_i| <= p/2) is below
 // 2^22 in magnitude and exact in FP32; r = s - p * nearest(s / p) lies in
 // [-(p-1)/2, (p-1)/2] for odd p. For p = 256 the weights vanish and r is the
 // low byte of d_0. Each residue is produced as the float MAGIC + r, whose low
 // byte is r in two's complement: the int8 value without a conversion.
+__device__ __forceinline__ float small_int_to_float(int d) {  // |d| < 2^22
+  return __int_as_float(0x4B400000 + d) - 12582912.0f;
+}
+
 template <int NDIG>
-__device__ __forceinline__ void digits13(double x, float (&d)[5]) {
-  const double b = 8192.0, ib = 1.0 / 8192.0;
-  double q = x;
-#pragma unroll
-  for (int i = 0; i < NDIG - 1; ++i) {
-    const double qn = rint(q * ib);
-    d[i] = float(fma(qn, -b, q));
-    q = qn;
+__device__ __forceinline__ void digits13(double y, float (&d)[5]) {
+  constexpr double kM52 = 6755399441055744.0;  // 1.5 * 2^52: ulp 1
+  constexpr long long kM52Bits = 0x4338000000000000ll;
+  const double t = fma(y, 1.0 / 67108864.0, kM52);  // kM52 + round(y 2^-26)
+  const double xl_d = fma(t - kM52, -67108864.0, y);  // exact, |xl_d| <= 2^25
+  const int xl = int(__double2loint(xl_d + kM52));  // round(xl_d), two's complement
+  const long long xh = __double_as_longlong(t) - kM52Bits;
+  d[0] = small_int_to_float(xl & 0x1FFF);
+  d[1] = small_int_to_float(xl >> 13);
+  if (NDIG == 3) {
+    d[2] = small_int_to_float(int(xh));
+  } else if (NDIG == 4) {
+    d[2] = small_int_to_float(int(xh & 0x1FFF));
+    d[3] = small_int_to_float(int(xh >> 13));
+  } else {
+    d[2] = small_int_to_float(int(xh & 0x1FFF));
+    d[3] = small_int_to_float(int((xh >> 13) & 0x1FFF));
+    d[4] = small_int_to_float(int(xh >> 26));
   }
-  d[NDIG - 1] = float(q);
 #pragma unroll
   for (int i = NDIG; i < 5; ++i) d[i] = 0.0f;
 }
 
 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: ulp 1, low mantissa bits hold r
+
+// Two floats in one 64-bit register for the packed FP32 instructions of
+// sm_100 (fma/add .f32x2: one instruction, two lanes of work).
+__host__ __device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+#ifdef __CUDA_ARCH__
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+#else
+  uint32_t a, b;
+  std::memcpy(&a, &lo, 4);
+  std::memcpy(&b, &hi, 4);
+  return (static_cast<unsigned long long>(b) << 32) | a;
+#endif
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
 
 __device__ __forceinline__ uint32_t pack4(float a, float b, float c, float d) {
   const uint32_t t0 = __byte_perm(__float_as_uint(a), __float_as_uint(b), 0x0040);
@@ -164,93 +212,108 @@ __device__ __forceinline__ uint32_t neg_odd_bytes(uint32_t w) {
 }
 
 // Residues of one operand, written K-major: res[t][row][l] (row stride kp).
-// Each thread handles 16 consecutive reals of one row.
+// Each thread handles EL (8 or 16) consecutive reals of one row.
 // mode 0: plain rows (A rows, or B rows of a real product): out row = row.
 // mode 1: complex B rows -> u row `row` and v row `row + rows` with sign s:
 //         u = (br, -s*bi), v = (bi, s*br) interleaved.
 // TIn: double (|x| < 2^62, five digits) or float (|x| < 2^38, three digits).
-template <typename TIn, bool VEC, int NDIG>
-__global__ void __launch_bounds__(256) oz_slice(const TIn* __restrict__ X, int64_t ld_doubles,
-                                                int64_t len, int rows, int64_t kp,
-                                                const int* __restrict__ sigma, int mode,
-                                                int s_sign, int8_t* __restrict__ res,
-                                                int64_t res_mod_stride, SliceConsts sc) {
-  const int64_t groups = kp / 16;
+template <typename TIn, bool VEC, int NDIG, int EL>
+__global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
+    oz_slice(const TIn* __restrict__ X, int64_t ld_doubles, int64_t len, int rows, int64_t kp,
+             const int* __restrict__ sigma, int mode, int s_sign, int8_t* __restrict__ res,
+             int64_t res_mod_stride, SliceConsts sc, int t_begin, int t_end) {
+  static_assert(EL == 8 || EL == 16, "8 or 16 reals per thread");
+  constexpr int W = EL / 4;  // packed words per modulus
+  const int64_t groups = kp / EL;
   const int64_t gid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   const int row = int(gid / groups);
   if (row >= rows) return;
-  const int64_t l0 = (gid % groups) * 16;
+  const int64_t l0 = (gid % groups) * EL;
   const TIn* x = X + int64_t(row) * ld_doubles + l0;
   const int sg = sigma[row];
   // 2^sg as a double when representable, else ldexp per element
   const bool direct = sg > -1000 && sg < 1000;
   const double scale = direct ? __longlong_as_double((long long)(sg + 1023) << 52) : 1.0;
-  double v[16];
-  if (VEC && l0 + 16 <= len) {
-    if constexpr (sizeof(TIn) == 8) {
+  unsigned long long dp[EL / 2][5];  // digits of elements 2i, 2i + 1
+  {
+    double v[EL];
+    if (VEC && l0 + EL <= len) {
+      if constexpr (sizeof(TIn) == 8) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const double2 t = __ldg(reinterpret_cast<const double2*>(x) + i);
-        v[2 * i] = t.x;
-        v[2 * i + 1] = t.y;
+        for (int i = 0; i < EL / 2; ++i) {
+          const double2 t = __ldg(reinterpret_cast<const double2*>(x) + i);
+          v[2 * i] = t.x;
+          v[2 * i + 1] = t.y;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < EL / 4; ++i) {
+          const float4 t = __ldg(reinterpret_cast<const float4*>(x) + i);
+          v[4 * i] = t.x;
+          v[4 * i + 1] = t.y;
+          v[4 * i + 2] = t.z;
+          v[4 * i + 3] = t.w;
+        }
       }
     } else {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const float4 t = __ldg(reinterpret_cast<const float4*>(x) + i);
-        v[4 * i] = t.x;
-        v[4 * i + 1] = t.y;
-        v[4 * i + 2] = t.z;
-        v[4 * i + 3] = t.w;
-      }
+      for (int i = 0; i < EL; ++i) v[i] = (l0 + i < len) ? double(x[i]) : 0.0;
     }
-  } else {
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = (l0 + i < len) ? double(x[i]) : 0.0;
+    for (int i = 0; i < EL / 2; ++i) {
+      float d0[5], d1[5];
+      digits13<NDIG>(direct ? v[2 * i] * scale : ldexp(v[2 * i], sg), d0);
+      digits13<NDIG>(direct ? v[2 * i + 1] * scale : ldexp(v[2 * i + 1], sg), d1);
+#pragma unroll
+      for (int j = 0; j < 5; ++j) dp[i][j] = f2_pack(d0[j], d1[j]);
+    }
   }
-  float d[16][5];
+  const unsigned long long M2 = f2_pack(kMagic, kMagic), NM2 = f2_pack(-kMagic, -kMagic);
+  int8_t* out = res + t_begin * res_mod_stride + int64_t(row) * kp + l0;
+  for (int t = t_begin; t < t_end; ++t, out += res_mod_stride) {
+    float r[EL];
+    if (t == 0 && sc.p0 == 256.0f) {
 #pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    const double xi = rint(direct ? v[i] * scale : ldexp(v[i], sg));
-    digits13<NDIG>(xi, d[i]);
-  }
-  for (int t = 0; t < sc.n; ++t) {
-    float r[16];
-    if (t == 0 && sc.p[0] == 256.0f) {
-#pragma unroll
-      for (int i = 0; i < 16; ++i) r[i] = d[i][0] + kMagic;
+      for (int i = 0; i < EL / 2; ++i) f2_unpack(f2_add(dp[i][0], M2), r[2 * i], r[2 * i + 1]);
     } else {
-      const float p = sc.p[t], ip = sc.inv_p[t];
-      const float c1 = sc.c[t][0], c2 = sc.c[t][1], c3 = sc.c[t][2], c4 = sc.c[t][3];
+      const unsigned long long np = sc.neg_p[t], ip = sc.inv_p[t];
+      const unsigned long long c1 = sc.c[t][0], c2 = sc.c[t][1], c3 = sc.c[t][2],
+                               c4 = sc.c[t][3];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        float s = fmaf(c1, d[i][1], d[i][0]);
-        if (NDIG > 2) s = fmaf(c2, d[i][2], s);
-        if (NDIG > 3) s = fmaf(c3, d[i][3], s);
-        if (NDIG > 4) s = fmaf(c4, d[i][4], s);
-        const float q = fmaf(s, ip, kMagic) - kMagic;
-        r[i] = fmaf(-q, p, s + kMagic);
+      for (int i = 0; i < EL / 2; ++i) {
+        unsigned long long s2 = f2_fma(c1, dp[i][1], dp[i][0]);
+        if (NDIG > 2) s2 = f2_fma(c2, dp[i][2], s2);
+        if (NDIG > 3) s2 = f2_fma(c3, dp[i][3], s2);
+        if (NDIG > 4) s2 = f2_fma(c4, dp[i][4], s2);
+        const unsigned long long q2 = f2_add(f2_fma(s2, ip, M2), NM2);
+        f2_unpack(f2_fma(q2, np, f2_add(s2, M2)), r[2 * i], r[2 * i + 1]);
       }
     }
-    uint32_t w[4];
+    uint32_t w[W];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) w[q] = pack4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
-    int8_t* out = res + t * res_mod_stride;
+    for (int q = 0; q < W; ++q) w[q] = pack4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
     if (mode == 0) {
-      *reinterpret_cast<uint4*>(out + int64_t(row) * kp + l0) = make_uint4(w[0], w[1], w[2], w[3]);
+      if constexpr (W == 4)
+        *reinterpret_cast<uint4*>(out) = make_uint4(w[0], w[1], w[2], w[3]);
+      else
+        *reinterpret_cast<uint2*>(out) = make_uint2(w[0], w[1]);
     } else {
       // w = [br0, bi0, br1, bi1]; u = [br, -s bi], v = [bi, s br]
-      uint32_t wu[4], wv[4];
+      uint32_t wu[W], wv[W];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < W; ++q) {
         const uint32_t sw = __byte_perm(w[q], 0u, 0x2301);  // [bi0, br0, bi1, br1]
         wu[q] = s_sign > 0 ? neg_odd_bytes(w[q]) : w[q];
         wv[q] = s_sign > 0 ? sw : neg_odd_bytes(sw);
       }
-      *reinterpret_cast<uint4*>(out + int64_t(row) * kp + l0) =
-          make_uint4(wu[0], wu[1], wu[2], wu[3]);
-      *reinterpret_cast<uint4*>(out + int64_t(row + rows) * kp + l0) =
-          make_uint4(wv[0], wv[1], wv[2], wv[3]);
+      int8_t* out_v = out + int64_t(rows) * kp;
+      if constexpr (W == 4) {
+        *reinterpret_cast<uint4*>(out) = make_uint4(wu[0], wu[1], wu[2], wu[3]);
+        *reinterpret_cast<uint4*>(out_v) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+      } else {
+        *reinterpret_cast<uint2*>(out) = make_uint2(wu[0], wu[1]);
+        *reinterpret_cast<uint2*>(out_v) = make_uint2(wv[0], wv[1]);
+      }
     }
   }
 }
@@ -264,8 +327,9 @@ struct GemmParams {
   int kblocks;       // kp / 128
   int nchunks;       // ceil(kblocks / kChunkBlocks)
   int nmod;
+  int t0;            // first modulus of this launch (units cover t0 ..)
   int tiles_m, tiles_n;
-  int total_units;   // nmod * nchunks * tiles_m * tiles_n
+  int total_units;   // moduli of the launch * nchunks * tiles
   int* R;            // accumulated residues [nmod][nb][m] (int32)
   int* status;       // set to 1 when a bounded wait gave up
   const int* active; // CTA-pair kernel: list of tiles to compute (fill mode), or null = all
@@ -287,7 +351,7 @@ __device__ __forceinline__ Unit decode_unit(int u, const GemmParams& g) {
   r.tm = tile % g.tiles_m;
   r.tn = tile / g.tiles_m;
   r.c = rest % g.nchunks;
-  r.t = rest / g.nchunks;
+  r.t = g.t0 + rest / g.nchunks;
   return r;
 }
 
@@ -546,7 +610,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     tm = tile % g.tiles_m;
     tn = tile / g.tiles_m;
     c = rest % g.nchunks;
-    t = rest / g.nchunks;
+    t = g.t0 + rest / g.nchunks;
   };
 
   bool aborted = false;
@@ -835,66 +899,156 @@ bool ozaki_supported(const GemmProblem& p) {
 }
 
 namespace {
-template <typename TIn, bool VEC>
-void launch_slice(int ndig, unsigned grid, cudaStream_t st, const TIn* X, int64_t ld, int64_t len,
-                  int rows, int64_t kp, const int* sig, int mode, int s_sign, int8_t* res,
-                  int64_t stride, const oz::SliceConsts& sc) {
-  using namespace oz;
-  if (ndig <= 3)
-    oz_slice<TIn, VEC, 3><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
-                                                 stride, sc);
-  else if (ndig == 4)
-    oz_slice<TIn, VEC, 4><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
-                                                 stride, sc);
-  else
-    oz_slice<TIn, VEC, 5><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
-                                                 stride, sc);
+// Reals per slicing thread: 8 by default (more resident warps), 16 with
+// SPLAB_OZAKI_SLICE_EL=16.
+int slice_elems() {
+  static const int el = [] {
+    const char* v = std::getenv("SPLAB_OZAKI_SLICE_EL");
+    return (v && std::atoi(v) == 16) ? 16 : 8;
+  }();
+  return el;
 }
 
+template <typename TIn, bool VEC, int EL>
+void launch_slice_el(int ndig, unsigned grid, cudaStream_t st, const TIn* X, int64_t ld,
+                     int64_t len, int rows, int64_t kp, const int* sig, int mode, int s_sign,
+                     int8_t* res, int64_t stride, const oz::SliceConsts& sc, int t0, int t1) {
+  using namespace oz;
+  if (ndig <= 3)
+    oz_slice<TIn, VEC, 3, EL><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
+                                                     stride, sc, t0, t1);
+  else if (ndig == 4)
+    oz_slice<TIn, VEC, 4, EL><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
+                                                     stride, sc, t0, t1);
+  else
+    oz_slice<TIn, VEC, 5, EL><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
+                                                     stride, sc, t0, t1);
+}
+
+template <typename TIn, bool VEC>
+void launch_slice(int ndig, cudaStream_t st, const TIn* X, int64_t ld, int64_t len, int rows,
+                  int64_t kp, const int* sig, int mode, int s_sign, int8_t* res, int64_t stride,
+                  const oz::SliceConsts& sc, int t0, int t1) {
+  const int el = slice_elems();
+  const unsigned grid = unsigned((int64_t(rows) * (kp / el) + 255) / 256);
+  if (el == 16)
+    launch_slice_el<TIn, VEC, 16>(ndig, grid, st, X, ld, len, rows, kp, sig, mode, s_sign, res,
+                                  stride, sc, t0, t1);
+  else
+    launch_slice_el<TIn, VEC, 8>(ndig, grid, st, X, ld, len, rows, kp, sig, mode, s_sign, res,
+                                 stride, sc, t0, t1);
+}
+
+// Row scale exponents of both operands.
+template <typename TIn>
+void scale_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
+                    int* sigA, int* sigB, cudaStream_t st) {
+  using namespace oz;
+  const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in real elements
+  const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
+  oz_row_scale<TIn><<<L.rowsA, 256, 0, st>>>(static_cast<const TIn*>(p.A), ldA, L.K2, L.rowsA,
+                                             crt.q_bits, sigA);
+  oz_row_scale<TIn><<<L.rowsB, 256, 0, st>>>(static_cast<const TIn*>(p.B), ldB, L.K2, L.rowsB,
+                                             crt.q_bits, sigB);
+}
+
+// Residues of moduli t0 .. t1-1 of both operands.
 template <typename TIn>
 void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
-                    int* sigA, int* sigB, int8_t* resA, int8_t* resB, cudaStream_t st) {
+                    const int* sigA, const int* sigB, int8_t* resA, int8_t* resB, int t0, int t1,
+                    cudaStream_t st) {
   using namespace oz;
   const TIn* A = static_cast<const TIn*>(p.A);
   const TIn* B = static_cast<const TIn*>(p.B);
   const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in real elements
   const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
-  oz_row_scale<TIn><<<L.rowsA, 256, 0, st>>>(A, ldA, L.K2, L.rowsA, crt.q_bits, sigA);
-  oz_row_scale<TIn><<<L.rowsB, 256, 0, st>>>(B, ldB, L.K2, L.rowsB, crt.q_bits, sigB);
   SliceConsts sc{};
   sc.n = L.nmod;
+  sc.p0 = float(crt.p[0]);
   for (int t = 0; t < L.nmod; ++t) {
     const int pt = crt.p[t];
-    sc.p[t] = float(pt);
-    sc.inv_p[t] = 1.0f / float(pt);
+    sc.neg_p[t] = f2_pack(-float(pt), -float(pt));
+    sc.inv_p[t] = f2_pack(1.0f / float(pt), 1.0f / float(pt));
     long long w = 1;
     for (int i = 0; i < 4; ++i) {
       w = (w * 8192) % pt;  // 2^(13 (i+1)) mod p
-      const long long c = w > pt / 2 ? w - pt : w;
-      sc.c[t][i] = float(c);
+      const float c = float(w > pt / 2 ? w - pt : w);
+      sc.c[t][i] = f2_pack(c, c);
     }
   }
   // digits of 13 bits covering |x| < 2^(Q+1)
   const int ndig = crt.q_bits + 1 <= 39 ? 3 : (crt.q_bits + 1 <= 52 ? 4 : 5);
-  const int64_t groups = L.kp / 16;
-  const unsigned gridA = unsigned((int64_t(L.rowsA) * groups + 255) / 256);
-  const unsigned gridB = unsigned((int64_t(L.rowsB) * groups + 255) / 256);
   const int vec_elems = 16 / int(sizeof(TIn));
   const bool vecA = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (ldA % vec_elems == 0);
   const bool vecB = (reinterpret_cast<uintptr_t>(B) % 16 == 0) && (ldB % vec_elems == 0);
   const int s_sign = p.opA == 2 ? -1 : 1;
+  const int64_t strideA = int64_t(L.rowsA) * L.kp, strideB = int64_t(L.nb) * L.kp;
   if (vecA)
-    launch_slice<TIn, true>(ndig, gridA, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA,
-                            int64_t(L.rowsA) * L.kp, sc);
+    launch_slice<TIn, true>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA, strideA, sc,
+                            t0, t1);
   else
-    launch_slice<TIn, false>(ndig, gridA, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA,
-                             int64_t(L.rowsA) * L.kp, sc);
+    launch_slice<TIn, false>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA, strideA,
+                             sc, t0, t1);
   if (vecB)
-    launch_slice<TIn, true>(ndig, gridB, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0,
-                            s_sign, resB, int64_t(L.nb) * L.kp, sc);
+    launch_slice<TIn, true>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0, s_sign,
+                            resB, strideB, sc, t0, t1);
   else
-    launch_slice<TIn, false>(ndig, gridB, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0,
-                             s_sign, resB, int64_t(L.nb) * L.kp, sc);
+    launch_slice<TIn, false>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0, s_sign,
+                             resB, strideB, sc, t0, t1);
+}
+
+// Side streams of the modulus-group pipeline (per device): residues of group
+// g + 1 are produced on `lo` while the GEMM of group g runs on `hi` (highest
+// priority, so that its persistent CTAs are placed first and the slicing
+// blocks fill the registers and issue slots the GEMM leaves free).
+struct PipeStreams {
+  cudaStream_t hi = nullptr, lo = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_done = nullptr, ev_sliced[oz::kMaxModuli] = {};
+  std::mutex mu;  // one enqueue sequence at a time
+  bool ok = false;
+};
+
+PipeStreams* pipe_streams() {
+  static PipeStreams per_dev[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  PipeStreams& ps = per_dev[dev];
+  static std::mutex init_mu;
+  std::lock_guard<std::mutex> lk(init_mu);
+  if (!ps.ok) {
+    int lo_prio = 0, hi_prio = 0;
+    bool good = cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio) == cudaSuccess &&
+                cudaStreamCreateWithPriority(&ps.hi, cudaStreamNonBlocking, hi_prio) ==
+                    cudaSuccess &&
+                cudaStreamCreateWithPriority(&ps.lo, cudaStreamNonBlocking, lo_prio) ==
+                    cudaSuccess &&
+                cudaEventCreateWithFlags(&ps.ev_start, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&ps.ev_done, cudaEventDisableTiming) == cudaSuccess;
+    for (int g = 0; good && g < oz::kMaxModuli; ++g)
+      good = cudaEventCreateWithFlags(&ps.ev_sliced[g], cudaEventDisableTiming) == cudaSuccess;
+    if (!good) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    ps.ok = true;
+  }
+  return &ps;
+}
+
+// Number of modulus groups. Default 1: overlapping the slicing of one group
+// with the GEMM of the previous one measured slower on B200 (both phases
+// draw on L2 bandwidth; the slicing ran at half speed beside the GEMM).
+// SPLAB_OZAKI_GROUPS = 2 .. number of moduli enables the pipeline.
+int modulus_groups(const oz::Layout& L) {
+  int g = 1;
+  if (const char* v = std::getenv("SPLAB_OZAKI_GROUPS")) {
+    const int f = std::atoi(v);
+    if (f > 0) g = f;
+  }
+  return std::max(1, std::min(g, L.nmod));
 }
 }  // namespace
 
@@ -916,23 +1070,31 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
   int* status = reinterpret_cast<int*>(w + L.off_status);
 
   cudaError_t e;
+  const bool dbl = dtype_is_double(p.dtype);
   phase_mark(0, false, st);
   if (p.k > 0) {
-    if (dtype_is_double(p.dtype))
-      slice_operands<double>(L, crt, p, cplx, sigA, sigB, resA, resB, st);
+    if (dbl)
+      scale_operands<double>(L, crt, p, cplx, sigA, sigB, st);
     else
-      slice_operands<float>(L, crt, p, cplx, sigA, sigB, resA, resB, st);
+      scale_operands<float>(L, crt, p, cplx, sigA, sigB, st);
   } else {
     cudaMemsetAsync(sigA, 0, sizeof(int) * L.rowsA, st);
     cudaMemsetAsync(sigB, 0, sizeof(int) * L.rowsB, st);
   }
   cudaMemsetAsync(R, 0, sizeof(int) * size_t(L.nmod) * L.nb * L.rowsA, st);
   cudaMemsetAsync(status, 0, sizeof(int), st);
-  phase_mark(0, true, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-
-  phase_mark(1, false, st);
-  if (p.k > 0) {
+  if (p.k <= 0) {
+    phase_mark(0, true, st);
+    phase_mark(1, false, st);
+    phase_mark(1, true, st);
+  } else {
+    auto slice = [&](int t0, int t1, cudaStream_t s) {
+      if (dbl)
+        slice_operands<double>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, s);
+      else
+        slice_operands<float>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, s);
+    };
     CUtensorMap mapA, mapB;
     if (!make_map(&mapA, resA, L.kp, int64_t(L.nmod) * L.rowsA, BM) ||
         !make_map(&mapB, resB, L.kp, int64_t(L.nmod) * L.nb, BN))
@@ -961,6 +1123,7 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
     for (int t = 0; t < L.nmod; ++t) g.p[t] = crt.p[t];
     const char* gk = std::getenv("SPLAB_OZAKI_GEMM");
     const bool pair = !(gk && gk[0] == '1');  // "1sm" selects the single-CTA kernel
+    CUtensorMap mapA2, mapB2;
     if (pair) {
       g.tiles_m = (L.rowsA + 255) / 256;
       g.tiles_n = (L.nb + 255) / 256;
@@ -1014,36 +1177,76 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
                              GEMM2_SMEM);
         attr2 = true;
       }
-      CUtensorMap mapA2, mapB2;
       if (!make_map(&mapA2, resA, L.kp, int64_t(L.nmod) * L.rowsA, 128) ||
           !make_map(&mapB2, resB, L.kp, int64_t(L.nmod) * L.nb, 128))
         return cudaErrorNotSupported;
-      const int pairs = std::max(1, std::min(g.total_units, sm_count() / 2));
-      cudaLaunchConfig_t cfg{};
-      cfg.gridDim = dim3(unsigned(2 * pairs));
-      cfg.blockDim = dim3(GEMM_THREADS);
-      cfg.dynamicSmemBytes = GEMM2_SMEM;
-      cfg.stream = st;
-      cudaLaunchAttribute at[1];
-      at[0].id = cudaLaunchAttributeClusterDimension;
-      at[0].val.clusterDim.x = 2;
-      at[0].val.clusterDim.y = 1;
-      at[0].val.clusterDim.z = 1;
-      cfg.attrs = at;
-      cfg.numAttrs = 1;
-      e = cudaLaunchKernelEx(&cfg, oz_gemm_pair, mapA2, mapB2, g);
-      if (e != cudaSuccess) return e;
-    } else {
+    }
+    const int units_per_mod = g.total_units / g.nmod;
+    // the INT8 GEMM over moduli t0 .. t1-1 on stream s
+    auto launch_gemm = [&](int t0, int t1, cudaStream_t s) -> cudaError_t {
+      GemmParams gg = g;
+      gg.t0 = t0;
+      gg.total_units = (t1 - t0) * units_per_mod;
+      if (pair) {
+        const int pairs = std::max(1, std::min(gg.total_units, sm_count() / 2));
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(unsigned(2 * pairs));
+        cfg.blockDim = dim3(GEMM_THREADS);
+        cfg.dynamicSmemBytes = GEMM2_SMEM;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, oz_gemm_pair, mapA2, mapB2, gg);
+      }
       static bool attr = false;
       if (!attr) {
         cudaFuncSetAttribute(oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
         attr = true;
       }
-      const int grid = std::min(g.total_units, sm_count());
-      oz_gemm<<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(mapA, mapB, g);
+      const int grid = std::min(gg.total_units, sm_count());
+      oz_gemm<<<grid, GEMM_THREADS, GEMM_SMEM, s>>>(mapA, mapB, gg);
+      return cudaGetLastError();
+    };
+
+    const int groups = modulus_groups(L);
+    PipeStreams* ps = groups > 1 ? pipe_streams() : nullptr;
+    if (!ps) {
+      slice(0, L.nmod, st);
+      phase_mark(0, true, st);
+      phase_mark(1, false, st);
+      phase_mark(3, false, st);
+      if ((e = launch_gemm(0, L.nmod, st)) != cudaSuccess) return e;
+      phase_mark(3, true, st);
+      phase_mark(1, true, st);
+    } else {
+      // modulus-group pipeline: slicing of group i + 1 (stream lo) overlaps
+      // the GEMM of group i (stream hi); the caller's stream joins at the end
+      std::lock_guard<std::mutex> lk(ps->mu);
+      auto bounds = [&](int i) { return i * L.nmod / groups; };
+      if ((e = cudaEventRecord(ps->ev_start, st)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(ps->lo, ps->ev_start, 0)) != cudaSuccess) return e;
+      for (int i = 0; i < groups; ++i) {
+        slice(bounds(i), bounds(i + 1), ps->lo);
+        if ((e = cudaEventRecord(ps->ev_sliced[i], ps->lo)) != cudaSuccess) return e;
+      }
+      phase_mark(0, true, ps->lo);
+      for (int i = 0; i < groups; ++i) {
+        if ((e = cudaStreamWaitEvent(ps->hi, ps->ev_sliced[i], 0)) != cudaSuccess) return e;
+        if (i == 0) phase_mark(1, false, ps->hi);
+        phase_mark(3 + i, false, ps->hi);
+        if ((e = launch_gemm(bounds(i), bounds(i + 1), ps->hi)) != cudaSuccess) return e;
+        phase_mark(3 + i, true, ps->hi);
+      }
+      phase_mark(1, true, ps->hi);
+      if ((e = cudaEventRecord(ps->ev_done, ps->hi)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(st, ps->ev_done, 0)) != cudaSuccess) return e;
     }
   }
-  phase_mark(1, true, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
 
   phase_mark(2, false, st);
