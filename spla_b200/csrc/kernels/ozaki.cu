@@ -939,24 +939,26 @@ void launch_slice(int ndig, cudaStream_t st, const TIn* X, int64_t ld, int64_t l
                                  stride, sc, t0, t1);
 }
 
-// Row scale exponents of both operands.
+// Row scale exponents of A (which & 1) and B (which & 2).
 template <typename TIn>
 void scale_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
-                    int* sigA, int* sigB, cudaStream_t st) {
+                    int* sigA, int* sigB, int which, cudaStream_t st) {
   using namespace oz;
   const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in real elements
   const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
-  oz_row_scale<TIn><<<L.rowsA, 256, 0, st>>>(static_cast<const TIn*>(p.A), ldA, L.K2, L.rowsA,
-                                             crt.q_bits, sigA);
-  oz_row_scale<TIn><<<L.rowsB, 256, 0, st>>>(static_cast<const TIn*>(p.B), ldB, L.K2, L.rowsB,
-                                             crt.q_bits, sigB);
+  if (which & 1)
+    oz_row_scale<TIn><<<L.rowsA, 256, 0, st>>>(static_cast<const TIn*>(p.A), ldA, L.K2,
+                                               L.rowsA, crt.q_bits, sigA);
+  if (which & 2)
+    oz_row_scale<TIn><<<L.rowsB, 256, 0, st>>>(static_cast<const TIn*>(p.B), ldB, L.K2,
+                                               L.rowsB, crt.q_bits, sigB);
 }
 
-// Residues of moduli t0 .. t1-1 of both operands.
+// Residues of moduli t0 .. t1-1 of A (which & 1) and B (which & 2).
 template <typename TIn>
 void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
                     const int* sigA, const int* sigB, int8_t* resA, int8_t* resB, int t0, int t1,
-                    cudaStream_t st) {
+                    int which, cudaStream_t st) {
   using namespace oz;
   const TIn* A = static_cast<const TIn*>(p.A);
   const TIn* B = static_cast<const TIn*>(p.B);
@@ -983,16 +985,16 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
   const bool vecB = (reinterpret_cast<uintptr_t>(B) % 16 == 0) && (ldB % vec_elems == 0);
   const int s_sign = p.opA == 2 ? -1 : 1;
   const int64_t strideA = int64_t(L.rowsA) * L.kp, strideB = int64_t(L.nb) * L.kp;
-  if (vecA)
+  if ((which & 1) && vecA)
     launch_slice<TIn, true>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA, strideA, sc,
                             t0, t1);
-  else
+  else if (which & 1)
     launch_slice<TIn, false>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA, strideA,
                              sc, t0, t1);
-  if (vecB)
+  if ((which & 2) && vecB)
     launch_slice<TIn, true>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0, s_sign,
                             resB, strideB, sc, t0, t1);
-  else
+  else if (which & 2)
     launch_slice<TIn, false>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0, s_sign,
                              resB, strideB, sc, t0, t1);
 }
@@ -1003,7 +1005,8 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
 // blocks fill the registers and issue slots the GEMM leaves free).
 struct PipeStreams {
   cudaStream_t hi = nullptr, lo = nullptr;
-  cudaEvent_t ev_start = nullptr, ev_done = nullptr, ev_sliced[oz::kMaxModuli] = {};
+  cudaEvent_t ev_start = nullptr, ev_done = nullptr, ev_scaled = nullptr,
+              ev_sliced[oz::kMaxModuli] = {};
   std::mutex mu;  // one enqueue sequence at a time
   bool ok = false;
 };
@@ -1026,7 +1029,8 @@ PipeStreams* pipe_streams() {
                 cudaStreamCreateWithPriority(&ps.lo, cudaStreamNonBlocking, lo_prio) ==
                     cudaSuccess &&
                 cudaEventCreateWithFlags(&ps.ev_start, cudaEventDisableTiming) == cudaSuccess &&
-                cudaEventCreateWithFlags(&ps.ev_done, cudaEventDisableTiming) == cudaSuccess;
+                cudaEventCreateWithFlags(&ps.ev_done, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&ps.ev_scaled, cudaEventDisableTiming) == cudaSuccess;
     for (int g = 0; good && g < oz::kMaxModuli; ++g)
       good = cudaEventCreateWithFlags(&ps.ev_sliced[g], cudaEventDisableTiming) == cudaSuccess;
     if (!good) {
@@ -1071,12 +1075,30 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
 
   cudaError_t e;
   const bool dbl = dtype_is_double(p.dtype);
-  phase_mark(0, false, st);
-  if (p.k > 0) {
+  const int groups = modulus_groups(L);
+  // Large problems use the side streams: the row norms of B (a pure read)
+  // run beside the slicing of A (arithmetic-bound), and with groups > 1 the
+  // modulus-group pipeline below.
+  const bool big = double(L.rowsA + L.rowsB) * double(L.K2) * dtype_bytes(p.dtype) /
+                       (cplx ? 2.0 : 1.0) >= 5e8;
+  PipeStreams* ps = (p.k > 0 && (groups > 1 || big)) ? pipe_streams() : nullptr;
+  std::unique_lock<std::mutex> lk;
+  if (ps) lk = std::unique_lock<std::mutex>(ps->mu);
+  auto scale = [&](int which, cudaStream_t s) {
     if (dbl)
-      scale_operands<double>(L, crt, p, cplx, sigA, sigB, st);
+      scale_operands<double>(L, crt, p, cplx, sigA, sigB, which, s);
     else
-      scale_operands<float>(L, crt, p, cplx, sigA, sigB, st);
+      scale_operands<float>(L, crt, p, cplx, sigA, sigB, which, s);
+  };
+  phase_mark(0, false, st);
+  if (p.k > 0 && ps) {
+    if ((e = cudaEventRecord(ps->ev_start, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ps->lo, ps->ev_start, 0)) != cudaSuccess) return e;
+    scale(2, ps->lo);
+    if ((e = cudaEventRecord(ps->ev_scaled, ps->lo)) != cudaSuccess) return e;
+    scale(1, st);
+  } else if (p.k > 0) {
+    scale(3, st);
   } else {
     cudaMemsetAsync(sigA, 0, sizeof(int) * L.rowsA, st);
     cudaMemsetAsync(sigB, 0, sizeof(int) * L.rowsB, st);
@@ -1089,11 +1111,11 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
     phase_mark(1, false, st);
     phase_mark(1, true, st);
   } else {
-    auto slice = [&](int t0, int t1, cudaStream_t s) {
+    auto slice = [&](int t0, int t1, int which, cudaStream_t s) {
       if (dbl)
-        slice_operands<double>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, s);
+        slice_operands<double>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, which, s);
       else
-        slice_operands<float>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, s);
+        slice_operands<float>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, which, s);
     };
     CUtensorMap mapA, mapB;
     if (!make_map(&mapA, resA, L.kp, int64_t(L.nmod) * L.rowsA, BM) ||
@@ -1213,10 +1235,14 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
       return cudaGetLastError();
     };
 
-    const int groups = modulus_groups(L);
-    PipeStreams* ps = groups > 1 ? pipe_streams() : nullptr;
-    if (!ps) {
-      slice(0, L.nmod, st);
+    if (groups == 1 || !ps) {
+      if (ps) {  // A on the caller's stream, B once its row norms are done
+        slice(0, L.nmod, 1, st);
+        if ((e = cudaStreamWaitEvent(st, ps->ev_scaled, 0)) != cudaSuccess) return e;
+        slice(0, L.nmod, 2, st);
+      } else {
+        slice(0, L.nmod, 3, st);
+      }
       phase_mark(0, true, st);
       phase_mark(1, false, st);
       phase_mark(3, false, st);
@@ -1226,12 +1252,13 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
     } else {
       // modulus-group pipeline: slicing of group i + 1 (stream lo) overlaps
       // the GEMM of group i (stream hi); the caller's stream joins at the end
-      std::lock_guard<std::mutex> lk(ps->mu);
       auto bounds = [&](int i) { return i * L.nmod / groups; };
+      // lo has the B row norms queued; it also needs A's row norms and the
+      // memsets of the caller's stream
       if ((e = cudaEventRecord(ps->ev_start, st)) != cudaSuccess) return e;
       if ((e = cudaStreamWaitEvent(ps->lo, ps->ev_start, 0)) != cudaSuccess) return e;
       for (int i = 0; i < groups; ++i) {
-        slice(bounds(i), bounds(i + 1), ps->lo);
+        slice(bounds(i), bounds(i + 1), 3, ps->lo);
         if ((e = cudaEventRecord(ps->ev_sliced[i], ps->lo)) != cudaSuccess) return e;
       }
       phase_mark(0, true, ps->lo);
