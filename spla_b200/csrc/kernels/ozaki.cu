@@ -541,11 +541,20 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 //   empty[s] (both):     commit of the MMAs, multicast to the pair
 //   accf[b]  (both):     commit after a tile's last k-block, multicast
 //   acce[b]  (even CTA): 256 epilogue threads of both CTAs, remote arrivals
-constexpr int STAGES2 = 6;
+// NT = 1: pair tile 256 x 256, two accumulator buffers (2 x 256 TMEM
+// columns), 6 stages. NT = 2: pair tile 256 x 512 (two MMAs of N = 256 per
+// k-step on one A tile: a quarter less L2 -> SMEM traffic per operation), one
+// accumulator buffer of 512 columns (drained once per unit of 976 k-blocks),
+// 4 stages.
 constexpr int A_STAGE2 = 128 * BKB;  // 16 KiB per CTA
-constexpr int B_STAGE2 = 128 * BKB;  // 16 KiB per CTA
-constexpr int STAGE2_BYTES = A_STAGE2 + B_STAGE2;
-constexpr int GEMM2_SMEM = STAGES2 * STAGE2_BYTES + 1024 + 1024;
+constexpr int B_HALF2 = 128 * BKB;   // 16 KiB per CTA and N = 256 half
+template <int NT>
+struct PairCfg {
+  static constexpr int STAGES = NT == 1 ? 6 : 4;
+  static constexpr int STAGE = A_STAGE2 + NT * B_HALF2;
+  static constexpr int SMEM = STAGES * STAGE + 1024 + 1024;
+  static constexpr int NBUF = NT == 1 ? 2 : 1;
+};
 constexpr uint32_t kIdescI8Pair = (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(256 >> 3) << 17) |
                                   (uint32_t(256 >> 4) << 24);
 
@@ -558,9 +567,13 @@ __device__ __forceinline__ void umma_i8_pair(uint32_t tmem_d, uint64_t adesc, ui
       "l"(adesc), "l"(bdesc), "r"(kIdescI8Pair), "r"(accumulate)
       : "memory");
 }
+template <int NT>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     oz_gemm_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  const __grid_constant__ GemmParams g) {
+  using P = PairCfg<NT>;
+  constexpr int STAGES2 = P::STAGES;
+  constexpr int STAGE2_BYTES = P::STAGE;
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw_addr = smem_u32(smem_raw);
   const uint32_t base = (raw_addr + 1023u) & ~1023u;
@@ -624,7 +637,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
       unit_of(u, t, c, tm, tn);
       const int kb0 = c * kChunkBlocks, kb1 = min(g.kblocks, kb0 + kChunkBlocks);
       const int arow = t * g.m + tm * 256 + int(rank) * 128;
-      const int brow = t * g.nb + tn * 256 + int(rank) * 128;
+      const int brow = t * g.nb + tn * (256 * NT) + int(rank) * 128;
       for (int kb = kb0; kb < kb1; ++kb) {
         if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort, g.wait_limit_ns)) {
           ok = false;
@@ -634,7 +647,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         if (rank == 0) mbar_arrive_expect_tx(full_bar(stage), 2 * STAGE2_BYTES);
         const uint32_t sa = base + stage * STAGE2_BYTES;
         tma_load_2d_pair(sa, &tmA, kb * BKB, arow, fb);
-        tma_load_2d_pair(sa + A_STAGE2, &tmB, kb * BKB, brow, fb);
+#pragma unroll
+        for (int h = 0; h < NT; ++h)
+          tma_load_2d_pair(sa + A_STAGE2 + h * B_HALF2, &tmB, kb * BKB, brow + h * 256, fb);
         if (++stage == STAGES2) {
           stage = 0;
           phase ^= 1u;
@@ -667,9 +682,14 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         tc_fence_after();
         const uint32_t sa = base + stage * STAGE2_BYTES;
 #pragma unroll
-        for (int kk = 0; kk < BKB / 32; ++kk)
-          umma_i8_pair(d, umma_desc_sw128(sa + kk * 32), umma_desc_sw128(sa + A_STAGE2 + kk * 32),
-                       (kb > kb0 || kk > 0) ? 1u : 0u);
+        for (int kk = 0; kk < BKB / 32; ++kk) {
+          const uint64_t adesc = umma_desc_sw128(sa + kk * 32);
+#pragma unroll
+          for (int h = 0; h < NT; ++h)
+            umma_i8_pair(d + uint32_t(h * 256),
+                         adesc, umma_desc_sw128(sa + A_STAGE2 + h * B_HALF2 + kk * 32),
+                         (kb > kb0 || kk > 0) ? 1u : 0u);
+        }
         umma_commit_pair(empty_bar(stage));
         if (++stage == STAGES2) {
           stage = 0;
@@ -679,7 +699,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
       if (!ok) break;
       umma_commit_pair(accf_bar(accb));
       acc_phase[accb] ^= 1u;
-      accb ^= 1;
+      accb = (accb + 1) % P::NBUF;
     }
     if (!ok) {
       asm volatile(
@@ -703,9 +723,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
       tc_fence_after();
       const int p = g.p[t];
       const int i = tm * 256 + row;
-      const int j0 = tn * 256;
+      const int j0 = tn * (256 * NT);
       int* Rt = g.R + int64_t(t) * g.nb * g.m;
-      for (int c0 = 0; c0 < 256; c0 += 32) {
+      for (int c0 = 0; c0 < 256 * NT; c0 += 32) {
         uint32_t v[32];
         tmem_ld32(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(accb * 256 + c0), v);
         if (i < g.m) {
@@ -723,7 +743,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
       tc_fence_before();
       mbar_arrive_cluster(map_to_rank(acce_bar(accb), 0));
       acc_phase[accb] ^= 1u;
-      accb ^= 1;
+      accb = (accb + 1) % P::NBUF;
     }
   }
 
@@ -1146,9 +1166,16 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
     const char* gk = std::getenv("SPLAB_OZAKI_GEMM");
     const bool pair = !(gk && gk[0] == '1');  // "1sm" selects the single-CTA kernel
     CUtensorMap mapA2, mapB2;
+    // pair tile 256 x 512 when B has at least 512 rows (SPLAB_OZAKI_NT=1|2 overrides)
+    int nt = L.nb >= 512 ? 2 : 1;
+    if (const char* v = std::getenv("SPLAB_OZAKI_NT")) {
+      if (v[0] == '1') nt = 1;
+      if (v[0] == '2') nt = 2;
+    }
+    const int tile_nb = 256 * nt;
     if (pair) {
       g.tiles_m = (L.rowsA + 255) / 256;
-      g.tiles_n = (L.nb + 255) / 256;
+      g.tiles_n = (L.nb + tile_nb - 1) / tile_nb;
       g.total_units = g.nmod * g.nchunks * g.tiles_m * g.tiles_n;
       if (p.fill_mode != 0) {
         // compute only the pair tiles that cover an element the reconstruction
@@ -1158,7 +1185,7 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
         for (int tn = 0; tn < g.tiles_n; ++tn)
           for (int tm = 0; tm < g.tiles_m; ++tm) {
             const int64_t r0 = int64_t(tm) * 256, r1 = std::min<int64_t>(r0 + 256, L.rowsA);
-            const int64_t b0 = int64_t(tn) * 256, b1 = std::min<int64_t>(b0 + 256, L.nb);
+            const int64_t b0 = int64_t(tn) * tile_nb, b1 = std::min<int64_t>(b0 + tile_nb, L.nb);
             // complex columns covered by the B rows (u rows j, v rows n + j)
             int64_t cr[2][2] = {{0, 0}, {0, 0}};
             int ncr = 0;
@@ -1195,8 +1222,10 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
       }
       static bool attr2 = false;
       if (!attr2) {
-        cudaFuncSetAttribute(oz_gemm_pair, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             GEMM2_SMEM);
+        cudaFuncSetAttribute(oz_gemm_pair<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             PairCfg<1>::SMEM);
+        cudaFuncSetAttribute(oz_gemm_pair<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             PairCfg<2>::SMEM);
         attr2 = true;
       }
       if (!make_map(&mapA2, resA, L.kp, int64_t(L.nmod) * L.rowsA, 128) ||
@@ -1214,7 +1243,7 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(unsigned(2 * pairs));
         cfg.blockDim = dim3(GEMM_THREADS);
-        cfg.dynamicSmemBytes = GEMM2_SMEM;
+        cfg.dynamicSmemBytes = nt == 2 ? PairCfg<2>::SMEM : PairCfg<1>::SMEM;
         cfg.stream = s;
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeClusterDimension;
@@ -1223,7 +1252,8 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
         at[0].val.clusterDim.z = 1;
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, oz_gemm_pair, mapA2, mapB2, gg);
+        return nt == 2 ? cudaLaunchKernelEx(&cfg, oz_gemm_pair<2>, mapA2, mapB2, gg)
+                       : cudaLaunchKernelEx(&cfg, oz_gemm_pair<1>, mapA2, mapB2, gg);
       }
       static bool attr = false;
       if (!attr) {

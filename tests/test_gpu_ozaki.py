@@ -64,6 +64,16 @@ def test_float_dtypes(dt, opA):
     assert oracle.rel_fro(got, ref) <= 1e-6
 
 
+@pytest.mark.parametrize("nt", ["1", "2"])
+def test_pair_tile_widths(nt, monkeypatch):
+    """Both INT8 GEMM tile widths (CTA pair 256 x 256 and 256 x 512) on a
+    problem with partial tiles in both dimensions and two k-chunks."""
+    monkeypatch.setenv("SPLAB_OZAKI_NT", nt)
+    m, n, k = 333, 291, 70000  # real form 333 x 582, 2k = 140000 -> 2 chunks
+    C0, got, ref, ldc = run_ssb(np.complex128, m, n, k, 2)
+    assert oracle.rel_fro(got, ref) <= 1e-14
+
+
 def test_real_double():
     m, n, k = 200, 330, 70000
     C0, got, ref, ldc = run_ssb(np.float64, m, n, k, 1, dist="uniform11")
