@@ -1,0 +1,90 @@
+"""Per-phase timing of one local contraction through the kernel C ABI
+(splab_gemm), device-resident operands, CUDA events on a private stream.
+
+    python -m spla_b200.timing complex128:2:1024:1024:250000 [more specs]
+
+A spec is dtype:path:m:n:k with dtype in {float32, float64, complex64,
+complex128} and path 0 auto, 1 DMMA, 2 Ozaki, 3 3xTF32; the problem is
+C = op(A) B with op = conjugate transpose (complex) or transpose (real),
+Gaussian operands scaled by 1/sqrt(k). One JSON line per spec: total time,
+TFLOP/s and the phase times the path reports (scale/slice, GEMM span,
+reduction or reconstruction, then one entry per GEMM launch).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import json
+import sys
+
+NPHASE = 3 + 16
+
+
+def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: int = 2,
+        moduli: int = 0) -> dict:
+    import torch
+    import spla_b200 as spla
+    L = spla.lib()
+    tdt = getattr(torch, dtype)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    A = torch.randn(m * k, dtype=tdt, device="cuda", generator=g) * (0.5 / k) ** 0.5
+    B = torch.randn(n * k, dtype=tdt, device="cuda", generator=g) * (0.5 / k) ** 0.5
+    C = torch.zeros(m * n, dtype=tdt, device="cuda")
+    op = 2 if A.is_complex() else 1
+    ws_bytes = spla.splab_gemm_workspace_size(dtype, path, op, 0, m, n, k, moduli)
+    ws = torch.empty(max(1, ws_bytes), dtype=torch.uint8, device="cuda")
+    st = torch.cuda.Stream()
+    pev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * NPHASE)]
+    for e in pev:  # torch creates the CUDA event on first record
+        e.record(st)
+    st.synchronize()
+    handles = (ct.c_void_p * (2 * NPHASE))(*[e.cuda_event for e in pev])
+
+    def step():
+        rc = spla.splab_gemm(dtype, path, op, 0, m, n, k, 1.0, A, k, B, k, 0.0, C, m,
+                             moduli=moduli, workspace=ws, workspace_bytes=ws_bytes,
+                             stream=st.cuda_stream)
+        if rc != 0:
+            raise RuntimeError(L.splab_status_string(rc).decode())
+
+    with torch.cuda.stream(st):
+        for _ in range(warmup):
+            step()
+        st.synchronize()
+        tot = [0.0] * NPHASE
+        ms = 0.0
+        for _ in range(steps):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            for e in pev:
+                e.record(st)  # phases a path does not have read as zero
+            L.splab_set_phase_events(handles, NPHASE)
+            try:
+                t0.record(st)
+                step()
+                t1.record(st)
+            finally:
+                L.splab_set_phase_events(None, 0)
+            st.synchronize()
+            ms += t0.elapsed_time(t1)
+            for p in range(NPHASE):
+                tot[p] += pev[2 * p].elapsed_time(pev[2 * p + 1])
+    ms /= steps
+    ph = [x / steps for x in tot]
+    flops = (8.0 if A.is_complex() else 2.0) * m * n * k
+    return {"dtype": dtype, "path": path,
+            "resolved_path": L.splab_gemm_path(spla._dtype_of(dtype=dtype), path, op, 0, m, n, k),
+            "m": m, "n": n, "k": k, "ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 1),
+            "phases_ms": [round(x, 3) for x in ph[:3]],
+            "gemm_launch_ms": [round(x, 3) for x in ph[3:] if x > 0.05],
+            "workspace_GB": round(ws_bytes / 1e9, 2)}
+
+
+def main(argv):
+    for spec in argv:
+        d, p, m, n, k = spec.split(":")
+        print(json.dumps(run(d, int(p), int(m), int(n), int(k))), flush=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or ["complex128:2:1024:1024:20000"])
