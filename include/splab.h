@@ -142,6 +142,16 @@ typedef struct splab_problem {
 
 SPLAB_API int splab_batch_create(int dtype, int count, const splab_problem *problems,
                                  void **plan, size_t *workspaceBytes);
+/* The same batch on a chosen path: SPLAB_PATH_DMMA or SPLAB_PATH_AUTO give the
+ * grouped FP64 launch above; SPLAB_PATH_OZAKI (any dtype) and
+ * SPLAB_PATH_TF32X3 (float dtypes) run the instances one after another on one
+ * stream with one shared workspace (the largest instance's), the sequence
+ * captured in a CUDA graph on the second run and replayed afterwards.
+ * SPLAB_ERR_UNSUPPORTED when an instance's dtype or op pair is not handled by
+ * the path (the tensor-core paths take op(A) in {T, C}, op(B) = N). */
+SPLAB_API int splab_batch_create_path(int dtype, int path, int count,
+                                      const splab_problem *problems, void **plan,
+                                      size_t *workspaceBytes);
 /* Run (and on the first call tune + capture) the batch on `stream`; workspace
  * must hold workspaceBytes of device memory and stay the same between runs
  * (a different pointer triggers a new capture). */
@@ -151,6 +161,9 @@ SPLAB_API int splab_batch_run(void *plan, void *workspace, size_t workspaceBytes
  * tuned; arrays of at least 32 entries. */
 SPLAB_API int splab_batch_info(void *plan, int64_t *kChunk, int *nCandidates, int64_t *candidates,
                                double *tuningMs);
+/* Synchronise `stream` and report SPLAB_ERR_TIMEOUT when a bounded device wait
+ * gave up in the last run of a tensor-core batch (SPLAB_OK otherwise). */
+SPLAB_API int splab_batch_check(void *plan, void *workspace, void *stream);
 SPLAB_API int splab_batch_destroy(void *plan);
 
 /*

@@ -395,16 +395,20 @@ class _Problem(ct.Structure):
 
 
 class Batch:
-    """A batch of independent local GEMMs of one dtype and op pair, run as one
-    persistent grouped launch replayed from a CUDA graph (splab_batch_*).
+    """A batch of independent local GEMMs of one dtype and op pair
+    (splab_batch_*). path PATH_DMMA (default): one persistent grouped launch
+    replayed from a CUDA graph; PATH_OZAKI / PATH_TF32X3: the instances in
+    sequence on one stream with a shared workspace, replayed from a CUDA graph
+    after the first run.
 
     problems: list of dicts with keys opA, opB, m, n, k, A, lda, B, ldb, C, ldc,
     alpha, beta (buffers as device tensors or integer addresses)."""
 
-    def __init__(self, dtype, problems):
+    def __init__(self, dtype, problems, path=None):
         L = lib()
-        L.splab_batch_create.argtypes = [ct.c_int, ct.c_int, ct.c_void_p, ct.POINTER(ct.c_void_p),
-                                         ct.POINTER(ct.c_size_t)]
+        L.splab_batch_create_path.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_void_p,
+                                              ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_size_t)]
+        L.splab_batch_check.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p]
         L.splab_batch_run.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_size_t, ct.c_int,
                                       ct.c_void_p]
         L.splab_batch_info.argtypes = [ct.c_void_p, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int),
@@ -420,10 +424,13 @@ class Batch:
         self._arr = arr
         self._plan = ct.c_void_p()
         ws = ct.c_size_t()
-        rc = L.splab_batch_create(self.dtype, len(problems), ct.cast(arr, ct.c_void_p),
-                                  ct.byref(self._plan), ct.byref(ws))
+        self.path = PATH_DMMA if path is None else int(path)
+        rc = L.splab_batch_create_path(self.dtype, self.path, len(problems),
+                                       ct.cast(arr, ct.c_void_p), ct.byref(self._plan),
+                                       ct.byref(ws))
         if rc != 0:
-            raise InvalidParameterError(f"splab_batch_create: {L.splab_status_string(rc)}")
+            raise InvalidParameterError(
+                f"splab_batch_create_path: {L.splab_status_string(rc).decode()}")
         self.workspace_bytes = ws.value
 
     def run(self, workspace, stream=0, autotune=True):
@@ -431,6 +438,12 @@ class Batch:
                                    int(bool(autotune)), stream)
         if rc != 0:
             raise GPULaunchError(f"splab_batch_run: {lib().splab_status_string(rc).decode()}")
+
+    def check(self, workspace, stream=0):
+        """Synchronise and raise GPULaunchError if a bounded device wait gave up."""
+        rc = lib().splab_batch_check(self._plan, _addr(workspace)[0], stream)
+        if rc != 0:
+            raise GPULaunchError(f"splab_batch_check: {lib().splab_status_string(rc).decode()}")
 
     def info(self):
         kc, nc = ct.c_int64(), ct.c_int()

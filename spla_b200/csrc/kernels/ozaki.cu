@@ -1019,6 +1019,10 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
                              resB, strideB, sc, t0, t1);
 }
 
+// Side streams may be used by this host thread (off while a batch captures
+// its sequence of contractions into a CUDA graph on one stream).
+thread_local bool t_side_streams = true;
+
 // Side streams of the modulus-group pipeline (per device): residues of group
 // g + 1 are produced on `lo` while the GEMM of group g runs on `hi` (highest
 // priority, so that its persistent CTAs are placed first and the slicing
@@ -1101,7 +1105,8 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
   // modulus-group pipeline below.
   const bool big = double(L.rowsA + L.rowsB) * double(L.K2) * dtype_bytes(p.dtype) /
                        (cplx ? 2.0 : 1.0) >= 5e8;
-  PipeStreams* ps = (p.k > 0 && (groups > 1 || big)) ? pipe_streams() : nullptr;
+  PipeStreams* ps =
+      (p.k > 0 && (groups > 1 || big) && t_side_streams) ? pipe_streams() : nullptr;
   std::unique_lock<std::mutex> lk;
   if (ps) lk = std::unique_lock<std::mutex>(ps->mu);
   auto scale = [&](int which, cudaStream_t s) {
@@ -1335,6 +1340,12 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return cudaSuccess;
 }
+
+int* ozaki_status_ptr(const GemmProblem& p, int moduli, void* ws) {
+  return reinterpret_cast<int*>(static_cast<char*>(ws) + oz::layout_of(p, moduli).off_status);
+}
+
+void ozaki_allow_side_streams(bool allow) { t_side_streams = allow; }
 
 int ozaki_status(const GemmProblem& p, int moduli, void* ws, cudaStream_t st) {
   const oz::Layout L = oz::layout_of(p, moduli);

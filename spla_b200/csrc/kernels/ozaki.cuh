@@ -25,4 +25,11 @@ int ozaki_status(const GemmProblem& prob, int moduli, void* workspace, cudaStrea
 cudaError_t ozaki_gemm(const GemmProblem& prob, int moduli, void* workspace, size_t ws_bytes,
                        cudaStream_t stream);
 
+// Device address of the status word inside the workspace.
+int* ozaki_status_ptr(const GemmProblem& prob, int moduli, void* workspace);
+
+// Whether ozaki_gemm may use its side streams on this host thread (default
+// yes); a batch turns them off while it captures a CUDA graph on one stream.
+void ozaki_allow_side_streams(bool allow);
+
 }  // namespace splab

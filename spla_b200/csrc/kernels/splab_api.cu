@@ -10,6 +10,7 @@
 #include "gemm_dmma.cuh"
 #include "ozaki.cuh"
 #include "tf32x3.cuh"
+#include "batch_seq.cuh"
 
 namespace splab {
 
@@ -123,6 +124,12 @@ __global__ void block_cyclic_info_kernel(int64_t rb, int64_t cb, int64_t gr, int
   o[7] = endCol - gCol;
   o[8] = (gbRow % gr) + (gbCol % gc) * gr;
 }
+
+// A batch plan: the grouped FP64 launch or a tensor-core sequence.
+struct BatchHandle {
+  BatchPlanImpl* grouped = nullptr;
+  SeqBatch* seq = nullptr;
+};
 
 }  // namespace
 }  // namespace splab
@@ -239,7 +246,13 @@ int splab_gemm_dmma_noalloc(int dtype, int opA, int opB, int64_t m, int64_t n, i
 
 int splab_batch_create(int dtype, int count, const splab_problem* problems, void** plan,
                        size_t* workspaceBytes) {
-  if (dtype < 0 || dtype > 3 || count < 1 || !problems || !plan || !workspaceBytes)
+  return splab_batch_create_path(dtype, SPLAB_PATH_DMMA, count, problems, plan, workspaceBytes);
+}
+
+int splab_batch_create_path(int dtype, int path, int count, const splab_problem* problems,
+                            void** plan, size_t* workspaceBytes) {
+  if (dtype < 0 || dtype > 3 || path < 0 || path > 3 || count < 1 || !problems || !plan ||
+      !workspaceBytes)
     return SPLAB_ERR_INVALID;
   std::vector<GemmProblem> probs;
   probs.reserve(count);
@@ -270,26 +283,57 @@ int splab_batch_create(int dtype, int count, const splab_problem* problems, void
     if (p.m > 0 && p.n > 0) probs.push_back(p);
   }
   if (probs.empty()) return SPLAB_ERR_INVALID;
-  BatchPlanImpl* b = batch_create(dtype, probs);
-  *plan = b;
-  *workspaceBytes = batch_workspace(b);
+  auto* h = new BatchHandle();
+  if (path == SPLAB_PATH_OZAKI || path == SPLAB_PATH_TF32X3) {
+    h->seq = seq_batch_create(path, probs);
+    if (!h->seq) {
+      delete h;
+      return SPLAB_ERR_UNSUPPORTED;
+    }
+    *workspaceBytes = seq_batch_workspace(h->seq);
+  } else {
+    h->grouped = batch_create(dtype, probs);
+    *workspaceBytes = batch_workspace(h->grouped);
+  }
+  *plan = h;
   return SPLAB_OK;
 }
 
 int splab_batch_run(void* plan, void* workspace, size_t workspaceBytes, int autotune,
                     void* stream) {
   if (!plan) return SPLAB_ERR_INVALID;
-  BatchPlanImpl* b = static_cast<BatchPlanImpl*>(plan);
-  if (!workspace || workspaceBytes < batch_workspace(b)) return SPLAB_ERR_WORKSPACE;
-  return batch_run(b, workspace, static_cast<cudaStream_t>(stream), autotune != 0) == cudaSuccess
-             ? SPLAB_OK
-             : SPLAB_ERR_LAUNCH;
+  BatchHandle* h = static_cast<BatchHandle*>(plan);
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e;
+  if (h->seq) {
+    if (!workspace || workspaceBytes < seq_batch_workspace(h->seq)) return SPLAB_ERR_WORKSPACE;
+    e = seq_batch_run(h->seq, workspace, st);
+  } else {
+    if (!workspace || workspaceBytes < batch_workspace(h->grouped)) return SPLAB_ERR_WORKSPACE;
+    e = batch_run(h->grouped, workspace, st, autotune != 0);
+  }
+  return e == cudaSuccess ? SPLAB_OK : SPLAB_ERR_LAUNCH;
+}
+
+int splab_batch_check(void* plan, void* workspace, void* stream) {
+  if (!plan) return SPLAB_ERR_INVALID;
+  BatchHandle* h = static_cast<BatchHandle*>(plan);
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return SPLAB_ERR_LAUNCH;
+  if (!h->seq || !workspace) return SPLAB_OK;
+  return seq_batch_status(h->seq, workspace, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
 }
 
 int splab_batch_info(void* plan, int64_t* kChunk, int* nCandidates, int64_t* candidates,
                      double* tuningMs) {
   if (!plan) return SPLAB_ERR_INVALID;
-  const BatchPlanImpl* b = static_cast<const BatchPlanImpl*>(plan);
+  const BatchHandle* h = static_cast<const BatchHandle*>(plan);
+  if (h->seq) {  // no k-chunk to tune: every instance runs its path's own split
+    if (kChunk) *kChunk = 0;
+    if (nCandidates) *nCandidates = 0;
+    return SPLAB_OK;
+  }
+  const BatchPlanImpl* b = h->grouped;
   if (kChunk) *kChunk = batch_kc(b);
   const auto& c = batch_candidates(b);
   const auto& t = batch_tuning(b);
@@ -303,7 +347,11 @@ int splab_batch_info(void* plan, int64_t* kChunk, int* nCandidates, int64_t* can
 }
 
 int splab_batch_destroy(void* plan) {
-  batch_destroy(static_cast<BatchPlanImpl*>(plan));
+  BatchHandle* h = static_cast<BatchHandle*>(plan);
+  if (!h) return SPLAB_OK;
+  if (h->seq) seq_batch_destroy(h->seq);
+  if (h->grouped) batch_destroy(h->grouped);
+  delete h;
   return SPLAB_OK;
 }
 

@@ -698,6 +698,10 @@ cudaError_t tf32x3_gemm(const GemmProblem& p, void* ws, size_t ws_bytes, cudaStr
   return cudaGetLastError();
 }
 
+int* tf32x3_status_ptr(const GemmProblem& p, void* ws) {
+  return reinterpret_cast<int*>(static_cast<char*>(ws) + tf3::layout_of(p).off_status);
+}
+
 int tf32x3_status(const GemmProblem& p, void* ws, cudaStream_t st) {
   const tf3::Layout L = tf3::layout_of(p);
   int h = 0;

@@ -25,4 +25,7 @@ cudaError_t tf32x3_gemm(const GemmProblem& prob, void* workspace, size_t ws_byte
 // `stream`): 0 = ok, 1 = a bounded device wait gave up.
 int tf32x3_status(const GemmProblem& prob, void* workspace, cudaStream_t stream);
 
+// Device address of the status word inside the workspace.
+int* tf32x3_status_ptr(const GemmProblem& prob, void* workspace);
+
 }  // namespace splab

@@ -73,3 +73,48 @@ def test_batch_graph_replay_sees_new_inputs():
     torch.cuda.synchronize()
     for p, f in zip(probs, first):
         assert torch.allclose(p["C"], 2.0 * f, rtol=1e-13, atol=1e-16)
+
+
+@pytest.mark.parametrize("dt,path,tol", [(np.complex64, 3, 1e-6), (np.float32, 3, 1e-6),
+                                         (np.complex128, 2, 1e-14), (np.complex64, 2, 1e-6)])
+def test_tensor_core_batch(dt, path, tol):
+    """Batches on the 3xTF32 (path 3) and Ozaki (path 2) paths: the instances
+    run in sequence with a shared workspace; the first run executes directly,
+    the second captures the sequence in a CUDA graph and replays it, the third
+    replays with changed inputs. Every result is checked against the oracle."""
+    import torch
+    import spla_b200 as spla
+    shapes = [(130, 70, 9000), (300, 257, 20000), (17, 300, 2048), (256, 128, 30001)]
+    probs, host = _problems(torch, dt, shapes, 500)
+    for p in probs:
+        p["beta"] = 0.0
+    batch = spla.Batch(np.dtype(dt).name, probs, path=path)
+    ws = torch.empty(batch.workspace_bytes, dtype=torch.uint8, device="cuda")
+
+    def check(scale):
+        torch.cuda.synchronize()
+        batch.check(ws)
+        for p, (A, B, C, alpha, beta) in zip(probs, host):
+            ref = np.zeros_like(C)
+            assert oracle.pgemm_ssb(p["m"], p["n"], p["k"], p["opA"], alpha * scale, A, p["k"],
+                                    B, p["k"], 0.0, ref, p["m"], 0, 0) == 0
+            err = oracle.rel_fro(p["C"].cpu().numpy(), ref)
+            assert err <= tol, (p["m"], p["n"], p["k"], err)
+
+    batch.run(ws)          # direct
+    check(1.0)
+    batch.run(ws)          # capture + replay
+    check(1.0)
+    for p in probs:
+        p["A"].mul_(2.0)   # exact for floats
+    batch.run(ws)          # replay sees the new data
+    check(2.0)
+    assert batch.info()["k_chunk"] == 0
+
+
+def test_tensor_core_batch_rejects_unsupported():
+    import torch
+    import spla_b200 as spla
+    probs, _ = _problems(torch, np.complex128, [(32, 32, 100)], 900)
+    with pytest.raises(spla.InvalidParameterError):
+        spla.Batch("complex128", probs, path=spla.PATH_TF32X3)  # 3xTF32 takes float dtypes
