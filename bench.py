@@ -513,12 +513,13 @@ def workload_cgemm_ssb(torch, spla, steps, warmup, path=None):
                                 3: "3xTF32"}[path]}}
 
 
-def workload_batch(torch, spla, steps, warmup, dtype="complex128", count=64, sub=32):
+def workload_batch(torch, spla, steps, warmup, dtype="complex128", count=64, sub=32, path=None):
     """64 ssb instances, k ~ U{120000..180000}, m = n ~ U{512, 768, 1024}
     (seeded draw order: k then m per instance), Gaussian/sqrt(k); run as
     sub-batches of `sub` instances (the complex-double operands of all 64,
-    ~236 GB, exceed HBM), each one persistent grouped launch replayed from a
-    CUDA graph with the autotuned k-chunk."""
+    ~236 GB, exceed HBM). path None/1: each sub-batch one persistent grouped
+    DMMA launch replayed from a CUDA graph with the autotuned k-chunk; path 2
+    (Ozaki) / 3 (3xTF32): the instances in sequence, replayed from a graph."""
     import numpy as np
     rng = np.random.default_rng(20250004)
     shapes = []
@@ -544,7 +545,7 @@ def workload_batch(torch, spla, steps, warmup, dtype="complex128", count=64, sub
             keep += [A, B, C]
             probs.append(dict(opA=2, opB=0, m=m, n=n, k=k, A=A, lda=k, B=B, ldb=k, C=C, ldc=m,
                               alpha=1.0, beta=0.0))
-        batch = spla.Batch(dtype, probs)
+        batch = spla.Batch(dtype, probs, path=path)
         ws = torch.empty(batch.workspace_bytes, dtype=torch.uint8, device="cuda")
         batch.run(ws, autotune=True)
         for _ in range(max(0, warmup - 1)):
@@ -557,6 +558,7 @@ def workload_batch(torch, spla, steps, warmup, dtype="complex128", count=64, sub
         e1.record()
         torch.cuda.synchronize()
         total_ms += e0.elapsed_time(e1) / steps
+        batch.check(ws)
         tuning.append(batch.info())
         # accuracy of one instance against torch (FP64 reference on the GPU)
         if b0 == 0:
@@ -570,7 +572,10 @@ def workload_batch(torch, spla, steps, warmup, dtype="complex128", count=64, sub
             "ms_per_batch": total_ms, "instances": count, "sub_batch": sub,
             "rel_err_instance0_vs_torch_fp64": err, "autotune": tuning,
             "config": {"workload": "64 x pgemm_ssb k~U{120000..180000} m=n~{512,768,1024}",
-                       "path": "DMMA grouped persistent + CUDA graph"}}
+                       "path": {None: "DMMA grouped persistent + CUDA graph",
+                                1: "DMMA grouped persistent + CUDA graph",
+                                2: "Ozaki INT8, instances in sequence, CUDA graph",
+                                3: "3xTF32, instances in sequence, CUDA graph"}[path]}}
 
 
 def run_workload(name, steps, warmup):
@@ -585,7 +590,12 @@ def run_workload(name, steps, warmup):
           "cgemm_ssb_ozaki": lambda t, s, st, w: workload_cgemm_ssb(t, s, st, w, 2),
           "cgemm_ssb_tf32x3": lambda t, s, st, w: workload_cgemm_ssb(t, s, st, w, 3),
           "batch": workload_batch,
-          "batch_c64": lambda t, s, st, w: workload_batch(t, s, st, w, "complex64", 64, 64)}[name]
+          "batch_c64": lambda t, s, st, w: workload_batch(t, s, st, w, "complex64", 64, 64),
+          "batch_ozaki": lambda t, s, st, w: workload_batch(t, s, st, w, "complex128", 64, 32, 2),
+          "batch_c64_ozaki": lambda t, s, st, w: workload_batch(t, s, st, w, "complex64", 64, 64,
+                                                                2),
+          "batch_c64_tf32x3": lambda t, s, st, w: workload_batch(t, s, st, w, "complex64", 64,
+                                                                 64, 3)}[name]
     line = fn(torch, spla, steps, warmup)
     line.update({"n_gpus": 1, "steps": steps, "warmup": warmup, "higher_is_better": True,
                  "data": "synthetic, seeded"})
@@ -607,7 +617,8 @@ def main():
     ap.add_argument("--workload", default="zgemm_ssb",
                     choices=["zgemm_ssb", "sbs", "ssbtr_float", "ssbtr_float_dmma",
                              "ssbtr_float_ozaki", "ssbtr_float_tf32x3", "cgemm_ssb_dmma",
-                             "cgemm_ssb_ozaki", "cgemm_ssb_tf32x3", "batch", "batch_c64"])
+                             "cgemm_ssb_ozaki", "cgemm_ssb_tf32x3", "batch", "batch_c64",
+                             "batch_ozaki", "batch_c64_ozaki", "batch_c64_tf32x3"])
     args = ap.parse_args()
     if args.workload != "zgemm_ssb" and args.impl == "ours":
         return run_workload(args.workload, args.steps, max(3, args.warmup))
