@@ -789,18 +789,12 @@ __global__ void oz_reconstruct(const int* __restrict__ R, int m, int n, int nb,
     }
     int r[kMaxModuli];
     const int64_t plane = int64_t(nb) * m;
-    for (int t = 0; t < rp.n; ++t) {
-      const int v = R[t * plane + int64_t(j) * m + i];
-      r[t] = v % rp.p[t];
-    }
+    for (int t = 0; t < rp.n; ++t) r[t] = R[t * plane + int64_t(j) * m + i];
     const int e = -(sigA[i] + sigB[j]);
     const double xr = ldexp(crt_value(r, rp), e);
     double xi = 0.0;
     if (CPLX) {
-      for (int t = 0; t < rp.n; ++t) {
-        const int v = R[t * plane + int64_t(n + j) * m + i];
-        r[t] = v % rp.p[t];
-      }
+      for (int t = 0; t < rp.n; ++t) r[t] = R[t * plane + int64_t(n + j) * m + i];
       xi = ldexp(crt_value(r, rp), e);
     }
     double outr = alr * xr - ali * xi, outi = alr * xi + ali * xr;

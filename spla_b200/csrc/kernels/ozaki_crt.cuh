@@ -104,30 +104,31 @@ __host__ __device__ __forceinline__ double i128_to_double(unsigned long long x1,
 }
 
 // X = (sum_t W_t r_t) mod P as a signed value in (-P/2, P/2], converted to double.
+// The r_t need not be reduced: any 0 <= r_t < 2^24 congruent to the residue
+// works (the INT8 GEMM hands over sums of per-chunk residues).
 __host__ __device__ __forceinline__ double crt_value(const int* r, const ReconParams& rp) {
-  // 192-bit accumulation S = s2:s1:s0
-  unsigned long long s0 = 0, s1 = 0, s2 = 0;
+  // S = sum_t W_t r_t accumulated per 32-bit limb of W_t: each product is
+  // below 2^56 and at most 16 of them below 2^60, so the four 64-bit limb sums
+  // need no carries (one 32x32->64 multiply-add per limb and modulus)
+  unsigned long long l0 = 0, l1 = 0, l2 = 0, l3 = 0;
   for (int t = 0; t < rp.n; ++t) {
-    const unsigned long long rt = (unsigned long long)r[t];
-    const unsigned long long lo_lo = rp.w_lo[t] * rt, lo_hi = mulhi64(rp.w_lo[t], rt);
-    const unsigned long long hi_lo = rp.w_hi[t] * rt, hi_hi = mulhi64(rp.w_hi[t], rt);
-    // add lo part
-    unsigned long long a = s0 + lo_lo;
-    unsigned long long c = a < s0;
-    s0 = a;
-    unsigned long long b = s1 + lo_hi;
-    unsigned long long c2 = b < s1;
-    b += c;
-    c2 += (b < c);
-    s1 = b;
-    s2 += c2;
-    // add hi part at 2^64
-    a = s1 + hi_lo;
-    c = a < s1;
-    s1 = a;
-    s2 += hi_hi + c;
+    const unsigned long long rt = (unsigned int)r[t];
+    l0 += rt * (unsigned int)rp.w_lo[t];
+    l1 += rt * (unsigned int)(rp.w_lo[t] >> 32);
+    l2 += rt * (unsigned int)rp.w_hi[t];
+    l3 += rt * (unsigned int)(rp.w_hi[t] >> 32);
   }
-  // q = floor(S / P) estimated in double (q < n * 256), then S - qP
+  // carry-propagate into the 192-bit S = s2:s1:s0
+  unsigned long long c = l0;
+  const unsigned long long d0 = c & 0xFFFFFFFFull;
+  c = (c >> 32) + l1;
+  const unsigned long long d1 = c & 0xFFFFFFFFull;
+  c = (c >> 32) + l2;
+  const unsigned long long d2 = c & 0xFFFFFFFFull;
+  c = (c >> 32) + l3;
+  const unsigned long long d3 = c & 0xFFFFFFFFull;
+  const unsigned long long s0 = d0 | (d1 << 32), s1 = d2 | (d3 << 32), s2 = c >> 32;
+  // q = floor(S / P) estimated in double (q < n * 2^24), then S - qP
   const double S_d = double(s2) * 3.402823669209385e38 + double(s1) * 18446744073709551616.0 +
                      double(s0);
   unsigned long long q = (unsigned long long)floor(S_d / rp.P_d);

@@ -1,7 +1,8 @@
 // CPU check of the Ozaki path's Chinese-remainder reconstruction (the same
 // host/device code the reconstruction kernel runs): random integers X with
 // |X| < P/2 are reduced modulo every modulus, reconstructed, and compared with
-// X converted to double. Also checks the CRT weights: W_t = 1 mod p_t and
+// X converted to double, also with unreduced residues (r + a multiple of p,
+// below 2^24). Also checks the CRT weights: W_t = 1 mod p_t and
 // 0 mod p_s (s != t). Prints "OK <cases>" on success.
 #include <cstdio>
 #include <cstdlib>
@@ -59,6 +60,14 @@ int main() {
       const double tol = (want < 0 ? -want : want) * 2.3e-16 + 1e-300;
       if (diff > tol) {
         printf("FAIL n=%d it=%d got %.17g want %.17g\n", n, it, got, want);
+        return 1;
+      }
+      // unreduced residues (sums of per-chunk residues, below 2^24)
+      for (int t = 0; t < n; ++t)
+        r[t] += c.p[t] * int(rng() % ((1u << 24) / unsigned(c.p[t]) - 1));
+      const double got2 = crt_value(r, rp);
+      if (got2 != got) {
+        printf("FAIL unreduced n=%d it=%d got %.17g want %.17g\n", n, it, got2, got);
         return 1;
       }
       ++cases;
