@@ -129,17 +129,24 @@ struct SliceConsts {
   unsigned long long c[kMaxModuli][4];
 };
 
-// Residues are computed on the FP32 pipe from base-2^13 digits of the scaled
-// integer x = round(2^sigma y) (|x| < 2^62), x = sum_i d_i 2^(13 i), which are
-// extracted without conversion instructions: x = xh 2^26 + xl with
-// xh = round(y 2^-26) and |xl| <= 2^25, both read as integers from the bits of
-// (value + 1.5 2^52); then d_0 = xl mod 2^13 (0 .. 8191), d_1 = xl >> 13
-// (|d_1| <= 4096), and xh gives d_2.. the same way (top digit signed). For a
-// modulus p the digit sum s = d_0 + sum_i c_i d_i (|c_i| <= p/2) is below
-// 2^22 in magnitude and exact in FP32; r = s - p * nearest(s / p) lies in
-// [-(p-1)/2, (p-1)/2] for odd p. For p = 256 the weights vanish and r is the
-// low byte of d_0. Each residue is produced as the float MAGIC + r, whose low
-// byte is r in two's complement: the int8 value without a conversion.
+// Residues are computed on the FP32 pipe from digits of the scaled integer
+// x = round(2^sigma y), x = sum_i d_i b^i, which are extracted without
+// conversion instructions: x = xh 2^h + xl with xh = round(y 2^-h), both read
+// as integers from the bits of (value + 1.5 2^52).
+//   NDIG 3 and 5 (|x| < 2^39, < 2^62): b = 2^13, h = 26; d_0 = xl mod 2^13
+//     (0 .. 8191), d_1 = xl >> 13 (|d_1| <= 4096), xh gives d_2.. the same
+//     way (top digit signed); the digit sum below stays under 2^22.
+//   NDIG 4 (|x| < 2^58, the default for double): b = 2^15, h = 30, balanced
+//     digits (|d_0|, |d_1|, |d_2| <= 2^14 + 1, |d_3| <= 2^13 + 1): one digit
+//     fewer; the digit sum stays under 5.3e6 < 2^23.
+// For a modulus p the digit sum s = d_0 + sum_i c_i d_i (c_i = b^i mod p in
+// symmetric form, |c_i| <= p/2) is exact in FP32, and since |s| < 2^23 the
+// quotient rounded from s * fl(1/p) is the nearest integer to s / p (for odd
+// p, s / p is at least 1/(2p) away from a half-integer; the product's error is
+// below that); r = s - p * nearest(s / p) lies in [-(p-1)/2, (p-1)/2]. For
+// p = 256 the weights vanish and r is the low byte of d_0. Each residue is
+// produced as the float MAGIC + r, whose low byte is r in two's complement:
+// the int8 value without a conversion.
 __device__ __forceinline__ float small_int_to_float(int d) {  // |d| < 2^22
   return __int_as_float(0x4B400000 + d) - 12582912.0f;
 }
@@ -148,6 +155,20 @@ template <int NDIG>
 __device__ __forceinline__ void digits13(double y, float (&d)[5]) {
   constexpr double kM52 = 6755399441055744.0;  // 1.5 * 2^52: ulp 1
   constexpr long long kM52Bits = 0x4338000000000000ll;
+  if (NDIG == 4) {  // balanced base-2^15 digits, |x| < 2^58
+    const double t = fma(y, 1.0 / 1073741824.0, kM52);  // kM52 + round(y 2^-30)
+    const double xl_d = fma(t - kM52, -1073741824.0, y);  // exact, |xl_d| <= 2^29
+    const int xl = int(__double2loint(xl_d + kM52));
+    const int xh = int(__double_as_longlong(t) - kM52Bits);  // |xh| <= 2^28 + 1
+    const int d0 = ((xl + 0x4000) & 0x7FFF) - 0x4000;
+    const int d2 = ((xh + 0x4000) & 0x7FFF) - 0x4000;
+    d[0] = small_int_to_float(d0);
+    d[1] = small_int_to_float((xl - d0) >> 15);
+    d[2] = small_int_to_float(d2);
+    d[3] = small_int_to_float((xh - d2) >> 15);
+    d[4] = 0.0f;
+    return;
+  }
   const double t = fma(y, 1.0 / 67108864.0, kM52);  // kM52 + round(y 2^-26)
   const double xl_d = fma(t - kM52, -67108864.0, y);  // exact, |xl_d| <= 2^25
   const int xl = int(__double2loint(xl_d + kM52));  // round(xl_d), two's complement
@@ -156,9 +177,6 @@ __device__ __forceinline__ void digits13(double y, float (&d)[5]) {
   d[1] = small_int_to_float(xl >> 13);
   if (NDIG == 3) {
     d[2] = small_int_to_float(int(xh));
-  } else if (NDIG == 4) {
-    d[2] = small_int_to_float(int(xh & 0x1FFF));
-    d[3] = small_int_to_float(int(xh >> 13));
   } else {
     d[2] = small_int_to_float(int(xh & 0x1FFF));
     d[3] = small_int_to_float(int((xh >> 13) & 0x1FFF));
@@ -286,7 +304,10 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
         if (NDIG > 3) s2 = f2_fma(c3, dp[i][3], s2);
         if (NDIG > 4) s2 = f2_fma(c4, dp[i][4], s2);
         const unsigned long long q2 = f2_add(f2_fma(s2, ip, M2), NM2);
-        f2_unpack(f2_fma(q2, np, f2_add(s2, M2)), r[2 * i], r[2 * i + 1]);
+        if (NDIG == 4)  // |s| may exceed 2^22: s + MAGIC is not exact, add it to r
+          f2_unpack(f2_add(f2_fma(q2, np, s2), M2), r[2 * i], r[2 * i + 1]);
+        else
+          f2_unpack(f2_fma(q2, np, f2_add(s2, M2)), r[2 * i], r[2 * i + 1]);
       }
     }
     uint32_t w[W];
@@ -985,15 +1006,19 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
     const int pt = crt.p[t];
     sc.neg_p[t] = f2_pack(-float(pt), -float(pt));
     sc.inv_p[t] = f2_pack(1.0f / float(pt), 1.0f / float(pt));
+  }
+  // digits covering |x| <= 2^Q: 3 of 13 bits, 4 balanced of 15 bits, or 5 of 13
+  const int ndig = crt.q_bits + 1 <= 39 ? 3 : (crt.q_bits + 1 <= 58 ? 4 : 5);
+  const long long base = ndig == 4 ? 32768 : 8192;
+  for (int t = 0; t < L.nmod; ++t) {
+    const int pt = crt.p[t];
     long long w = 1;
     for (int i = 0; i < 4; ++i) {
-      w = (w * 8192) % pt;  // 2^(13 (i+1)) mod p
+      w = (w * base) % pt;  // base^(i+1) mod p
       const float c = float(w > pt / 2 ? w - pt : w);
       sc.c[t][i] = f2_pack(c, c);
     }
   }
-  // digits of 13 bits covering |x| < 2^(Q+1)
-  const int ndig = crt.q_bits + 1 <= 39 ? 3 : (crt.q_bits + 1 <= 52 ? 4 : 5);
   const int vec_elems = 16 / int(sizeof(TIn));
   const bool vecA = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (ldA % vec_elems == 0);
   const bool vecB = (reinterpret_cast<uintptr_t>(B) % 16 == 0) && (ldB % vec_elems == 0);
