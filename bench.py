@@ -717,8 +717,17 @@ def main():
         int8_ops = 2.0 * nmod * M * (2 * N) * (2 * K)  # residue GEMMs: m x 2n x 2k per modulus
         achieved = int8_ops / (k_ms / 1e3) / 1e12
         peak = peaks.get("int8_tops")
+        # DRAM bytes of one full-size GEMM launch, from the ncu capture of the same kernel on
+        # m=n=1024, k=20000 (2.193 GB read, 0.120 GB written per launch): reads scale with the
+        # k-blocks processed (313 -> 3907), the accumulated-residue writes with the k-chunks
+        # (1 -> 5)
+        traffic = (2.193e9 * (2 * K / 128.0) / 313.0 + 0.120e9 * max(1, -(-2 * K // 124928))
+                   if (M, N) == (1024, 1024) else None)
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
-                "frac": (achieved / peak) if peak else None, "traffic": None,
+                "frac": (achieved / peak) if peak else None, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_{read,write}.sum of oz_gemm_pair<2> at "
+                                  "m=n=1024 k=20000, scaled to this k (k-blocks, k-chunks)",
+                "algorithmic_residue_bytes": float(OZAKI_MODULI) * (M + 2 * N) * 2 * K,
                 "kernel": "oz_gemm (tcgen05.mma kind::i8, TMA, TMEM)",
                 "peak_source": "measured here: cuBLASLt int8 GEMM 8192^3 via torch._int_mm",
                 "algorithmic_ops_per_launch": int8_ops}
