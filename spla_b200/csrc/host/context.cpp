@@ -104,7 +104,10 @@ ContextInternal::ContextInternal(SplaProcessingUnit pu)
   }
   check_cuda(cudaGetDevice(&deviceId_));
   fp64Path_ = path_from_env();
-  if (const char* v = std::getenv("SPLA_B200_OZAKI_MODULI")) ozakiModuli_ = std::atoi(v);
+  if (const char* v = std::getenv("SPLA_B200_OZAKI_MODULI")) {
+    const int m = std::atoi(v);  // valid: 8 .. 16; anything else keeps the default
+    if (m >= 8 && m <= 16) ozakiModuli_ = m;
+  }
   host_.reset(new ScratchPool(ScratchPool::kHost, std::malloc, std::free));
   pinned_.reset(new ScratchPool(
       ScratchPool::kPinned,

@@ -58,6 +58,10 @@ struct PhaseEvents {
   int count = 0;
 };
 PhaseEvents& phase_events();
+
+// cudaFuncAttributeMaxDynamicSharedMemorySize of `func` on the current device,
+// set once per device (thread-safe); returns the CUDA status of that call.
+cudaError_t set_dynamic_smem(const void* func, int bytes);
 inline void phase_mark(int phase, bool end, cudaStream_t st) {
   PhaseEvents& pe = phase_events();
   if (pe.ev && phase < pe.count &&

@@ -392,9 +392,8 @@ struct CfgFor<kR32, AK, BKM> {
 template <class Cfg>
 int occupancy() {
   static int occ = -1;
+  set_dynamic_smem(reinterpret_cast<const void*>(dmma_gemm_kernel<Cfg>), Cfg::SMEM_BYTES);
   if (occ < 0) {
-    cudaFuncSetAttribute(dmma_gemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         Cfg::SMEM_BYTES);
     int o = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, dmma_gemm_kernel<Cfg>, Cfg::THREADS,
                                                       Cfg::SMEM_BYTES) != cudaSuccess ||
@@ -638,9 +637,9 @@ namespace {
 template <class Cfg>
 int grouped_occupancy() {
   static int occ = -1;
+  set_dynamic_smem(reinterpret_cast<const void*>(dmma_gemm_grouped_kernel<Cfg>),
+                   Cfg::SMEM_BYTES);
   if (occ < 0) {
-    cudaFuncSetAttribute(dmma_gemm_grouped_kernel<Cfg>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES);
     int o = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, dmma_gemm_grouped_kernel<Cfg>,
                                                       Cfg::THREADS, Cfg::SMEM_BYTES) !=

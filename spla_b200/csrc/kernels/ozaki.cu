@@ -1244,14 +1244,11 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
         g.n_active = int(act.size());
         g.total_units = g.nmod * g.nchunks * g.n_active;
       }
-      static bool attr2 = false;
-      if (!attr2) {
-        cudaFuncSetAttribute(oz_gemm_pair<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             PairCfg<1>::SMEM);
-        cudaFuncSetAttribute(oz_gemm_pair<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             PairCfg<2>::SMEM);
-        attr2 = true;
-      }
+      if ((e = set_dynamic_smem(reinterpret_cast<const void*>(oz_gemm_pair<1>),
+                                PairCfg<1>::SMEM)) != cudaSuccess ||
+          (e = set_dynamic_smem(reinterpret_cast<const void*>(oz_gemm_pair<2>),
+                                PairCfg<2>::SMEM)) != cudaSuccess)
+        return e;
       if (!make_map(&mapA2, resA, L.kp, int64_t(L.nmod) * L.rowsA, 128) ||
           !make_map(&mapB2, resB, L.kp, int64_t(L.nmod) * L.nb, 128))
         return cudaErrorNotSupported;
@@ -1279,11 +1276,8 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
         return nt == 2 ? cudaLaunchKernelEx(&cfg, oz_gemm_pair<2>, mapA2, mapB2, gg)
                        : cudaLaunchKernelEx(&cfg, oz_gemm_pair<1>, mapA2, mapB2, gg);
       }
-      static bool attr = false;
-      if (!attr) {
-        cudaFuncSetAttribute(oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
-        attr = true;
-      }
+      const cudaError_t ea = set_dynamic_smem(reinterpret_cast<const void*>(oz_gemm), GEMM_SMEM);
+      if (ea != cudaSuccess) return ea;
       const int grid = std::min(gg.total_units, sm_count());
       oz_gemm<<<grid, GEMM_THREADS, GEMM_SMEM, s>>>(mapA, mapB, gg);
       return cudaGetLastError();

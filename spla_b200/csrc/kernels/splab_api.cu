@@ -4,6 +4,9 @@
 #include <vector>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "../../../include/splab.h"
 #include "common.cuh"
@@ -17,6 +20,19 @@ namespace splab {
 PhaseEvents& phase_events() {
   static thread_local PhaseEvents pe;
   return pe;
+}
+
+cudaError_t set_dynamic_smem(const void* func, int bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, func})) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.insert({dev, func});
+  return e;
 }
 
 namespace {

@@ -658,11 +658,9 @@ cudaError_t tf32x3_gemm(const GemmProblem& p, void* ws, size_t ws_bytes, cudaStr
       ntiles = g.n_active;
     }
     g.total_units = ntiles * g.nsuper;
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(tf3_gemm_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
-      attr = true;
-    }
+    if ((e = set_dynamic_smem(reinterpret_cast<const void*>(tf3_gemm_pair), SMEM)) !=
+        cudaSuccess)
+      return e;
     const int pairs = std::max(1, std::min(g.total_units, sm_count() / 2));
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(unsigned(2 * pairs));
