@@ -122,9 +122,9 @@ SPLAB_API int splab_gemm_dmma_noalloc(int dtype, int opA, int opB, int64_t m, in
  * alpha and beta (as (re, im) doubles; im ignored for real dtypes). One
  * persistent launch walks every (problem, tile, k-chunk) work item, one
  * grouped launch reduces the split-K partials; the pair is captured in a CUDA
- * graph on the first run and replayed afterwards. The k-chunk size is chosen
- * by measuring the candidates on the first run (autotune != 0; C is not
- * written while measuring) or by a model otherwise. FP64 tensor-core path
+ * graph on the first run and replayed afterwards. The CTA tile and the
+ * k-chunk size are chosen by measuring every candidate pair on the first run
+ * (autotune != 0; C is not written while measuring) or by a model otherwise. FP64 tensor-core path
  * (float inputs accumulate in FP64). No counterpart in the reference library
  * (a batch there is a loop of pgemm_ssb calls).
  */
@@ -157,10 +157,18 @@ SPLAB_API int splab_batch_create_path(int dtype, int path, int count,
  * (a different pointer triggers a new capture). */
 SPLAB_API int splab_batch_run(void *plan, void *workspace, size_t workspaceBytes, int autotune,
                               void *stream);
-/* Chosen k-chunk, and the measured time (ms) of each candidate k-chunk when
- * tuned; arrays of at least 32 entries. */
+/* Chosen k-chunk; the k-chunk and measured time (ms) of each tuning entry
+ * (one per tile configuration and k-chunk) when tuned, else the candidate
+ * k-chunks with time -1; arrays of at least 32 entries. */
 SPLAB_API int splab_batch_info(void *plan, int64_t *kChunk, int *nCandidates, int64_t *candidates,
                                double *tuningMs);
+/* CTA tile chosen for the grouped FP64 launch, and per tuning entry (the
+ * entries of splab_batch_info, arrays of at least 32) the tile it measured;
+ * the autotuner tries each k-chunk with the default tile (complex 64x64,
+ * real 128x64) and a larger one (complex 128x64, real 128x128). Zero for the
+ * tensor-core paths. */
+SPLAB_API int splab_batch_tiles(void *plan, int *tileM, int *tileN, int *nEntries,
+                                int *entryTileM, int *entryTileN);
 /* Synchronise `stream` and report SPLAB_ERR_TIMEOUT when a bounded device wait
  * gave up in the last run of a tensor-core batch (SPLAB_OK otherwise). */
 SPLAB_API int splab_batch_check(void *plan, void *workspace, void *stream);

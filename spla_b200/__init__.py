@@ -446,13 +446,22 @@ class Batch:
             raise GPULaunchError(f"splab_batch_check: {lib().splab_status_string(rc).decode()}")
 
     def info(self):
+        """Chosen k-chunk and CTA tile; per tuning entry its k-chunk, tile and
+        measured time (ms)."""
+        L = lib()
         kc, nc = ct.c_int64(), ct.c_int()
         cands = (ct.c_int64 * 32)()
         ms = (ct.c_double * 32)()
-        lib().splab_batch_info(self._plan, ct.byref(kc), ct.byref(nc), ct.cast(cands, ct.c_void_p),
-                               ct.cast(ms, ct.c_void_p))
-        return {"k_chunk": kc.value, "candidates": list(cands[:nc.value]),
-                "tuning_ms": list(ms[:nc.value])}
+        L.splab_batch_info(self._plan, ct.byref(kc), ct.byref(nc), ct.cast(cands, ct.c_void_p),
+                           ct.cast(ms, ct.c_void_p))
+        L.splab_batch_tiles.argtypes = [ct.c_void_p] + [ct.c_void_p] * 5
+        tm, tn, ne = ct.c_int(), ct.c_int(), ct.c_int()
+        etm, etn = (ct.c_int * 32)(), (ct.c_int * 32)()
+        L.splab_batch_tiles(self._plan, ct.byref(tm), ct.byref(tn), ct.byref(ne),
+                            ct.cast(etm, ct.c_void_p), ct.cast(etn, ct.c_void_p))
+        return {"k_chunk": kc.value, "tile": (tm.value, tn.value),
+                "candidates": list(cands[:nc.value]), "tuning_ms": list(ms[:nc.value]),
+                "candidate_tiles": list(zip(etm[:ne.value], etn[:ne.value]))}
 
     def __del__(self):
         try:

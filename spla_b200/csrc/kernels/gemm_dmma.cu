@@ -389,6 +389,28 @@ struct CfgFor<kR32, AK, BKM> {
   using type = DmmaCfg<kR32, AK, BKM, 128, 64, 16, 32, 32, 3>;
 };
 
+// Larger-tile variant that the batch autotuner measures beside the default:
+// complex 128x64 (8 warps), real 128x128 (16 warps); same k-step as CfgFor.
+template <int DT, bool AK, bool BKM>
+struct CfgWide;
+template <bool AK, bool BKM>
+struct CfgWide<kC64, AK, BKM> {
+  using type = DmmaCfg<kC64, AK, BKM, 128, 64, 8, 32, 32, 3>;
+};
+template <bool AK, bool BKM>
+struct CfgWide<kC32, AK, BKM> {
+  using type = DmmaCfg<kC32, AK, BKM, 128, 64, 8, 32, 32, 3>;
+};
+template <bool AK, bool BKM>
+struct CfgWide<kR64, AK, BKM> {
+  using type = DmmaCfg<kR64, AK, BKM, 128, 128, 16, 32, 32, 3>;
+};
+template <bool AK, bool BKM>
+struct CfgWide<kR32, AK, BKM> {
+  using type = DmmaCfg<kR32, AK, BKM, 128, 128, 16, 32, 32, 3>;
+};
+constexpr int kBatchTileVariants = 2;
+
 template <class Cfg>
 int occupancy() {
   static int occ = -1;
@@ -658,15 +680,20 @@ struct BatchPlanImpl {
   int bm = 0, bn = 0, bk = 0;
   std::vector<GemmProblem> probs;
   int64_t kc = 0;  // k per split (multiple of BK)
+  int variant = 0;  // tile configuration: 0 default, 1 larger tiles
   std::vector<int64_t> candidates;
   bool tuned = false;
+  // one entry per measured (tile configuration, k-chunk)
   std::vector<double> tuning_ms;
+  std::vector<int64_t> entry_kc;
+  std::vector<int> entry_bm, entry_bn;
   // device-side tables (allocated by the caller's workspace)
   size_t off_params = 0, off_items = 0, off_splits = 0, off_partials = 0, total = 0;
   int n_items = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   void* graph_ws = nullptr;
+  void* tables_ws = nullptr;  // workspace holding the tables of the chosen configuration
   // private stream the graph is captured on and replayed on (the caller's
   // stream may be the legacy default stream, which cannot be captured)
   cudaStream_t own = nullptr;
@@ -677,8 +704,20 @@ namespace {
 
 size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Work items of the batch for tiles bm x bn and k-chunk kc.
+size_t batch_items(const BatchPlanImpl& b, int bm, int bn, int64_t kc) {
+  size_t items = 0;
+  for (auto& p : b.probs) {
+    const int64_t sp = std::max<int64_t>(1, (p.k + kc - 1) / kc);
+    items += size_t(sp) * ((p.m + bm - 1) / bm) * ((p.n + bn - 1) / bn);
+  }
+  return items;
+}
+
+// min_bm x min_bn: the smallest tile of the configurations the plan may use
+// (sizes the item table)
 template <class Cfg>
-void batch_geometry(BatchPlanImpl& b) {
+void batch_geometry(BatchPlanImpl& b, int min_bm, int min_bn) {
   b.bm = Cfg::BM;
   b.bn = Cfg::BN;
   b.bk = Cfg::BK;
@@ -697,13 +736,13 @@ void batch_geometry(BatchPlanImpl& b) {
   for (int64_t c = c0; c <= std::max<int64_t>(c0, kmin / 2); c *= 2) b.candidates.push_back(c);
   // workspace: tables + partials for the smallest candidate (most splits)
   const int64_t cmin = b.candidates.front();
-  size_t partial_bytes = 0, items = 0;
+  size_t partial_bytes = 0;
   const size_t esz = Cfg::CPLX ? 16 : 8;
   for (auto& p : b.probs) {
     const int64_t sp = std::max<int64_t>(1, (p.k + cmin - 1) / cmin);
     partial_bytes += al256(size_t(sp) * p.m * p.n * esz);
-    items += size_t(sp) * ((p.m + Cfg::BM - 1) / Cfg::BM) * ((p.n + Cfg::BN - 1) / Cfg::BN);
   }
+  const size_t items = batch_items(b, min_bm, min_bn, cmin);
   b.off_params = 0;
   b.off_splits = al256(sizeof(DmmaParams) * b.count);
   b.off_items = b.off_splits + al256(sizeof(int) * b.count);
@@ -801,48 +840,40 @@ cudaError_t batch_launch_reduce(BatchPlanImpl& b, char* ws, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Time one launch of the grouped GEMM for configuration Cfg and k-chunk kc
+// (tables uploaded for it first; a warm-up launch before the timed one).
 template <class Cfg>
-cudaError_t batch_run_cfg(BatchPlanImpl& b, char* ws, cudaStream_t st, bool autotune) {
+cudaError_t batch_time(BatchPlanImpl& b, int64_t kc, char* ws, cudaStream_t st, float* ms) {
   cudaError_t e;
-  if (!b.tuned) {
-    if (autotune && b.candidates.size() > 1) {
-      cudaEvent_t e0, e1;
-      cudaEventCreate(&e0);
-      cudaEventCreate(&e1);
-      double best = 1e30;
-      int64_t best_kc = b.candidates.front();
-      b.tuning_ms.clear();
-      for (int64_t kc : b.candidates) {
-        if ((e = batch_tables<Cfg>(b, kc, ws, st)) != cudaSuccess) return e;
-        if ((e = batch_launch_gemm<Cfg>(b, ws, st)) != cudaSuccess) return e;  // warm
-        cudaEventRecord(e0, st);
-        if ((e = batch_launch_gemm<Cfg>(b, ws, st)) != cudaSuccess) return e;
-        cudaEventRecord(e1, st);
-        cudaEventSynchronize(e1);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        b.tuning_ms.push_back(ms);
-        if (ms < best) {
-          best = ms;
-          best_kc = kc;
-        }
-      }
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
-      b.kc = best_kc;
-    } else {
-      // model choice: the candidate closest to 8 k-tiles per ... one wave multiple
-      b.kc = b.candidates.size() > 2 ? b.candidates[2] : b.candidates.back();
-    }
-    if ((e = batch_tables<Cfg>(b, b.kc, ws, st)) != cudaSuccess) return e;
-    b.tuned = true;
-  }
+  if ((e = batch_tables<Cfg>(b, kc, ws, st)) != cudaSuccess) return e;
+  if ((e = batch_launch_gemm<Cfg>(b, ws, st)) != cudaSuccess) return e;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  e = batch_launch_gemm<Cfg>(b, ws, st);
+  cudaEventRecord(e1, st);
+  cudaEventSynchronize(e1);
+  *ms = 0.f;
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return e;
+}
+
+template <class Cfg>
+cudaError_t batch_run_cfg(BatchPlanImpl& b, char* ws, cudaStream_t st) {
+  cudaError_t e;
   // capture once per workspace on the plan's own stream, then replay there,
   // ordered after / before the caller's stream with events
   if (!b.own) {
     if ((e = cudaStreamCreateWithFlags(&b.own, cudaStreamNonBlocking)) != cudaSuccess) return e;
     if ((e = cudaEventCreateWithFlags(&b.ev_in, cudaEventDisableTiming)) != cudaSuccess) return e;
     if ((e = cudaEventCreateWithFlags(&b.ev_out, cudaEventDisableTiming)) != cudaSuccess) return e;
+  }
+  if (b.tables_ws != ws) {  // a different workspace than the one tuned on
+    if ((e = batch_tables<Cfg>(b, b.kc, ws, st)) != cudaSuccess) return e;
+    b.tables_ws = ws;
   }
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;  // tables uploaded on st
   if (!b.exec || b.graph_ws != ws) {
@@ -870,13 +901,37 @@ cudaError_t batch_run_cfg(BatchPlanImpl& b, char* ws, cudaStream_t st, bool auto
   return cudaStreamWaitEvent(st, b.ev_out, 0);
 }
 
+template <int DT, int V, class F>
+auto with_cfg_v(const GemmProblem& pr, F&& f) {
+  if constexpr (V == 0) {
+    return with_cfg<DT>(pr, f);
+  } else {
+    const bool ak = pr.opA != 0, bk = pr.opB == 0;
+    if (ak && bk) return f(typename CfgWide<DT, true, true>::type{});
+    if (ak && !bk) return f(typename CfgWide<DT, true, false>::type{});
+    if (!ak && bk) return f(typename CfgWide<DT, false, true>::type{});
+    return f(typename CfgWide<DT, false, false>::type{});
+  }
+}
+
+template <int DT, class F>
+auto with_variant(const GemmProblem& pr, int v, F&& f) {
+  return v == 0 ? with_cfg_v<DT, 0>(pr, f) : with_cfg_v<DT, 1>(pr, f);
+}
+
+// Run f with the configuration of the plan's dtype, op pair and tile variant.
 template <class F>
-auto batch_dispatch(const BatchPlanImpl& b, F&& f) {
+auto batch_dispatch(const BatchPlanImpl& b, int variant, F&& f) {
   GemmProblem pr{};
   pr.dtype = b.dtype;
   pr.opA = b.opA;
   pr.opB = b.opB;
-  return dispatch(pr, f);
+  switch (pr.dtype) {
+    case kR32: return with_variant<kR32>(pr, variant, f);
+    case kR64: return with_variant<kR64>(pr, variant, f);
+    case kC32: return with_variant<kC32>(pr, variant, f);
+    default: return with_variant<kC64>(pr, variant, f);
+  }
 }
 
 }  // namespace
@@ -888,8 +943,15 @@ BatchPlanImpl* batch_create(int dtype, const std::vector<GemmProblem>& probs) {
   b->opB = probs.front().opB;
   b->count = int(probs.size());
   b->probs = probs;
-  batch_dispatch(*b, [&](auto cfg) {
-    batch_geometry<decltype(cfg)>(*b);
+  int min_bm = 1 << 30, min_bn = 1 << 30;
+  for (int v = 0; v < kBatchTileVariants; ++v)
+    batch_dispatch(*b, v, [&](auto cfg) {
+      min_bm = std::min(min_bm, decltype(cfg)::BM);
+      min_bn = std::min(min_bn, decltype(cfg)::BN);
+      return 0;
+    });
+  batch_dispatch(*b, 0, [&](auto cfg) {
+    batch_geometry<decltype(cfg)>(*b, min_bm, min_bn);
     return 0;
   });
   return b;
@@ -898,9 +960,50 @@ BatchPlanImpl* batch_create(int dtype, const std::vector<GemmProblem>& probs) {
 size_t batch_workspace(const BatchPlanImpl* b) { return b->total; }
 
 cudaError_t batch_run(BatchPlanImpl* b, void* ws, cudaStream_t st, bool autotune) {
-  return batch_dispatch(*b, [&](auto cfg) {
-    return batch_run_cfg<decltype(cfg)>(*b, static_cast<char*>(ws), st, autotune);
-  });
+  char* w = static_cast<char*>(ws);
+  cudaError_t e;
+  if (!b->tuned) {
+    b->tuning_ms.clear();
+    b->entry_kc.clear();
+    b->entry_bm.clear();
+    b->entry_bn.clear();
+    if (autotune) {
+      // measure every (tile configuration, k-chunk) pair and keep the fastest
+      double best = 1e30;
+      for (int v = 0; v < kBatchTileVariants; ++v)
+        for (int64_t kc : b->candidates) {
+          float ms = 0.f;
+          e = batch_dispatch(*b, v, [&](auto cfg) {
+            b->entry_bm.push_back(decltype(cfg)::BM);
+            b->entry_bn.push_back(decltype(cfg)::BN);
+            return batch_time<decltype(cfg)>(*b, kc, w, st, &ms);
+          });
+          if (e != cudaSuccess) return e;
+          b->tuning_ms.push_back(ms);
+          b->entry_kc.push_back(kc);
+          if (ms < best) {
+            best = ms;
+            b->variant = v;
+            b->kc = kc;
+          }
+        }
+    } else {
+      // model choice: default tiles, the third candidate (8 or more k-tiles
+      // per split and several splits per problem for these sizes)
+      b->variant = 0;
+      b->kc = b->candidates.size() > 2 ? b->candidates[2] : b->candidates.back();
+    }
+    e = batch_dispatch(*b, b->variant, [&](auto cfg) {
+      b->bm = decltype(cfg)::BM;
+      b->bn = decltype(cfg)::BN;
+      return batch_tables<decltype(cfg)>(*b, b->kc, w, st);
+    });
+    if (e != cudaSuccess) return e;
+    b->tables_ws = ws;
+    b->tuned = true;
+  }
+  return batch_dispatch(*b, b->variant,
+                        [&](auto cfg) { return batch_run_cfg<decltype(cfg)>(*b, w, st); });
 }
 
 void batch_destroy(BatchPlanImpl* b) {
@@ -916,5 +1019,14 @@ void batch_destroy(BatchPlanImpl* b) {
 
 int64_t batch_kc(const BatchPlanImpl* b) { return b->kc; }
 const std::vector<double>& batch_tuning(const BatchPlanImpl* b) { return b->tuning_ms; }
-const std::vector<int64_t>& batch_candidates(const BatchPlanImpl* b) { return b->candidates; }
+const std::vector<int64_t>& batch_candidates(const BatchPlanImpl* b) {
+  return b->tuned && !b->entry_kc.empty() ? b->entry_kc : b->candidates;
+}
+void batch_tiles(const BatchPlanImpl* b, int* bm, int* bn, std::vector<int>* entry_bm,
+                 std::vector<int>* entry_bn) {
+  *bm = b->bm;
+  *bn = b->bn;
+  *entry_bm = b->entry_bm;
+  *entry_bn = b->entry_bn;
+}
 }  // namespace splab

@@ -54,13 +54,19 @@ int dmma_gemm_noalloc(const GemmProblem& prob, int num_sms, cudaStream_t stream)
 struct BatchPlanImpl;
 BatchPlanImpl* batch_create(int dtype, const std::vector<GemmProblem>& probs);
 size_t batch_workspace(const BatchPlanImpl* plan);
-// First run measures the candidate k-chunk sizes (autotune) or takes the model
-// choice, then captures the grouped launch in a CUDA graph; later runs replay.
+// First run measures every (CTA tile configuration, k-chunk) pair (autotune)
+// or takes the model choice, then captures the grouped launch in a CUDA graph;
+// later runs replay.
 cudaError_t batch_run(BatchPlanImpl* plan, void* workspace, cudaStream_t stream, bool autotune);
 void batch_destroy(BatchPlanImpl* plan);
 int64_t batch_kc(const BatchPlanImpl* plan);
 const std::vector<double>& batch_tuning(const BatchPlanImpl* plan);
+// The k-chunk of each tuning entry after an autotuned first run (the
+// candidate k-chunks before it).
 const std::vector<int64_t>& batch_candidates(const BatchPlanImpl* plan);
+// Chosen CTA tile and the tile of each tuning entry.
+void batch_tiles(const BatchPlanImpl* plan, int* bm, int* bn, std::vector<int>* entry_bm,
+                 std::vector<int>* entry_bn);
 
 // Sum `splits` FP64 partial tiles in order and apply alpha/beta into C.
 cudaError_t reduce_partials(const GemmProblem& prob, const void* partials, int splits, int tile_m,

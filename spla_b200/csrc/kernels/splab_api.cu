@@ -362,6 +362,30 @@ int splab_batch_info(void* plan, int64_t* kChunk, int* nCandidates, int64_t* can
   return SPLAB_OK;
 }
 
+int splab_batch_tiles(void* plan, int* tileM, int* tileN, int* nEntries, int* entryTileM,
+                      int* entryTileN) {
+  if (!plan) return SPLAB_ERR_INVALID;
+  const BatchHandle* h = static_cast<const BatchHandle*>(plan);
+  if (h->seq) {  // the tensor-core paths pick their own tiles
+    if (tileM) *tileM = 0;
+    if (tileN) *tileN = 0;
+    if (nEntries) *nEntries = 0;
+    return SPLAB_OK;
+  }
+  int bm = 0, bn = 0;
+  std::vector<int> ebm, ebn;
+  batch_tiles(h->grouped, &bm, &bn, &ebm, &ebn);
+  if (tileM) *tileM = bm;
+  if (tileN) *tileN = bn;
+  const int ne = int(std::min<size_t>(ebm.size(), 32));
+  if (nEntries) *nEntries = ne;
+  for (int i = 0; i < ne; ++i) {
+    if (entryTileM) entryTileM[i] = ebm[i];
+    if (entryTileN) entryTileN[i] = ebn[i];
+  }
+  return SPLAB_OK;
+}
+
 int splab_batch_destroy(void* plan) {
   BatchHandle* h = static_cast<BatchHandle*>(plan);
   if (!h) return SPLAB_OK;

@@ -43,8 +43,16 @@ def test_batch_matches_oracle(dt, tol, autotune):
     torch.cuda.synchronize()
     info = batch.info()
     assert info["k_chunk"] in info["candidates"]
-    if autotune and len(info["candidates"]) > 1:
+    if autotune:
+        # every (tile, k-chunk) pair measured; the chosen pair is the fastest
+        assert len(info["candidate_tiles"]) == len(info["tuning_ms"]) == len(info["candidates"])
+        assert len(set(info["candidate_tiles"])) == 2
         assert all(t > 0 for t in info["tuning_ms"])
+        best = int(np.argmin(info["tuning_ms"]))
+        assert info["tile"] == info["candidate_tiles"][best]
+        assert info["k_chunk"] == info["candidates"][best]
+    else:
+        assert info["tile"] in ((64, 64), (128, 64))
     for p, (A, B, C, alpha, beta) in zip(probs, host):
         ref = C.copy()
         assert oracle.pgemm_ssb(p["m"], p["n"], p["k"], p["opA"], alpha, A, p["k"], B, p["k"],
@@ -118,3 +126,28 @@ def test_tensor_core_batch_rejects_unsupported():
     probs, _ = _problems(torch, np.complex128, [(32, 32, 100)], 900)
     with pytest.raises(spla.InvalidParameterError):
         spla.Batch("complex128", probs, path=spla.PATH_TF32X3)  # 3xTF32 takes float dtypes
+
+
+def test_batch_new_workspace_after_tuning():
+    """A run with a different workspace than the tuning run uploads the work
+    tables there before capturing: results stay correct."""
+    import torch
+    import spla_b200 as spla
+    shapes = [(70, 90, 6000), (128, 32, 9000)]
+    probs, host = _problems(torch, np.complex128, shapes, 700)
+    for p in probs:
+        p["beta"] = 0.0
+    batch = spla.Batch("complex128", probs)
+    ws1 = torch.empty(batch.workspace_bytes, dtype=torch.uint8, device="cuda")
+    batch.run(ws1)
+    ws2 = torch.full((batch.workspace_bytes,), 0xFF, dtype=torch.uint8, device="cuda")
+    del ws1
+    for p in probs:
+        p["C"].zero_()
+    batch.run(ws2)
+    torch.cuda.synchronize()
+    for p, (A, B, C, alpha, beta) in zip(probs, host):
+        ref = np.zeros_like(C)
+        assert oracle.pgemm_ssb(p["m"], p["n"], p["k"], p["opA"], alpha, A, p["k"], B, p["k"],
+                                0.0, ref, p["m"], 0, 0) == 0
+        assert oracle.rel_fro(p["C"].cpu().numpy(), ref) <= 1e-14
