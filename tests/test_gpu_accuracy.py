@@ -1,7 +1,7 @@
 """Accuracy at the benchmark's scale of k against the double-double (Dot2)
 oracle, through the spla_* C ABI with device-resident operands.
 
-Bars (BASELINE metric): relative Frobenius error <= 1e-14 for double and
+Bars: relative Frobenius error <= 1e-14 for double and
 complex double; <= 1e-6 against the reference (so <= 5e-7 against the exact
 result) for float."""
 import numpy as np
