@@ -223,11 +223,6 @@ __device__ __forceinline__ uint32_t pack4(float a, float b, float c, float d) {
   return __byte_perm(t0, t1, 0x5410);
 }
 
-// negate the int8 residues in bytes 1 and 3 of a packed word (mod 2^8, which
-// keeps every residue class, including -128 for p = 256)
-__device__ __forceinline__ uint32_t neg_odd_bytes(uint32_t w) {
-  return (w & 0x00FF00FFu) | (__vsub4(0u, w) & 0xFF00FF00u);
-}
 
 // Residues of one operand, written K-major: res[t][row][l] (row stride kp).
 // Each thread handles EL (8 or 16) consecutive reals of one row.
@@ -287,12 +282,13 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
     }
   }
   const unsigned long long M2 = f2_pack(kMagic, kMagic), NM2 = f2_pack(-kMagic, -kMagic);
+  const unsigned long long NEG1 = f2_pack(-1.0f, -1.0f), TWO_M2 = f2_pack(2 * kMagic, 2 * kMagic);
   int8_t* out = res + t_begin * res_mod_stride + int64_t(row) * kp + l0;
   for (int t = t_begin; t < t_end; ++t, out += res_mod_stride) {
-    float r[EL];
+    unsigned long long rp2[EL / 2];  // MAGIC + residue of elements 2i, 2i + 1
     if (t == 0 && sc.p0 == 256.0f) {
 #pragma unroll
-      for (int i = 0; i < EL / 2; ++i) f2_unpack(f2_add(dp[i][0], M2), r[2 * i], r[2 * i + 1]);
+      for (int i = 0; i < EL / 2; ++i) rp2[i] = f2_add(dp[i][0], M2);
     } else {
       const unsigned long long np = sc.neg_p[t], ip = sc.inv_p[t];
       const unsigned long long c1 = sc.c[t][0], c2 = sc.c[t][1], c3 = sc.c[t][2],
@@ -305,27 +301,39 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
         if (NDIG > 4) s2 = f2_fma(c4, dp[i][4], s2);
         const unsigned long long q2 = f2_add(f2_fma(s2, ip, M2), NM2);
         if (NDIG == 4)  // |s| may exceed 2^22: s + MAGIC is not exact, add it to r
-          f2_unpack(f2_add(f2_fma(q2, np, s2), M2), r[2 * i], r[2 * i + 1]);
+          rp2[i] = f2_add(f2_fma(q2, np, s2), M2);
         else
-          f2_unpack(f2_fma(q2, np, f2_add(s2, M2)), r[2 * i], r[2 * i + 1]);
+          rp2[i] = f2_fma(q2, np, f2_add(s2, M2));
       }
     }
-    uint32_t w[W];
+    float r[EL];
 #pragma unroll
-    for (int q = 0; q < W; ++q) w[q] = pack4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
+    for (int i = 0; i < EL / 2; ++i) f2_unpack(rp2[i], r[2 * i], r[2 * i + 1]);
+    uint32_t wu[W], wv[W];
     if (mode == 0) {
+#pragma unroll
+      for (int q = 0; q < W; ++q)
+        wu[q] = pack4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
       if constexpr (W == 4)
-        *reinterpret_cast<uint4*>(out) = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4*>(out) = make_uint4(wu[0], wu[1], wu[2], wu[3]);
       else
-        *reinterpret_cast<uint2*>(out) = make_uint2(w[0], w[1]);
+        *reinterpret_cast<uint2*>(out) = make_uint2(wu[0], wu[1]);
     } else {
-      // w = [br0, bi0, br1, bi1]; u = [br, -s bi], v = [bi, s br]
-      uint32_t wu[W], wv[W];
+      // complex element e: reals (2e, 2e + 1) = (br, bi); u = (br, -s bi),
+      // v = (bi, s br). -r is MAGIC - r = 2 MAGIC - (MAGIC + r), exact.
+      float ng[EL];
+#pragma unroll
+      for (int i = 0; i < EL / 2; ++i) f2_unpack(f2_fma(rp2[i], NEG1, TWO_M2), ng[2 * i], ng[2 * i + 1]);
 #pragma unroll
       for (int q = 0; q < W; ++q) {
-        const uint32_t sw = __byte_perm(w[q], 0u, 0x2301);  // [bi0, br0, bi1, br1]
-        wu[q] = s_sign > 0 ? neg_odd_bytes(w[q]) : w[q];
-        wv[q] = s_sign > 0 ? sw : neg_odd_bytes(sw);
+        const float br0 = r[4 * q], bi0 = r[4 * q + 1], br1 = r[4 * q + 2], bi1 = r[4 * q + 3];
+        if (s_sign < 0) {
+          wu[q] = pack4(br0, bi0, br1, bi1);
+          wv[q] = pack4(bi0, ng[4 * q], bi1, ng[4 * q + 2]);
+        } else {
+          wu[q] = pack4(br0, ng[4 * q + 1], br1, ng[4 * q + 3]);
+          wv[q] = pack4(bi0, br0, bi1, br1);
+        }
       }
       int8_t* out_v = out + int64_t(rows) * kp;
       if constexpr (W == 4) {
