@@ -36,7 +36,7 @@ extern "C" {
 #define SPLAB_C64 3
 
 /* Compute paths for the contraction. */
-#define SPLAB_PATH_AUTO 0  /* Ozaki for large ssb-shaped problems, else DMMA */
+#define SPLAB_PATH_AUTO 0  /* the supported path with the least modelled time */
 #define SPLAB_PATH_DMMA 1  /* FP64 tensor cores (mma.sync f64); float inputs accumulate in FP64 */
 #define SPLAB_PATH_OZAKI 2 /* Ozaki scheme II on INT8 tcgen05 (all four dtypes) with
                               op(A) in {T, C}, op(B) = N; other problems use DMMA */
@@ -54,9 +54,13 @@ extern "C" {
 
 SPLAB_API const char *splab_status_string(int status);
 
-/* The concrete path (SPLAB_PATH_DMMA or SPLAB_PATH_OZAKI) `path` resolves to
- * for this problem; SPLAB_PATH_AUTO looks at the shape and the free device
- * memory, so resolve once and pass the result to the calls below. */
+/* The concrete path (SPLAB_PATH_DMMA, SPLAB_PATH_OZAKI or SPLAB_PATH_TF32X3)
+ * `path` resolves to for this problem. An explicit path resolves to itself when
+ * it supports the problem, else to DMMA. SPLAB_PATH_AUTO picks, among the
+ * supported paths whose workspace fits in a quarter of the device memory, the
+ * one with the least modelled time (a model of each path measured on B200;
+ * a tensor-core path must beat DMMA by 10 %). The result depends only on the
+ * problem and the device. */
 SPLAB_API int splab_gemm_path(int dtype, int path, int opA, int opB, int64_t m, int64_t n,
                               int64_t k);
 

@@ -1144,11 +1144,13 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
   };
   phase_mark(0, false, st);
   if (p.k > 0 && ps) {
+    // A's norms alone (both are pure reads and would share the bandwidth),
+    // then B's norms on the side stream while A is sliced
+    scale(1, st);
     if ((e = cudaEventRecord(ps->ev_start, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(ps->lo, ps->ev_start, 0)) != cudaSuccess) return e;
     scale(2, ps->lo);
     if ((e = cudaEventRecord(ps->ev_scaled, ps->lo)) != cudaSuccess) return e;
-    scale(1, st);
   } else if (p.k > 0) {
     scale(3, st);
   } else {

@@ -1,5 +1,6 @@
 // splab_* C ABI: argument checks and dispatch to the sm_100a kernels.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <vector>
 #include <cstdlib>
@@ -92,28 +93,99 @@ GemmProblem make_problem(int dtype, int opA, int opB, int64_t m, int64_t n, int6
   return p;
 }
 
-// Ozaki when requested, or, for AUTO, when the problem is a large ssb-shaped
-// FP64 contraction (where it measured faster than the FP64 tensor cores) whose
-// residue workspace is at most a quarter of the free device memory; DMMA
-// otherwise and whenever the layout is not supported.
-bool use_ozaki(const GemmProblem& p, int path) {
-  if (!ozaki_supported(p)) return false;
-  if (path == SPLAB_PATH_OZAKI) return true;
-  if (path == SPLAB_PATH_DMMA) return false;
-  const double flops = double(p.m) * p.n * p.k * (p.dtype == kC64 ? 8.0 : 2.0);
-  if (!(p.m >= 256 && p.n >= 128 && p.k >= 8192 && flops >= 1e13)) return false;
-  if (!dtype_is_double(p.dtype) && flops < 4e13) return false;
-  size_t free_b = 0, total_b = 0;
-  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return ozaki_workspace_bytes(p, 0) <= free_b / 4;
+// Path selection. An explicit path is taken when it supports the problem
+// (the tensor-core paths need op(A) in {T, C}, op(B) = N; 3xTF32 float dtypes
+// only), else the FP64 DMMA kernel runs. AUTO takes the path with the least
+// modelled time among the supported ones whose workspace fits in a quarter of
+// the device memory. The model's constants were measured on B200 (complex and
+// real, m = n from 128 to 2048, k from 8192 to 65536, and the k = 250000
+// configurations): DMMA at 33 / 29 TFLOP/s (complex / real) plus 0.05 ms; the
+// Ozaki path as slicing (6.3e-13 s per real element and modulus, plus the
+// norms' read at 6 TB/s), INT8 GEMM at 2.5 POP/s scaled by how evenly its work
+// units fill the 74 CTA pairs, reconstruction (3e-12 s per real output and
+// modulus) and 0.08 ms; 3xTF32 as splitting (bytes at 5.5 TB/s), three TF32
+// products at 480 TFLOP/s scaled by the same fill, and 0.05 ms. The choice only
+// depends on the problem and the device (no free-memory query), so that
+// resolving a path, sizing its workspace and running it agree.
+namespace model {
+
+constexpr int kPairs = 74;
+
+double fill(double units) {
+  if (units <= 0) return 1.0;
+  const double rounds = std::ceil(units / kPairs);
+  return units / (rounds * kPairs);
 }
 
-// 3xTF32 only when requested and the problem is a float ssb-shaped one.
-bool use_tf32x3(const GemmProblem& p, int path) {
-  return path == SPLAB_PATH_TF32X3 && tf32x3_supported(p);
+double dmma_ms(const GemmProblem& p) {
+  const bool c = dtype_is_complex(p.dtype);
+  const double flops = double(p.m) * p.n * p.k * (c ? 8.0 : 2.0);
+  return flops / (c ? 33e12 : 29e12) * 1e3 + 0.05;
+}
+
+double ozaki_ms(const GemmProblem& p) {
+  const bool c = dtype_is_complex(p.dtype);
+  const int nmod = dtype_is_double(p.dtype) ? 15 : 9;
+  const double K2 = c ? 2.0 * p.k : double(p.k), nb = c ? 2.0 * p.n : double(p.n);
+  const double kp = std::ceil(K2 / 128.0) * 128.0;
+  const double reals = double(p.m + p.n) * K2;
+  const double slice = 6.3e-13 * reals * nmod + reals * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12;
+  const double nt = nb >= 512 ? 2.0 : 1.0;
+  const double tiles = std::ceil(p.m / 256.0) * std::ceil(nb / (256.0 * nt));
+  const double chunks = std::ceil(kp / 128.0 / 976.0);
+  const double gemm = 2.0 * nmod * p.m * nb * kp / (2.5e15 * fill(nmod * chunks * tiles));
+  const double recon = 3e-12 * p.m * nb * nmod;
+  return (slice + gemm + recon) * 1e3 + 0.08;
+}
+
+double tf32x3_ms(const GemmProblem& p) {
+  const bool c = dtype_is_complex(p.dtype);
+  const double K2 = c ? 2.0 * p.k : double(p.k), nb = c ? 2.0 * p.n : double(p.n);
+  const double kp = std::ceil(K2 / 32.0) * 32.0;
+  const double bytes = double(p.m + p.n) * K2 * 4 + (p.m + nb) * kp * 8;
+  const double tiles = std::ceil(p.m / 256.0) * std::ceil(nb / 128.0);
+  const double splits = std::max(1.0, std::floor(kp / 32.0 / 64.0));
+  // the split count is chosen to balance the units over the pairs when k allows
+  const double units = tiles * splits;
+  const double gemm = 6.0 * p.m * nb * kp / (4.8e14 * (units >= kPairs ? 0.95 : units / kPairs));
+  return (bytes / 5.5e12 + gemm) * 1e3 + 0.05;
+}
+
+}  // namespace model
+
+size_t device_total_memory() {
+  static size_t total = 0;
+  if (!total) {
+    size_t f = 0, t = 0;
+    if (cudaMemGetInfo(&f, &t) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    total = t;
+  }
+  return total;
+}
+
+int resolve_path(const GemmProblem& p, int path, int moduli) {
+  const bool oz = ozaki_supported(p), tf = tf32x3_supported(p);
+  if (path == SPLAB_PATH_TF32X3) return tf ? SPLAB_PATH_TF32X3 : SPLAB_PATH_DMMA;
+  if (path == SPLAB_PATH_OZAKI) return oz ? SPLAB_PATH_OZAKI : SPLAB_PATH_DMMA;
+  if (path == SPLAB_PATH_DMMA || p.m <= 0 || p.n <= 0 || p.k <= 0) return SPLAB_PATH_DMMA;
+  const size_t cap = device_total_memory() / 4;
+  int best = SPLAB_PATH_DMMA;
+  double best_ms = model::dmma_ms(p);
+  if (oz && ozaki_workspace_bytes(p, moduli) <= cap) {
+    const double t = model::ozaki_ms(p);
+    if (t < 0.9 * best_ms) {
+      best = SPLAB_PATH_OZAKI;
+      best_ms = t;
+    }
+  }
+  if (tf && tf32x3_workspace_bytes(p) <= cap) {
+    const double t = model::tf32x3_ms(p);
+    if (t < 0.9 * best_ms) best = SPLAB_PATH_TF32X3;
+  }
+  return best;
 }
 
 __global__ void block_cyclic_info_kernel(int64_t rb, int64_t cb, int64_t gr, int64_t gc,
@@ -175,8 +247,7 @@ int splab_gemm_path(int dtype, int path, int opA, int opB, int64_t m, int64_t n,
   p.n = n;
   p.k = k;
   if (dtype < 0 || dtype > 3 || m <= 0 || n <= 0 || k < 0) return SPLAB_PATH_DMMA;
-  if (use_tf32x3(p, path)) return SPLAB_PATH_TF32X3;
-  return use_ozaki(p, path) ? SPLAB_PATH_OZAKI : SPLAB_PATH_DMMA;
+  return resolve_path(p, path, 0);
 }
 
 size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t m, int64_t n,
@@ -189,8 +260,9 @@ size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t 
   p.m = m;
   p.n = n;
   p.k = k;
-  if (use_tf32x3(p, path)) return tf32x3_workspace_bytes(p);
-  if (use_ozaki(p, path)) return ozaki_workspace_bytes(p, ozakiModuli);
+  const int rp = resolve_path(p, path, ozakiModuli);
+  if (rp == SPLAB_PATH_TF32X3) return tf32x3_workspace_bytes(p);
+  if (rp == SPLAB_PATH_OZAKI) return ozaki_workspace_bytes(p, ozakiModuli);
   return dmma_plan(p, num_sms()).workspace_bytes;
 }
 
@@ -206,8 +278,10 @@ int splab_gemm_check(int dtype, int path, int opA, int opB, int64_t m, int64_t n
   p.k = k;
   if (cudaStreamSynchronize(st) != cudaSuccess) return SPLAB_ERR_LAUNCH;
   if (m <= 0 || n <= 0 || !workspace) return SPLAB_OK;
-  if (use_tf32x3(p, path)) return tf32x3_status(p, workspace, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
-  if (!use_ozaki(p, path)) return SPLAB_OK;
+  const int rp = resolve_path(p, path, ozakiModuli);
+  if (rp == SPLAB_PATH_TF32X3)
+    return tf32x3_status(p, workspace, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
+  if (rp != SPLAB_PATH_OZAKI) return SPLAB_OK;
   return ozaki_status(p, ozakiModuli, workspace, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
 }
 
@@ -224,11 +298,12 @@ int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int6
                                fill, ro, co);
   cudaError_t err;
   if (ozakiModuli != 0 && (ozakiModuli < 8 || ozakiModuli > 16)) return SPLAB_ERR_INVALID;
-  if (use_tf32x3(p, path)) {
+  const int rp = resolve_path(p, path, ozakiModuli);
+  if (rp == SPLAB_PATH_TF32X3) {
     const size_t need = tf32x3_workspace_bytes(p);
     if (need > workspaceBytes || (need && !workspace)) return SPLAB_ERR_WORKSPACE;
     err = tf32x3_gemm(p, workspace, workspaceBytes, st);
-  } else if (use_ozaki(p, path)) {
+  } else if (rp == SPLAB_PATH_OZAKI) {
     const size_t need = ozaki_workspace_bytes(p, ozakiModuli);
     if (need > workspaceBytes || (need && !workspace)) return SPLAB_ERR_WORKSPACE;
     err = ozaki_gemm(p, ozakiModuli, workspace, workspaceBytes, st);
