@@ -2,6 +2,7 @@
 (splab_gemm), device-resident operands, CUDA events on a private stream.
 
     python -m spla_b200.timing complex128:2:1024:1024:250000 [more specs]
+    python -m spla_b200.timing --sweep     # every path and AUTO on a grid
 
 A spec is dtype:path:m:n:k with dtype in {float32, float64, complex64,
 complex128} and path 0 auto, 1 DMMA, 2 Ozaki, 3 3xTF32; the problem is
@@ -80,7 +81,26 @@ def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: i
             "workspace_GB": round(ws_bytes / 1e9, 2)}
 
 
+def sweep():
+    """Every path and AUTO's choice on a grid of square ssb problems: one JSON
+    line per (dtype, m = n, k) with the time (ms) of each path."""
+    for dt in ("complex128", "float64", "complex64", "float32"):
+        paths = (0, 1, 2) if dt in ("complex128", "float64") else (0, 1, 2, 3)
+        for (m, k) in [(128, 8192), (256, 8192), (256, 32768), (512, 16384), (512, 65536),
+                       (1024, 16384), (2048, 8192)]:
+            row = {"dtype": dt, "m": m, "n": m, "k": k}
+            for p in paths:
+                r = run(dt, p, m, m, k, steps=3, warmup=1)
+                row[f"ms_path{p}"] = r["ms"]
+                if p == 0:
+                    row["auto_resolves_to"] = r["resolved_path"]
+            print(json.dumps(row), flush=True)
+
+
 def main(argv):
+    if argv == ["--sweep"]:
+        sweep()
+        return
     for spec in argv:
         d, p, m, n, k = spec.split(":")
         print(json.dumps(run(d, int(p), int(m), int(n), int(k))), flush=True)
