@@ -355,6 +355,7 @@ struct GemmParams {
   int nb;            // rows of B per modulus
   int kblocks;       // kp / 128
   int nchunks;       // ceil(kblocks / kChunkBlocks)
+  int chunk_blocks;  // k-blocks per chunk: ceil(kblocks / nchunks) <= kChunkBlocks
   int nmod;
   int t0;            // first modulus of this launch (units cover t0 ..)
   int tiles_m, tiles_n;
@@ -434,8 +435,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     bool ok = g.stall_test == 0;
     for (int u = blockIdx.x; u < g.total_units && ok; u += gridDim.x) {
       const Unit w = decode_unit(u, g);
-      const int kb0 = w.c * kChunkBlocks;
-      const int kb1 = min(g.kblocks, kb0 + kChunkBlocks);
+      const int kb0 = w.c * g.chunk_blocks;
+      const int kb1 = min(g.kblocks, kb0 + g.chunk_blocks);
       const int arow = w.t * g.m + w.tm * BM;
       const int brow = w.t * g.nb + w.tn * BN;
       for (int kb = kb0; kb < kb1; ++kb) {
@@ -471,8 +472,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     bool ok = true;
     for (int u = blockIdx.x; u < g.total_units && ok; u += gridDim.x) {
       const Unit w = decode_unit(u, g);
-      const int kb0 = w.c * kChunkBlocks;
-      const int kb1 = min(g.kblocks, kb0 + kChunkBlocks);
+      const int kb0 = w.c * g.chunk_blocks;
+      const int kb1 = min(g.kblocks, kb0 + g.chunk_blocks);
       if (!mbar_wait(acce_bar(accb), acc_phase[accb] ^ 1u, abort, g.wait_limit_ns)) {
         ok = false;
         break;
@@ -664,7 +665,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     for (int u = pair; u < g.total_units && ok; u += npairs) {
       int t, c, tm, tn;
       unit_of(u, t, c, tm, tn);
-      const int kb0 = c * kChunkBlocks, kb1 = min(g.kblocks, kb0 + kChunkBlocks);
+      const int kb0 = c * g.chunk_blocks, kb1 = min(g.kblocks, kb0 + g.chunk_blocks);
       const int arow = t * g.m + tm * 256 + int(rank) * 128;
       const int brow = t * g.nb + tn * (256 * NT) + int(rank) * 128;
       for (int kb = kb0; kb < kb1; ++kb) {
@@ -696,7 +697,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     for (int u = pair; u < g.total_units && ok; u += npairs) {
       int t, c, tm, tn;
       unit_of(u, t, c, tm, tn);
-      const int kb0 = c * kChunkBlocks, kb1 = min(g.kblocks, kb0 + kChunkBlocks);
+      const int kb0 = c * g.chunk_blocks, kb1 = min(g.kblocks, kb0 + g.chunk_blocks);
       if (!mbar_wait(acce_bar(accb), acc_phase[accb] ^ 1u, abort, g.wait_limit_ns)) {
         ok = false;
         break;
@@ -1180,6 +1181,8 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
     g.nb = L.nb;
     g.kblocks = int(L.kp / BKB);
     g.nchunks = (g.kblocks + kChunkBlocks - 1) / kChunkBlocks;
+    // equal chunks (each within the exact INT32 bound): equal work units
+    g.chunk_blocks = std::max(1, (g.kblocks + g.nchunks - 1) / std::max(1, g.nchunks));
     g.nmod = L.nmod;
     g.tiles_m = (L.rowsA + BM - 1) / BM;
     g.tiles_n = (L.nb + BN - 1) / BN;
@@ -1200,8 +1203,21 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
     const char* gk = std::getenv("SPLAB_OZAKI_GEMM");
     const bool pair = !(gk && gk[0] == '1');  // "1sm" selects the single-CTA kernel
     CUtensorMap mapA2, mapB2;
-    // pair tile 256 x 512 when B has at least 512 rows (SPLAB_OZAKI_NT=1|2 overrides)
-    int nt = L.nb >= 512 ? 2 : 1;
+    // pair tile 256 x 256 (two accumulator buffers: the epilogue of one unit
+    // overlaps the next unit's MMAs) unless the 256 x 512 tile (one A tile for
+    // two MMAs, one 512-column accumulator) needs fewer rounds of work units;
+    // with equal k-chunks the two measured within a few percent of each other
+    // per operation (SPLAB_OZAKI_NT=1|2 overrides)
+    int nt = 1;
+    if (L.nb >= 512) {
+      const int pairs = std::max(1, sm_count() / 2);
+      auto rounds = [&](int w) {
+        const long long units = (long long)g.nmod * g.nchunks * ((L.rowsA + 255) / 256) *
+                                ((L.nb + 256 * w - 1) / (256 * w));
+        return double((units + pairs - 1) / pairs);
+      };
+      nt = rounds(2) * 2.0 < rounds(1) ? 2 : 1;
+    }
     if (const char* v = std::getenv("SPLAB_OZAKI_NT")) {
       if (v[0] == '1') nt = 1;
       if (v[0] == '2') nt = 2;

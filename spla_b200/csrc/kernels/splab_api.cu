@@ -100,8 +100,8 @@ GemmProblem make_problem(int dtype, int opA, int opB, int64_t m, int64_t n, int6
 // the device memory. The model's constants were measured on B200 (complex and
 // real, m = n from 128 to 2048, k from 8192 to 65536, and the k = 250000
 // configurations): DMMA at 33 / 29 TFLOP/s (complex / real) plus 0.05 ms; the
-// Ozaki path as slicing (6.3e-13 s per real element and modulus, plus the
-// norms' read at 6 TB/s), INT8 GEMM at 2.5 POP/s scaled by how evenly its work
+// Ozaki path as slicing (6.0e-13 s per real element and modulus, plus the
+// norms' read at 6 TB/s), INT8 GEMM at 2.8 POP/s scaled by how evenly its work
 // units fill the 74 CTA pairs, reconstruction (3e-12 s per real output and
 // modulus) and 0.08 ms; 3xTF32 as splitting (bytes at 5.5 TB/s), three TF32
 // products at 480 TFLOP/s scaled by the same fill, and 0.05 ms. The choice only
@@ -129,11 +129,10 @@ double ozaki_ms(const GemmProblem& p) {
   const double K2 = c ? 2.0 * p.k : double(p.k), nb = c ? 2.0 * p.n : double(p.n);
   const double kp = std::ceil(K2 / 128.0) * 128.0;
   const double reals = double(p.m + p.n) * K2;
-  const double slice = 6.3e-13 * reals * nmod + reals * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12;
-  const double nt = nb >= 512 ? 2.0 : 1.0;
-  const double tiles = std::ceil(p.m / 256.0) * std::ceil(nb / (256.0 * nt));
+  const double slice = 6.0e-13 * reals * nmod + reals * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12;
+  const double tiles = std::ceil(p.m / 256.0) * std::ceil(nb / 256.0);
   const double chunks = std::ceil(kp / 128.0 / 976.0);
-  const double gemm = 2.0 * nmod * p.m * nb * kp / (2.5e15 * fill(nmod * chunks * tiles));
+  const double gemm = 2.0 * nmod * p.m * nb * kp / (2.8e15 * fill(nmod * chunks * tiles));
   const double recon = 3e-12 * p.m * nb * nmod;
   return (slice + gemm + recon) * 1e3 + 0.08;
 }
