@@ -719,16 +719,14 @@ def main():
         int8_ops = 2.0 * nmod * M * (2 * N) * (2 * K)  # residue GEMMs: m x 2n x 2k per modulus
         achieved = int8_ops / (k_ms / 1e3) / 1e12
         peak = peaks.get("int8_tops")
-        # DRAM bytes of one full-size GEMM launch, from the ncu capture of the same kernel on
-        # m=n=1024, k=20000 (2.193 GB read, 0.120 GB written per launch): reads scale with the
-        # k-blocks processed (313 -> 3907), the accumulated-residue writes with the k-chunks
-        # (1 -> 5)
-        traffic = (2.193e9 * (2 * K / 128.0) / 313.0 + 0.120e9 * max(1, -(-2 * K // 124928))
-                   if (M, N) == (1024, 1024) else None)
+        # DRAM bytes of one GEMM launch of this workload (m=n=1024, k=250000), from a one-pass
+        # ncu capture of oz_gemm_pair on it: 52.89 GB read + 0.472 GB written
+        traffic = 52.89e9 + 0.472e9 if (M, N, K) == (1024, 1024, 250000) else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
                 "frac": (achieved / peak) if peak else None, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_{read,write}.sum of oz_gemm_pair<2> at "
-                                  "m=n=1024 k=20000, scaled to this k (k-blocks, k-chunks)",
+                "traffic_source": "ncu dram__bytes_{read,write}.sum of oz_gemm_pair, one-pass "
+                                  "capture of this launch (profiles/oz_gemm_pair_int8_traffic_"
+                                  "zgemm_m1024_k250000.md)",
                 "algorithmic_residue_bytes": float(OZAKI_MODULI) * (M + 2 * N) * 2 * K,
                 "kernel": "oz_gemm_pair (tcgen05.mma.cta_group::2.kind::i8, TMA, TMEM)",
                 "peak_source": "measured here: cuBLASLt int8 GEMM 8192^3 via torch._int_mm",
