@@ -348,10 +348,11 @@ def _events(torch):
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def workload_sbs(torch, spla, steps, warmup):
+def workload_sbs(torch, spla, steps, warmup, path=None):
     """pzgemm_sbs subspace rotation: A 200000 x 2048 (Gaussian/sqrt(k)), B a
     Haar-random unitary 2048 x 2048 (QR of a complex Gaussian, phases of
-    diag(R) folded in), C 200000 x 2048 U[-1,1], alpha = beta = 1."""
+    diag(R) folded in), C 200000 x 2048 U[-1,1], alpha = beta = 1. The path
+    is AUTO (None), FP64 DMMA (1) or Ozaki INT8 (2)."""
     import numpy as np
     import oracle
     mloc, n, k = 200000, 2048, 2048
@@ -369,6 +370,10 @@ def workload_sbs(torch, spla, steps, warmup):
     C = C0.clone()
     flops = 8.0 * mloc * n * k
     ctx = spla.Context(spla.PU_GPU)
+    if path is not None:
+        ctx.set_fp64_path(path)
+    resolved = spla.lib().splab_gemm_path(3, spla.PATH_AUTO if path is None else path, 0, 0, mloc,
+                                          n, k)
     dist = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128,
                                                              128)
 
@@ -405,10 +410,11 @@ def workload_sbs(torch, spla, steps, warmup):
     got = C.cpu().numpy()[cols].ravel()
     err = oracle.rel_fro(got, ref)
     t = ms - ms_copy
-    return {"metric": "ZGEMM-SBS TFLOP/s (pzgemm_sbs, FP64 DMMA)", "value": flops / (t / 1e3) / 1e12,
+    name = {1: "FP64 DMMA", 2: "Ozaki INT8", 3: "3xTF32"}[resolved]
+    return {"metric": f"ZGEMM-SBS TFLOP/s (pzgemm_sbs, {name})", "value": flops / (t / 1e3) / 1e12,
             "unit": "TFLOP/s", "ms_per_step": t, "rel_err_vs_oracle_3cols": err,
             "config": {"workload": "pzgemm_sbs mLocal=200000 n=k=2048 alpha=beta=1, B unitary",
-                       "path": "dmma"}}
+                       "path": ("auto: " if path is None else "") + name}}
 
 
 def workload_ssbtr_float(torch, spla, steps, warmup, path=None):
@@ -582,7 +588,10 @@ def run_workload(name, steps, warmup):
     import torch
     import spla_b200 as spla
     torch.cuda.set_device(0)
-    fn = {"sbs": workload_sbs, "ssbtr_float": workload_ssbtr_float,
+    fn = {"sbs": workload_sbs,
+          "sbs_dmma": lambda t, s, st, w: workload_sbs(t, s, st, w, 1),
+          "sbs_ozaki": lambda t, s, st, w: workload_sbs(t, s, st, w, 2),
+          "ssbtr_float": workload_ssbtr_float,
           "ssbtr_float_dmma": lambda t, s, st, w: workload_ssbtr_float(t, s, st, w, 1),
           "ssbtr_float_ozaki": lambda t, s, st, w: workload_ssbtr_float(t, s, st, w, 2),
           "ssbtr_float_tf32x3": lambda t, s, st, w: workload_ssbtr_float(t, s, st, w, 3),
@@ -615,7 +624,8 @@ def main():
     ap.add_argument("--m", type=int, default=1024, help="m = n (profiling of smaller cases)")
     ap.add_argument("--k", type=int, default=250000, help="k (profiling of smaller cases)")
     ap.add_argument("--workload", default="zgemm_ssb",
-                    choices=["zgemm_ssb", "sbs", "ssbtr_float", "ssbtr_float_dmma",
+                    choices=["zgemm_ssb", "sbs", "sbs_dmma", "sbs_ozaki", "ssbtr_float",
+                             "ssbtr_float_dmma",
                              "ssbtr_float_ozaki", "ssbtr_float_tf32x3", "cgemm_ssb_dmma",
                              "cgemm_ssb_ozaki", "cgemm_ssb_tf32x3", "batch", "batch_c64",
                              "batch_ozaki", "batch_c64_ozaki", "batch_c64_tf32x3"])

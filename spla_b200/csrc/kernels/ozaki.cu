@@ -360,7 +360,8 @@ struct GemmParams {
   int t0;            // first modulus of this launch (units cover t0 ..)
   int tiles_m, tiles_n;
   int total_units;   // moduli of the launch * nchunks * tiles
-  int* R;            // accumulated residues [nmod][nb][m] (int32)
+  int* R;            // accumulated residues [nmod][nb][m] (int32), or
+  unsigned char* R8; // with a single k-chunk: the residues as bytes (no accumulation)
   int* status;       // set to 1 when a bounded wait gave up
   const int* active; // CTA-pair kernel: list of tiles to compute (fill mode), or null = all
   int n_active;
@@ -373,13 +374,28 @@ struct Unit {
   int t, c, tm, tn;
 };
 
+// Tile raster within one (modulus, k-chunk): bands of kBandTiles row tiles,
+// row tiles fastest within a band. The units in flight at one time cover a
+// few row tiles of A and a few column tiles of B, so that each A tile is
+// read from DRAM once even when A is much taller than L2 holds (a plain
+// row-fastest order re-reads all of A once per column tile).
+constexpr int kBandTiles = 8;
+__host__ __device__ __forceinline__ void band_tile(int tile, int tiles_m, int tiles_n, int& tm,
+                                                   int& tn) {
+  const int band_units = kBandTiles * tiles_n;
+  const int band = tile / band_units, r = tile - band * band_units;
+  const int left = tiles_m - band * kBandTiles;
+  const int rows = left < kBandTiles ? left : kBandTiles;
+  tm = band * kBandTiles + r % rows;
+  tn = r / rows;
+}
+
 __device__ __forceinline__ Unit decode_unit(int u, const GemmParams& g) {
   Unit r;
   const int tiles = g.tiles_m * g.tiles_n;
   const int tile = u % tiles;
   const int rest = u / tiles;
-  r.tm = tile % g.tiles_m;
-  r.tn = tile / g.tiles_m;
+  band_tile(tile, g.tiles_m, g.tiles_n, r.tm, r.tn);
   r.c = rest % g.nchunks;
   r.t = g.t0 + rest / g.nchunks;
   return r;
@@ -535,7 +551,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             if (j < g.nb) {
               int r = int(v[c]) % p;
               if (r < 0) r += p;
-              atomicAdd(Rt + int64_t(j) * g.m + i, r);
+              if (g.R8)
+                g.R8[int64_t(w.t) * g.nb * g.m + int64_t(j) * g.m + i] = (unsigned char)r;
+              else
+                atomicAdd(Rt + int64_t(j) * g.m + i, r);
             }
           }
         }
@@ -649,9 +668,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
   const int ntl = g.active ? g.n_active : tiles;
   auto unit_of = [&](int u, int& t, int& c, int& tm, int& tn) {
     const int tl = u % ntl, rest = u / ntl;
-    const int tile = g.active ? g.active[tl] : tl;
-    tm = tile % g.tiles_m;
-    tn = tile / g.tiles_m;
+    if (g.active) {  // explicit list: tm + tn * tiles_m
+      const int tile = g.active[tl];
+      tm = tile % g.tiles_m;
+      tn = tile / g.tiles_m;
+    } else {
+      band_tile(tl, g.tiles_m, g.tiles_n, tm, tn);
+    }
     c = rest % g.nchunks;
     t = g.t0 + rest / g.nchunks;
   };
@@ -765,7 +788,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             if (j < g.nb) {
               int r = int(v[cc]) % p;
               if (r < 0) r += p;
-              atomicAdd(Rt + int64_t(j) * g.m + i, r);
+              if (g.R8)
+                g.R8[int64_t(t) * g.nb * g.m + int64_t(j) * g.m + i] = (unsigned char)r;
+              else
+                atomicAdd(Rt + int64_t(j) * g.m + i, r);
             }
           }
         }
@@ -798,61 +824,146 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
 // --------------------------------------------------------------------------
 // 4. reconstruction
 
-// C(i, j) <- alpha * 2^(-sigma_i - tau_j) * X + beta * C(i, j); complex: real
-// part from R row j, imaginary part from R row n + j.
+// x * 2^e, correctly rounded: a multiplication by the power of two when the
+// result stays normal (|x| is an integer below 2^128 or zero), ldexp otherwise.
+__device__ __forceinline__ double scale_pow2(double x, int e) {
+  if (e >= -1022 && e <= 895)
+    return x * __longlong_as_double((long long)(e + 1023) << 52);
+  return ldexp(x, e);
+}
+
+// C(i, j) <- alpha * x + beta * C(i, j) (x = xr + i xi for complex types)
 template <int DT>
-__global__ void oz_reconstruct(const int* __restrict__ R, int m, int n, int nb,
+__device__ __forceinline__ void store_c(void* C, int64_t ci, double xr, double xi, double alr,
+                                        double ali, double ber, double bei, bool read_c) {
+  double outr = alr * xr - ali * xi, outi = alr * xi + ali * xr;
+  if constexpr (DT == kC64) {
+    double2* c = static_cast<double2*>(C) + ci;
+    if (read_c) {
+      const double2 old = *c;
+      outr += ber * old.x - bei * old.y;
+      outi += ber * old.y + bei * old.x;
+    }
+    *c = make_double2(outr, outi);
+  } else if constexpr (DT == kC32) {
+    float2* c = static_cast<float2*>(C) + ci;
+    if (read_c) {
+      const float2 old = *c;
+      outr += ber * double(old.x) - bei * double(old.y);
+      outi += ber * double(old.y) + bei * double(old.x);
+    }
+    *c = make_float2(float(outr), float(outi));
+  } else if constexpr (DT == kR64) {
+    double* c = static_cast<double*>(C) + ci;
+    *c = read_c ? fma(ber, *c, outr) : outr;
+  } else {
+    float* c = static_cast<float*>(C) + ci;
+    *c = float(read_c ? fma(ber, double(*c), outr) : outr);
+  }
+}
+
+// C(i, j) <- alpha * 2^(-sigma_i - tau_j) * X + beta * C(i, j); complex: real
+// part from R row j, imaginary part from R row n + j. R holds int32 sums of
+// per-chunk residues or, with one k-chunk, the residues as bytes (RT). Threads
+// run along i (contiguous in R and C), blocks along j: no index division.
+// V4 (byte residues, m % 4 == 0): each thread takes four consecutive rows and
+// loads their residues of one modulus as one 32-bit word.
+template <int DT, typename RT, bool V4>
+__global__ void oz_reconstruct(const RT* __restrict__ R, int m, int n, int nb,
                                const int* __restrict__ sigA, const int* __restrict__ sigB,
                                void* C, int64_t ldc, double alr, double ali, double ber,
                                double bei, int fill, int64_t ro, int64_t co, int tile_m, int tile_n,
                                ReconParams rp) {
   constexpr bool CPLX = dtype_is_complex(DT);
-  const int64_t total = int64_t(m) * n;
-  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
-       idx += int64_t(gridDim.x) * blockDim.x) {
-    const int i = int(idx % m), j = int(idx / m);
-    if (fill != 0) {
-      const int64_t ti = (i / tile_m) * int64_t(tile_m), tj = (j / tile_n) * int64_t(tile_n);
-      if (!tile_is_active(fill, ti, tj, ::min((int64_t)tile_m, (int64_t)m - ti), ::min((int64_t)tile_n, (int64_t)n - tj),
-                          ro, co))
-        continue;
-    }
-    int r[kMaxModuli];
-    const int64_t plane = int64_t(nb) * m;
-    for (int t = 0; t < rp.n; ++t) r[t] = R[t * plane + int64_t(j) * m + i];
-    const int e = -(sigA[i] + sigB[j]);
-    const double xr = ldexp(crt_value(r, rp), e);
-    double xi = 0.0;
-    if (CPLX) {
-      for (int t = 0; t < rp.n; ++t) r[t] = R[t * plane + int64_t(n + j) * m + i];
-      xi = ldexp(crt_value(r, rp), e);
-    }
-    double outr = alr * xr - ali * xi, outi = alr * xi + ali * xr;
-    const bool read_c = (ber != 0.0 || bei != 0.0);
-    const int64_t ci = i + int64_t(j) * ldc;
-    if constexpr (DT == kC64) {
-      double2* c = static_cast<double2*>(C) + ci;
-      if (read_c) {
-        const double2 old = *c;
-        outr += ber * old.x - bei * old.y;
-        outi += ber * old.y + bei * old.x;
+  constexpr int NV = V4 ? 4 : 1;
+  const int64_t plane = int64_t(nb) * m;
+  const bool read_c = (ber != 0.0 || bei != 0.0);
+  for (int j = blockIdx.y; j < n; j += gridDim.y) {
+    const int tauj = sigB[j];
+    const int64_t tj = (j / tile_n) * int64_t(tile_n);
+    for (int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * NV; i0 < m;
+         i0 += gridDim.x * blockDim.x * NV) {
+      if (fill != 0) {  // tile_m is a multiple of 4: the NV rows share a tile
+        const int64_t ti = (i0 / tile_m) * int64_t(tile_m);
+        if (!tile_is_active(fill, ti, tj, ::min((int64_t)tile_m, (int64_t)m - ti),
+                            ::min((int64_t)tile_n, (int64_t)n - tj), ro, co))
+          continue;
       }
-      *c = make_double2(outr, outi);
-    } else if constexpr (DT == kC32) {
-      float2* c = static_cast<float2*>(C) + ci;
-      if (read_c) {
-        const float2 old = *c;
-        outr += ber * double(old.x) - bei * double(old.y);
-        outi += ber * double(old.y) + bei * double(old.x);
+      const RT* src = R + int64_t(j) * m + i0;
+      if constexpr (V4) {
+        unsigned wr[kMaxUsableModuli], wi[kMaxUsableModuli];
+        const unsigned* s4 = reinterpret_cast<const unsigned*>(src);
+        const int64_t p4 = plane / 4;
+#pragma unroll
+        for (int t = 0; t < kMaxUsableModuli; ++t)
+          if (t < rp.n) wr[t] = s4[t * p4];
+        if (CPLX) {
+          const unsigned* s4i = s4 + int64_t(n) * m / 4;
+#pragma unroll
+          for (int t = 0; t < kMaxUsableModuli; ++t)
+            if (t < rp.n) wi[t] = s4i[t * p4];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int i = i0 + q;
+          const int e = -(sigA[i] + tauj);
+          int r[kMaxUsableModuli];
+#pragma unroll
+          for (int t = 0; t < kMaxUsableModuli; ++t)
+            if (t < rp.n) r[t] = int((wr[t] >> (8 * q)) & 255u);
+          const double xr = scale_pow2(crt_value(r, rp), e);
+          double xi = 0.0;
+          if (CPLX) {
+#pragma unroll
+            for (int t = 0; t < kMaxUsableModuli; ++t)
+              if (t < rp.n) r[t] = int((wi[t] >> (8 * q)) & 255u);
+            xi = scale_pow2(crt_value(r, rp), e);
+          }
+          store_c<DT>(C, i + int64_t(j) * ldc, xr, xi, alr, ali, ber, bei, read_c);
+        }
+      } else {
+        const int i = i0;
+        int r[kMaxUsableModuli];
+#pragma unroll
+        for (int t = 0; t < kMaxUsableModuli; ++t)
+          if (t < rp.n) r[t] = int(src[t * plane]);
+        const int e = -(sigA[i] + tauj);
+        const double xr = scale_pow2(crt_value(r, rp), e);
+        double xi = 0.0;
+        if (CPLX) {
+          src += int64_t(n) * m;
+#pragma unroll
+          for (int t = 0; t < kMaxUsableModuli; ++t)
+            if (t < rp.n) r[t] = int(src[t * plane]);
+          xi = scale_pow2(crt_value(r, rp), e);
+        }
+        store_c<DT>(C, i + int64_t(j) * ldc, xr, xi, alr, ali, ber, bei, read_c);
       }
-      *c = make_float2(float(outr), float(outi));
-    } else if constexpr (DT == kR64) {
-      double* c = static_cast<double*>(C) + ci;
-      *c = read_c ? fma(ber, *c, outr) : outr;
-    } else {
-      float* c = static_cast<float*>(C) + ci;
-      *c = float(read_c ? fma(ber, double(*c), outr) : outr);
     }
+  }
+}
+
+// At(kk, i) <- A(i, kk): op(A) = N operands (A stored m-major) are copied
+// k-major so that the row norms and the slicing read them like op(A) = T.
+// 32 x 32 tiles through shared memory: reads run along i, writes along kk.
+template <typename E>
+__global__ void oz_transpose(const E* __restrict__ A, int64_t lda, int m, int64_t k,
+                             E* __restrict__ At, int64_t ldat) {
+  __shared__ E tile[32][33];
+  const int i0 = blockIdx.x * 32;
+  for (int64_t k0 = int64_t(blockIdx.y) * 32; k0 < k; k0 += int64_t(gridDim.y) * 32) {
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int i = i0 + threadIdx.x;
+      const int64_t kk = k0 + r;
+      if (i < m && kk < k) tile[r][threadIdx.x] = A[i + kk * lda];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int i = i0 + r;
+      const int64_t kk = k0 + threadIdx.x;
+      if (i < m && kk < k) At[int64_t(i) * ldat + kk] = tile[threadIdx.x][r];
+    }
+    __syncthreads();
   }
 }
 
@@ -863,7 +974,10 @@ struct Layout {
   int nmod;
   int64_t K2, kp;          // real depth, padded to 128
   int rowsA, rowsB, nb;    // A rows, B source rows, B residue rows
-  size_t off_sigA, off_sigB, off_resA, off_resB, off_R, off_status, off_tiles, total;
+  bool at;                 // op(A) = N: A is first copied k-major into At
+  bool r8;                 // one k-chunk: the residues of C are stored as bytes
+  int64_t ldAt;            // leading dimension of At (elements of A's type)
+  size_t off_sigA, off_sigB, off_resA, off_resB, off_R, off_At, off_status, off_tiles, total;
 };
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -878,6 +992,9 @@ Layout layout_of(const GemmProblem& p, int moduli) {
   L.rowsA = int(p.m);
   L.rowsB = int(p.n);
   L.nb = cplx ? int(2 * p.n) : int(p.n);
+  L.at = p.opA == 0;
+  L.r8 = (L.kp / BKB + kChunkBlocks - 1) / kChunkBlocks == 1;
+  L.ldAt = L.at ? (p.k + 7) / 8 * 8 : 0;
   size_t off = 0;
   L.off_sigA = off;
   off = align256(off + sizeof(int) * L.rowsA);
@@ -888,7 +1005,9 @@ Layout layout_of(const GemmProblem& p, int moduli) {
   L.off_resB = off;
   off = align256(off + size_t(L.nmod) * L.nb * L.kp);
   L.off_R = off;
-  off = align256(off + sizeof(int) * size_t(L.nmod) * L.nb * L.rowsA);
+  off = align256(off + (L.r8 ? 1 : sizeof(int)) * size_t(L.nmod) * L.nb * L.rowsA);
+  L.off_At = off;
+  off = align256(off + size_t(dtype_bytes(p.dtype)) * size_t(L.rowsA) * size_t(L.ldAt));
   L.off_status = off;
   off = align256(off + 256);
   L.off_tiles = off;
@@ -939,7 +1058,7 @@ size_t ozaki_workspace_bytes(const GemmProblem& p, int moduli) {
 }
 
 bool ozaki_supported(const GemmProblem& p) {
-  return p.opA != 0 && p.opB == 0 && p.m <= (1 << 24) && p.n <= (1 << 23);
+  return p.opB == 0 && p.m <= (1 << 24) && p.n <= (1 << 23);
 }
 
 namespace {
@@ -1108,24 +1227,53 @@ int modulus_groups(const oz::Layout& L) {
 }
 }  // namespace
 
-cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_bytes,
+namespace {
+// At <- A k-major (op(A) = N operands); see oz_transpose
+cudaError_t transpose_a(const GemmProblem& p, const oz::Layout& L, void* At, cudaStream_t st) {
+  const dim3 block(32, 8);
+  const dim3 grid(unsigned((p.m + 31) / 32),
+                  unsigned(std::min<int64_t>((p.k + 31) / 32, 65535)));
+  auto run = [&](auto tag) {
+    using E = decltype(tag);
+    oz::oz_transpose<E><<<grid, block, 0, st>>>(static_cast<const E*>(p.A), p.lda, int(p.m),
+                                                p.k, static_cast<E*>(At), L.ldAt);
+  };
+  switch (p.dtype) {
+    case kC64: run(double2{}); break;
+    case kC32: run(float2{}); break;
+    case kR64: run(double{}); break;
+    default: run(float{}); break;
+  }
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_bytes,
                        cudaStream_t st) {
   using namespace oz;
-  if (!ozaki_supported(p)) return cudaErrorNotSupported;
-  if (p.m <= 0 || p.n <= 0) return cudaSuccess;
-  const Layout L = layout_of(p, moduli);
+  if (!ozaki_supported(p_in)) return cudaErrorNotSupported;
+  if (p_in.m <= 0 || p_in.n <= 0) return cudaSuccess;
+  const Layout L = layout_of(p_in, moduli);
   if (ws_bytes < L.total || !ws) return cudaErrorInvalidValue;
   const Crt crt = make_crt(L.nmod);
-  const bool cplx = dtype_is_complex(p.dtype);
+  const bool cplx = dtype_is_complex(p_in.dtype);
   char* w = static_cast<char*>(ws);
   int* sigA = reinterpret_cast<int*>(w + L.off_sigA);
   int* sigB = reinterpret_cast<int*>(w + L.off_sigB);
   int8_t* resA = reinterpret_cast<int8_t*>(w + L.off_resA);
   int8_t* resB = reinterpret_cast<int8_t*>(w + L.off_resB);
   int* R = reinterpret_cast<int*>(w + L.off_R);
+  unsigned char* R8 = L.r8 ? reinterpret_cast<unsigned char*>(w + L.off_R) : nullptr;
   int* status = reinterpret_cast<int*>(w + L.off_status);
 
   cudaError_t e;
+  // op(A) = N: everything below reads the k-major copy At as op(A) = T
+  GemmProblem p = p_in;
+  if (L.at && p.k > 0) {
+    p.A = w + L.off_At;
+    p.lda = L.ldAt;
+    p.opA = 1;
+  }
   const bool dbl = dtype_is_double(p.dtype);
   const int groups = modulus_groups(L);
   // Large problems use the side streams: the row norms of B (a pure read)
@@ -1144,6 +1292,7 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
       scale_operands<float>(L, crt, p, cplx, sigA, sigB, which, s);
   };
   phase_mark(0, false, st);
+  if (L.at && p.k > 0 && (e = transpose_a(p_in, L, w + L.off_At, st)) != cudaSuccess) return e;
   if (p.k > 0 && ps) {
     // A's norms alone (both are pure reads and would share the bandwidth),
     // then B's norms on the side stream while A is sliced
@@ -1158,7 +1307,9 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
     cudaMemsetAsync(sigA, 0, sizeof(int) * L.rowsA, st);
     cudaMemsetAsync(sigB, 0, sizeof(int) * L.rowsB, st);
   }
-  cudaMemsetAsync(R, 0, sizeof(int) * size_t(L.nmod) * L.nb * L.rowsA, st);
+  // byte residues are stored, not accumulated: every element the
+  // reconstruction reads is written by the GEMM
+  if (!L.r8) cudaMemsetAsync(R, 0, sizeof(int) * size_t(L.nmod) * L.nb * L.rowsA, st);
   cudaMemsetAsync(status, 0, sizeof(int), st);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (p.k <= 0) {
@@ -1188,6 +1339,7 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
     g.tiles_n = (L.nb + BN - 1) / BN;
     g.total_units = g.nmod * g.nchunks * g.tiles_m * g.tiles_n;
     g.R = R;
+    g.R8 = R8;
     g.status = status;
     g.wait_limit_ns = kWaitLimitNs;
     g.stall_test = 0;
@@ -1351,29 +1503,44 @@ cudaError_t ozaki_gemm(const GemmProblem& p, int moduli, void* ws, size_t ws_byt
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
 
   phase_mark(2, false, st);
-  ReconParams rp{};
-  rp.n = L.nmod;
-  for (int t = 0; t < L.nmod; ++t) {
-    rp.p[t] = crt.p[t];
-    rp.w_lo[t] = crt.w_lo[t];
-    rp.w_hi[t] = crt.w_hi[t];
-  }
-  rp.P_lo = crt.P_lo;
-  rp.P_hi = crt.P_hi;
-  rp.P_d = crt.P_d;
-  const int64_t total = p.m * p.n;
+  const ReconParams rp = make_recon(crt);
+  // threads along the rows of C (four rows each with byte residues and
+  // m % 4 == 0), blocks along its columns (grid-stride in both, about 64
+  // blocks of 256 threads per SM)
   const int threads = 256;
-  const unsigned blocks = unsigned(std::min<int64_t>((total + threads - 1) / threads, 148 * 32));
-  auto recon = [&](auto kern) {
-    kern<<<blocks, threads, 0, st>>>(R, L.rowsA, int(p.n), L.nb, sigA, sigB, p.C, p.ldc,
-                                     p.alpha[0], p.alpha[1], p.beta[0], p.beta[1], p.fill_mode,
-                                     p.fill_ro, p.fill_co, BM, cplx ? BN / 2 : BN, rp);
+  const bool v4 = R8 && L.rowsA % 4 == 0;
+  const int64_t rows_per_block = int64_t(threads) * (v4 ? 4 : 1);
+  const unsigned gy = unsigned(std::min<int64_t>(p.n, 65535));
+  const unsigned gx = unsigned(std::max<int64_t>(
+      1, std::min<int64_t>((p.m + rows_per_block - 1) / rows_per_block, (148 * 64 + gy - 1) / gy)));
+  auto recon = [&](auto kern, const auto* Rsrc) {
+    kern<<<dim3(gx, gy), threads, 0, st>>>(Rsrc, L.rowsA, int(p.n), L.nb, sigA, sigB, p.C, p.ldc,
+                                           p.alpha[0], p.alpha[1], p.beta[0], p.beta[1],
+                                           p.fill_mode, p.fill_ro, p.fill_co, BM,
+                                           cplx ? BN / 2 : BN, rp);
   };
-  switch (p.dtype) {
-    case kC64: recon(oz_reconstruct<kC64>); break;
-    case kC32: recon(oz_reconstruct<kC32>); break;
-    case kR64: recon(oz_reconstruct<kR64>); break;
-    default: recon(oz_reconstruct<kR32>); break;
+  using u8 = unsigned char;
+  if (v4) {
+    switch (p.dtype) {
+      case kC64: recon(oz_reconstruct<kC64, u8, true>, R8); break;
+      case kC32: recon(oz_reconstruct<kC32, u8, true>, R8); break;
+      case kR64: recon(oz_reconstruct<kR64, u8, true>, R8); break;
+      default: recon(oz_reconstruct<kR32, u8, true>, R8); break;
+    }
+  } else if (R8) {
+    switch (p.dtype) {
+      case kC64: recon(oz_reconstruct<kC64, u8, false>, R8); break;
+      case kC32: recon(oz_reconstruct<kC32, u8, false>, R8); break;
+      case kR64: recon(oz_reconstruct<kR64, u8, false>, R8); break;
+      default: recon(oz_reconstruct<kR32, u8, false>, R8); break;
+    }
+  } else {
+    switch (p.dtype) {
+      case kC64: recon(oz_reconstruct<kC64, int, false>, R); break;
+      case kC32: recon(oz_reconstruct<kC32, int, false>, R); break;
+      case kR64: recon(oz_reconstruct<kR64, int, false>, R); break;
+      default: recon(oz_reconstruct<kR32, int, false>, R); break;
+    }
   }
   phase_mark(2, true, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -64,8 +64,23 @@ struct ReconParams {
   int p[kMaxModuli];
   unsigned long long w_lo[kMaxModuli], w_hi[kMaxModuli];
   unsigned long long P_lo, P_hi;
-  double P_d;
+  double P_d, inv_P;
 };
+
+inline ReconParams make_recon(const Crt& c) {
+  ReconParams rp{};
+  rp.n = c.n;
+  for (int t = 0; t < c.n; ++t) {
+    rp.p[t] = c.p[t];
+    rp.w_lo[t] = c.w_lo[t];
+    rp.w_hi[t] = c.w_hi[t];
+  }
+  rp.P_lo = c.P_lo;
+  rp.P_hi = c.P_hi;
+  rp.P_d = c.P_d;
+  rp.inv_P = 1.0 / c.P_d;
+  return rp;
+}
 
 __host__ __device__ __forceinline__ unsigned long long mulhi64(unsigned long long a,
                                                                unsigned long long b) {
@@ -98,7 +113,12 @@ __host__ __device__ __forceinline__ double i128_to_double(unsigned long long x1,
 #endif
     const unsigned long long top = lz ? ((x1 << lz) | (x0 >> (64 - lz))) : x1;
     const unsigned long long rest = lz ? (x0 << lz) : x0;
-    mag = ldexp(double(top | (rest != 0 ? 1ull : 0ull)), 64 - lz);
+    const double t = double(top | (rest != 0 ? 1ull : 0ull));
+#ifdef __CUDA_ARCH__
+    mag = t * __longlong_as_double((long long)(1023 + 64 - lz) << 52);  // exact: 2^(64-lz)
+#else
+    mag = std::ldexp(t, 64 - lz);
+#endif
   }
   return neg ? -mag : mag;
 }
@@ -110,8 +130,11 @@ __host__ __device__ __forceinline__ double crt_value(const int* r, const ReconPa
   // S = sum_t W_t r_t accumulated per 32-bit limb of W_t: each product is
   // below 2^56 and at most 16 of them below 2^60, so the four 64-bit limb sums
   // need no carries (one 32x32->64 multiply-add per limb and modulus)
+  // (unrolled to the usable maximum so that r stays in registers)
   unsigned long long l0 = 0, l1 = 0, l2 = 0, l3 = 0;
-  for (int t = 0; t < rp.n; ++t) {
+#pragma unroll
+  for (int t = 0; t < kMaxUsableModuli; ++t) {
+    if (t >= rp.n) break;
     const unsigned long long rt = (unsigned int)r[t];
     l0 += rt * (unsigned int)rp.w_lo[t];
     l1 += rt * (unsigned int)(rp.w_lo[t] >> 32);
@@ -128,10 +151,13 @@ __host__ __device__ __forceinline__ double crt_value(const int* r, const ReconPa
   c = (c >> 32) + l3;
   const unsigned long long d3 = c & 0xFFFFFFFFull;
   const unsigned long long s0 = d0 | (d1 << 32), s1 = d2 | (d3 << 32), s2 = c >> 32;
-  // q = floor(S / P) estimated in double (q < n * 2^24), then S - qP
+  // q = floor(S / P) estimated in double, then S - qP. S / P < 16 * 2^24 and
+  // the estimate S_d * (1 / P_d) carries at most ~6 roundings of 2^-53
+  // relative, an absolute error below 2^-22: q is off by at most one, and one
+  // conditional add or subtract of P brings S - qP into [0, P).
   const double S_d = double(s2) * 3.402823669209385e38 + double(s1) * 18446744073709551616.0 +
                      double(s0);
-  unsigned long long q = (unsigned long long)floor(S_d / rp.P_d);
+  unsigned long long q = (unsigned long long)floor(S_d * rp.inv_P);
   // qP (192-bit)
   const unsigned long long qp0 = rp.P_lo * q, qp0h = mulhi64(rp.P_lo, q);
   const unsigned long long qp1l = rp.P_hi * q, qp1h = mulhi64(rp.P_hi, q);
@@ -144,7 +170,7 @@ __host__ __device__ __forceinline__ double crt_value(const int* r, const ReconPa
   unsigned long long br1 = (s1 < t1) || (s1 - t1 < br);
   unsigned long long x2 = s2 - t2 - br1;
   // fix-up into [0, P)
-  for (int it = 0; it < 3; ++it) {
+  {
     if ((long long)x2 < 0) {  // X < 0: X += P
       unsigned long long n0 = x0 + rp.P_lo;
       unsigned long long cy = n0 < x0;

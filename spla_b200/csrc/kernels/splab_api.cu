@@ -134,7 +134,10 @@ double ozaki_ms(const GemmProblem& p) {
   const double chunks = std::ceil(kp / 128.0 / 976.0);
   const double gemm = 2.0 * nmod * p.m * nb * kp / (2.8e15 * fill(nmod * chunks * tiles));
   const double recon = 3e-12 * p.m * nb * nmod;
-  return (slice + gemm + recon) * 1e3 + 0.08;
+  // op(A) = N: A is first copied k-major (one read, one write)
+  const double transpose =
+      p.opA == 0 ? 2.0 * p.m * K2 * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12 : 0.0;
+  return (slice + gemm + recon + transpose) * 1e3 + 0.08;
 }
 
 double tf32x3_ms(const GemmProblem& p) {

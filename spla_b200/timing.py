@@ -4,10 +4,11 @@
     python -m spla_b200.timing complex128:2:1024:1024:250000 [more specs]
     python -m spla_b200.timing --sweep     # every path and AUTO on a grid
 
-A spec is dtype:path:m:n:k with dtype in {float32, float64, complex64,
+A spec is dtype:path:m:n:k[:opA] with dtype in {float32, float64, complex64,
 complex128} and path 0 auto, 1 DMMA, 2 Ozaki, 3 3xTF32; the problem is
-C = op(A) B with op = conjugate transpose (complex) or transpose (real),
-Gaussian operands scaled by 1/sqrt(k). One JSON line per spec: total time,
+C = op(A) B with op = conjugate transpose (complex) or transpose (real)
+unless opA is given (0 = N: A is m x k, the pgemm_sbs shape), Gaussian
+operands scaled by 1/sqrt(k). One JSON line per spec: total time,
 TFLOP/s and the phase times the path reports (scale/slice, GEMM span,
 reduction or reconstruction, then one entry per GEMM launch).
 """
@@ -21,7 +22,7 @@ NPHASE = 3 + 16
 
 
 def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: int = 2,
-        moduli: int = 0) -> dict:
+        moduli: int = 0, opA: int | None = None) -> dict:
     import torch
     import spla_b200 as spla
     L = spla.lib()
@@ -31,7 +32,8 @@ def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: i
     A = torch.randn(m * k, dtype=tdt, device="cuda", generator=g) * (0.5 / k) ** 0.5
     B = torch.randn(n * k, dtype=tdt, device="cuda", generator=g) * (0.5 / k) ** 0.5
     C = torch.zeros(m * n, dtype=tdt, device="cuda")
-    op = 2 if A.is_complex() else 1
+    op = (2 if A.is_complex() else 1) if opA is None else opA
+    lda = m if op == 0 else k
     ws_bytes = spla.splab_gemm_workspace_size(dtype, path, op, 0, m, n, k, moduli)
     ws = torch.empty(max(1, ws_bytes), dtype=torch.uint8, device="cuda")
     st = torch.cuda.Stream()
@@ -42,7 +44,7 @@ def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: i
     handles = (ct.c_void_p * (2 * NPHASE))(*[e.cuda_event for e in pev])
 
     def step():
-        rc = spla.splab_gemm(dtype, path, op, 0, m, n, k, 1.0, A, k, B, k, 0.0, C, m,
+        rc = spla.splab_gemm(dtype, path, op, 0, m, n, k, 1.0, A, lda, B, k, 0.0, C, m,
                              moduli=moduli, workspace=ws, workspace_bytes=ws_bytes,
                              stream=st.cuda_stream)
         if rc != 0:
@@ -75,7 +77,7 @@ def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: i
     flops = (8.0 if A.is_complex() else 2.0) * m * n * k
     return {"dtype": dtype, "path": path,
             "resolved_path": L.splab_gemm_path(spla._dtype_of(dtype=dtype), path, op, 0, m, n, k),
-            "m": m, "n": n, "k": k, "ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 1),
+            "opA": op, "m": m, "n": n, "k": k, "ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 1),
             "phases_ms": [round(x, 3) for x in ph[:3]],
             "gemm_launch_ms": [round(x, 3) for x in ph[3:] if x > 0.05],
             "workspace_GB": round(ws_bytes / 1e9, 2)}
@@ -102,8 +104,9 @@ def main(argv):
         sweep()
         return
     for spec in argv:
-        d, p, m, n, k = spec.split(":")
-        print(json.dumps(run(d, int(p), int(m), int(n), int(k))), flush=True)
+        d, p, m, n, k, *op = spec.split(":")
+        print(json.dumps(run(d, int(p), int(m), int(n), int(k),
+                             opA=int(op[0]) if op else None)), flush=True)
 
 
 if __name__ == "__main__":

@@ -34,10 +34,7 @@ int main() {
         if (r != (s == t ? 1 : 0)) { printf("FAIL weight %d mod %d = %d\n", t, c.p[s], r); return 1; }
       }
     }
-    ReconParams rp{};
-    rp.n = n;
-    for (int t = 0; t < n; ++t) { rp.p[t] = c.p[t]; rp.w_lo[t] = c.w_lo[t]; rp.w_hi[t] = c.w_hi[t]; }
-    rp.P_lo = c.P_lo; rp.P_hi = c.P_hi; rp.P_d = c.P_d;
+    const ReconParams rp = make_recon(c);
     const i128 half = i128(P / 2);
     for (int it = 0; it < 20000; ++it) {
       i128 X;

@@ -1,8 +1,8 @@
 """Local gemm() over the full operation matrix: op(A), op(B) in {N, T, C}
 (all nine pairs) for the four dtypes, sizes that are not multiples of any
-tile, alpha/beta complex, padded leading dimensions, on the default path and
-on the FP64 DMMA path, against the double-double oracle (1e-14 double,
-1e-6 float)."""
+tile, alpha/beta complex, padded leading dimensions, on the default path, the
+FP64 DMMA path and the Ozaki path (op(B) = N; DMMA otherwise), against the
+double-double oracle (1e-14 double, 1e-6 float)."""
 import numpy as np
 import pytest
 
@@ -17,7 +17,7 @@ OPS = [(a, b) for a in (0, 1, 2) for b in (0, 1, 2)]
 
 
 @pytest.mark.parametrize("dt,tol", DT)
-@pytest.mark.parametrize("path", [spla.PATH_AUTO, spla.PATH_DMMA])
+@pytest.mark.parametrize("path", [spla.PATH_AUTO, spla.PATH_DMMA, spla.PATH_OZAKI])
 def test_gemm_all_ops(dt, tol, path):
     import torch
     ctx = spla.Context(spla.PU_GPU)

@@ -2,9 +2,11 @@
 
 Covers: complex A^H B and A^T B, real A^T B, partial tiles in both
 dimensions, several k-chunks (k*2 > 124928), alpha/beta with C offsets and
-ldc padding, k = 0, the modulus-count knob, the fill-mode tile skipping, and
-the failure path of the bounded device waits (no GPU fault: the producer
-issues no copies, every wait runs into a 50 ms bound)."""
+ldc padding, k = 0, the modulus-count knob, the fill-mode tile skipping,
+op(A) = N (pgemm_sbs and gemm: A copied k-major first) with one k-chunk (byte
+residues) and several (int32 sums), more row tiles than one band of the unit
+raster, and the failure path of the bounded device waits (no GPU fault: the
+producer issues no copies, every wait runs into a 50 ms bound)."""
 import os
 import subprocess
 import sys
@@ -124,6 +126,70 @@ def test_fill_lower_triangle():
     off = ~tri
     ok = np.isclose(g[off], r[off], rtol=1e-12, atol=1e-14) | (g[off] == c0[off])
     assert ok.all()
+
+
+@pytest.mark.parametrize("dt,tol", [(np.complex128, 1e-14), (np.float64, 1e-14),
+                                    (np.complex64, 1e-6), (np.float32, 1e-6)])
+def test_sbs_op_n(dt, tol):
+    """pgemm_sbs (C = alpha A B + beta C, A an m-major stripe) on the Ozaki
+    path: ragged sizes, padded leading dimensions, one k-chunk."""
+    cplx = np.dtype(dt).kind == "c"
+    mloc, n, k, pad = 701, 130, 900, 3
+    alpha, beta = ((0.5 - 0.25j), (1.0 + 0.5j)) if cplx else (0.5, 1.0)
+    A = buffer(dt, mloc + pad, k, 31, "gauss_k", k)
+    B = buffer(dt, k + pad, n, 32, "uniform11")
+    C = buffer(dt, mloc + pad, n, 33, "uniform11")
+    ctx = spla.Context(spla.PU_GPU)
+    ctx.set_fp64_path(spla.PATH_OZAKI)
+    d = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128, 128)
+    dC = _dev(C)
+    spla.pgemm_sbs(mloc, n, k, alpha, _dev(A), mloc + pad, _dev(B), k + pad, 0, 0, d, beta, dC,
+                   mloc + pad, ctx)
+    got = dC.cpu().numpy()
+    ref = C.copy()
+    assert oracle.pgemm_sbs(mloc, n, k, alpha, A, mloc + pad, B, k + pad, 0, 0, beta, ref,
+                            mloc + pad) == 0
+    blk = lambda x: x.reshape(n, mloc + pad)[:, :mloc]  # noqa: E731
+    assert oracle.rel_fro(blk(got), blk(ref)) <= tol
+    assert np.array_equal(got.reshape(n, mloc + pad)[:, mloc:], C.reshape(n, mloc + pad)[:, mloc:])
+
+
+def test_gemm_op_n_multi_chunk():
+    """gemm(N, N) on the Ozaki path with 2k > 124928 (two k-chunks: the
+    residues are int32 sums) and a padded A."""
+    m, n, k, lda = 90, 40, 70000, 97
+    alpha, beta = 1.0 - 0.5j, -0.5 + 0.25j
+    A = buffer(np.complex128, lda, k, 41, "gauss_k", k)
+    B = buffer(np.complex128, k, n, 42, "gauss_k", k)
+    C = buffer(np.complex128, m, n, 43, "uniform11")
+    ctx = spla.Context(spla.PU_GPU)
+    ctx.set_fp64_path(spla.PATH_OZAKI)
+    dC = _dev(C)
+    spla.gemm(0, 0, m, n, k, alpha, _dev(A), lda, _dev(B), k, beta, dC, m, ctx)
+    ref = C.copy()
+    assert oracle.gemm(0, 0, m, n, k, alpha, A, lda, B, k, beta, ref, m) == 0
+    assert oracle.rel_fro(dC.cpu().numpy(), ref) <= 1e-14
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.complex128])
+def test_tall_banded_raster(dt):
+    """More row tiles than one band (8 x 256 rows) with a partial last band,
+    on the ssb (op(A) = T/C) and gemm op(A) = N forms: every tile of the
+    banded unit order is computed once."""
+    import torch
+    cplx = np.dtype(dt).kind == "c"
+    m, n, k = 2600, 300, 400
+    C0, got, ref, ldc = run_ssb(dt, m, n, k, 2 if cplx else 1, dist="uniform11")
+    assert oracle.rel_fro(got, ref) <= 1e-14
+    A = buffer(dt, m, k, 51, "uniform11")
+    B = buffer(dt, k, n, 52, "uniform11")
+    ctx = spla.Context(spla.PU_GPU)
+    ctx.set_fp64_path(spla.PATH_OZAKI)
+    dC = torch.zeros(m * n, dtype=torch.complex128 if cplx else torch.float64, device="cuda")
+    spla.gemm(0, 0, m, n, k, 1.0, _dev(A), m, _dev(B), k, 0.0, dC, m, ctx)
+    ref = np.zeros(m * n, dtype=dt)
+    assert oracle.gemm(0, 0, m, n, k, 1.0, A, m, B, k, 0.0, ref, m) == 0
+    assert oracle.rel_fro(dC.cpu().numpy(), ref) <= 1e-14
 
 
 def test_bounded_wait_failure_path():

@@ -29,7 +29,10 @@ def test_explicit_paths():
     assert L.splab_gemm_path(C64, OZAKI, 2, 0, 64, 64, 100) == OZAKI
     assert L.splab_gemm_path(C64, TF3, 2, 0, 4096, 4096, 100000) == DMMA  # double: no 3xTF32
     assert L.splab_gemm_path(C32, TF3, 0, 0, 512, 512, 4096) == DMMA      # op(A) = N
-    assert L.splab_gemm_path(C64, spla.PATH_AUTO, 0, 0, 4096, 4096, 100000) == DMMA
+    assert L.splab_gemm_path(C64, OZAKI, 0, 1, 64, 64, 100) == DMMA       # op(B) = T
+    # op(A) = N on Ozaki (A copied k-major first): the subspace rotation shape
+    assert L.splab_gemm_path(C64, spla.PATH_AUTO, 0, 0, 200000, 2048, 2048) == OZAKI
+    assert L.splab_gemm_path(C64, spla.PATH_AUTO, 0, 0, 4096, 4096, 100000) == OZAKI
 
 
 def test_auto_workspace_matches_run():
