@@ -368,6 +368,9 @@ struct GemmParams {
   unsigned long long wait_limit_ns;  // bound on every barrier wait
   int stall_test;    // 1: the producer issues no copies (exercises the bounded waits)
   int p[kMaxModuli];
+  int c16[kMaxModuli], off[kMaxModuli];  // division-free v mod p (mod_residue)
+  unsigned M[kMaxModuli];
+  int epi_split;     // CTA-pair kernel: epilogue warps per TMEM lane quarter (1 or 2)
 };
 
 struct Unit {
@@ -537,7 +540,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
       const Unit w = decode_unit(u, g);
       if (!mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)) break;
       tc_fence_after();
-      const int p = g.p[w.t];
+      const int p = g.p[w.t], c16 = g.c16[w.t], off = g.off[w.t];
+      const unsigned M = g.M[w.t];
       const int i = w.tm * BM + row;
       const int j0 = w.tn * BN;
       int* Rt = g.R + int64_t(w.t) * g.nb * g.m;
@@ -549,8 +553,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
           for (int c = 0; c < 32; ++c) {
             const int j = j0 + c0 + c;
             if (j < g.nb) {
-              int r = int(v[c]) % p;
-              if (r < 0) r += p;
+              const int r = mod_residue(int(v[c]), p, c16, off, M);
               if (g.R8)
                 g.R8[int64_t(w.t) * g.nb * g.m + int64_t(j) * g.m + i] = (unsigned char)r;
               else
@@ -616,8 +619,14 @@ __device__ __forceinline__ void umma_i8_pair(uint32_t tmem_d, uint64_t adesc, ui
       "l"(adesc), "l"(bdesc), "r"(kIdescI8Pair), "r"(accumulate)
       : "memory");
 }
+// warp 0: TMA, warp 1: MMA, warps 2-9: epilogue. With g.epi_split = 2 two
+// warps per TMEM lane quarter each drain half of the tile's columns: the
+// per-value reduction is issue-bound, and one warp per scheduler made it the
+// bottleneck when the units are short in k. With long units (the drain hides
+// behind the next unit's MMAs) warps 2-5 drain alone and warps 6-9 idle.
+constexpr int PAIR_THREADS = 320;
 template <int NT>
-__global__ void __launch_bounds__(GEMM_THREADS, 1)
+__global__ void __launch_bounds__(PAIR_THREADS, 1)
     oz_gemm_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  const __grid_constant__ GemmParams g) {
   using P = PairCfg<NT>;
@@ -648,7 +657,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(accf_bar(b), 1);
-      mbar_init(acce_bar(b), 256);
+      mbar_init(acce_bar(b), 2 * 128 * g.epi_split);
     }
     mbar_init(drain_bar, 1);
     *abort = 0;
@@ -763,9 +772,11 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
       while (!mbar_try_wait(drain_bar, 0) && globaltimer() - t0 < 1000000ull) {
       }
     }
-  } else if (warp >= 2) {
+  } else if (warp >= 2 && ((warp - 2) >> 2) < g.epi_split) {
     // ---- epilogue (both CTAs): own TMEM rows -> mod p -> R
-    const int quarter = warp & 3;
+    const int quarter = warp & 3;        // TMEM lanes 32*quarter .. +31
+    const int half = (warp - 2) >> 2;    // columns half*kCols .. +kCols-1
+    const int kCols = 256 * NT / g.epi_split;
     const int row = int(rank) * 128 + quarter * 32 + lane;
     uint32_t acc_phase[2] = {0, 0};
     int accb = 0;
@@ -774,24 +785,41 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
       unit_of(u, t, c, tm, tn);
       if (!mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)) break;
       tc_fence_after();
-      const int p = g.p[t];
+      const int p = g.p[t], c16 = g.c16[t], off = g.off[t];
+      const unsigned M = g.M[t];
       const int i = tm * 256 + row;
-      const int j0 = tn * (256 * NT);
-      int* Rt = g.R + int64_t(t) * g.nb * g.m;
-      for (int c0 = 0; c0 < 256 * NT; c0 += 32) {
+      const int jw = tn * (256 * NT) + half * kCols;
+      const int64_t plane = int64_t(t) * g.nb * g.m;
+      for (int c0 = 0; c0 < kCols; c0 += 32) {
         uint32_t v[32];
-        tmem_ld32(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(accb * 256 + c0), v);
-        if (i < g.m) {
+        tmem_ld32(tmem_base + (uint32_t(quarter * 32) << 16) +
+                      uint32_t(accb * 256 + half * kCols + c0),
+                  v);
+        const int jb = jw + c0;
+        if (i < g.m && jb < g.nb) {
+          const int64_t base = plane + int64_t(jb) * g.m + i;
+          if (jb + 32 <= g.nb) {  // whole group of columns: no per-column test
+            if (g.R8) {
+              unsigned char* d = g.R8 + base;
 #pragma unroll
-          for (int cc = 0; cc < 32; ++cc) {
-            const int j = j0 + c0 + cc;
-            if (j < g.nb) {
-              int r = int(v[cc]) % p;
-              if (r < 0) r += p;
-              if (g.R8)
-                g.R8[int64_t(t) * g.nb * g.m + int64_t(j) * g.m + i] = (unsigned char)r;
-              else
-                atomicAdd(Rt + int64_t(j) * g.m + i, r);
+              for (int cc = 0; cc < 32; ++cc)
+                d[int64_t(cc) * g.m] = (unsigned char)mod_residue(int(v[cc]), p, c16, off, M);
+            } else {
+              int* d = g.R + base;
+#pragma unroll
+              for (int cc = 0; cc < 32; ++cc)
+                atomicAdd(d + int64_t(cc) * g.m, mod_residue(int(v[cc]), p, c16, off, M));
+            }
+          } else {
+#pragma unroll
+            for (int cc = 0; cc < 32; ++cc) {
+              if (jb + cc < g.nb) {
+                const int r = mod_residue(int(v[cc]), p, c16, off, M);
+                if (g.R8)
+                  g.R8[base + int64_t(cc) * g.m] = (unsigned char)r;
+                else
+                  atomicAdd(g.R + base + int64_t(cc) * g.m, r);
+              }
             }
           }
         }
@@ -1351,7 +1379,19 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
         g.wait_limit_ns = 50000000ull;
       }
     }
-    for (int t = 0; t < L.nmod; ++t) g.p[t] = crt.p[t];
+    // short units (few k-blocks): two epilogue warps per lane quarter
+    g.epi_split = g.chunk_blocks < 128 ? 2 : 1;
+    if (const char* v = std::getenv("SPLAB_OZAKI_EPI_SPLIT")) {
+      if (v[0] == '1') g.epi_split = 1;
+      if (v[0] == '2') g.epi_split = 2;
+    }
+    for (int t = 0; t < L.nmod; ++t) {
+      g.p[t] = crt.p[t];
+      const ModMagic mm = make_mod_magic(crt.p[t]);
+      g.c16[t] = mm.c16;
+      g.off[t] = mm.off;
+      g.M[t] = mm.M;
+    }
     const char* gk = std::getenv("SPLAB_OZAKI_GEMM");
     const bool pair = !(gk && gk[0] == '1');  // "1sm" selects the single-CTA kernel
     CUtensorMap mapA2, mapB2;
@@ -1441,7 +1481,7 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
         const int pairs = std::max(1, std::min(gg.total_units, sm_count() / 2));
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(unsigned(2 * pairs));
-        cfg.blockDim = dim3(GEMM_THREADS);
+        cfg.blockDim = dim3(PAIR_THREADS);
         cfg.dynamicSmemBytes = nt == 2 ? PairCfg<2>::SMEM : PairCfg<1>::SMEM;
         cfg.stream = s;
         cudaLaunchAttribute at[1];

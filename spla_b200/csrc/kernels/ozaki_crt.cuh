@@ -92,6 +92,38 @@ __host__ __device__ __forceinline__ unsigned long long mulhi64(unsigned long lon
 }
 
 
+// v mod p in [0, p) for any int32 v and 2 <= p <= 256 without a division:
+// v = hi * 2^16 + lo, t = hi * (2^16 mod p) + lo = v (mod p) with |t| < 2^24,
+// x = t + off (off a multiple of p, >= 2^24) in [0, 2^26), and
+// floor(x / p) = floor(x * M / 2^34) with M = ceil(2^34 / p): the product
+// overestimates x / p by less than x / 2^34 < 2^-8 <= 1 / p, which cannot
+// reach the next integer.
+struct ModMagic {
+  int c16;     // 2^16 mod p
+  int off;     // p * ceil(2^24 / p)
+  unsigned M;  // ceil(2^34 / p) < 2^27
+};
+
+inline ModMagic make_mod_magic(int p) {
+  ModMagic mm;
+  mm.c16 = 65536 % p;
+  mm.off = p * (((1 << 24) + p - 1) / p);
+  mm.M = unsigned(((1ull << 34) + unsigned(p) - 1) / unsigned(p));
+  return mm;
+}
+
+__host__ __device__ __forceinline__ int mod_residue(int v, int p, int c16, int off, unsigned M) {
+  const int hi = v >> 16;  // arithmetic shift
+  const int lo = v & 0xFFFF;
+  const unsigned x = unsigned(hi * c16 + lo + off);
+#ifdef __CUDA_ARCH__
+  const unsigned q = __umulhi(x, M) >> 2;
+#else
+  const unsigned q = unsigned((unsigned long long)x * M >> 34);
+#endif
+  return int(x - q * unsigned(p));
+}
+
 // Correctly rounded conversion of the signed 128-bit value x1:x0 (two's
 // complement) to double: the magnitude's top 64 bits (with a sticky bit for
 // the rest) are converted once and scaled by a power of two.

@@ -2,7 +2,9 @@
 // host/device code the reconstruction kernel runs): random integers X with
 // |X| < P/2 are reduced modulo every modulus, reconstructed, and compared with
 // X converted to double, also with unreduced residues (r + a multiple of p,
-// below 2^24). Also checks the CRT weights: W_t = 1 mod p_t and
+// below 2^24), and the division-free reduction of int32 GEMM sums modulo each
+// modulus (edges of the int32 range, around zero, random). Also checks the
+// CRT weights: W_t = 1 mod p_t and
 // 0 mod p_s (s != t). Prints "OK <cases>" on success.
 #include <cstdio>
 #include <cstdlib>
@@ -69,6 +71,30 @@ int main() {
       }
       ++cases;
     }
+  }
+  // v mod p for int32 GEMM sums
+  for (int t = 0; t < kMaxModuli; ++t) {
+    const int p = kModuli[t];
+    const ModMagic mm = make_mod_magic(p);
+    auto check = [&](long long v) {
+      long long want = v % p;
+      if (want < 0) want += p;
+      const int got = mod_residue(int(v), p, mm.c16, mm.off, mm.M);
+      if (got != want) {
+        printf("FAIL mod p=%d v=%lld got %d want %lld\n", p, v, got, want);
+        return false;
+      }
+      return true;
+    };
+    for (long long v = -2147483648ll; v < -2147483648ll + 200000; ++v)
+      if (!check(v)) return 1;
+    for (long long v = 2147483647ll - 200000; v <= 2147483647ll; ++v)
+      if (!check(v)) return 1;
+    for (long long v = -300000; v <= 300000; ++v)
+      if (!check(v)) return 1;
+    for (int it = 0; it < 2000000; ++it)
+      if (!check((long long)(int)(unsigned)rng())) return 1;
+    cases += 1;
   }
   printf("OK %ld\n", cases);
   return 0;
