@@ -28,6 +28,12 @@ __device__ __forceinline__ void cp_async_4(void* smem, const void* gmem, bool va
   const int n = valid ? 4 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
 }
+// 16-byte asynchronous global->shared copy through L2 only (both addresses
+// 16-byte aligned).
+__device__ __forceinline__ void cp_async_16_cg(void* smem, const void* gmem) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {

@@ -38,6 +38,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -895,15 +896,17 @@ __device__ __forceinline__ void store_c(void* C, int64_t ci, double xr, double x
 // per-chunk residues or, with one k-chunk, the residues as bytes (RT). Threads
 // run along i (contiguous in R and C), blocks along j: no index division.
 // V4 (byte residues, m % 4 == 0): each thread takes four consecutive rows and
-// loads their residues of one modulus as one 32-bit word.
-template <int DT, typename RT, bool V4>
-__global__ void oz_reconstruct(const RT* __restrict__ R, int m, int n, int nb,
+// loads their residues of one modulus as one 32-bit word. NM: the number of
+// moduli when fixed at compile time (the defaults), 0 for rp.n.
+template <int DT, typename RT, bool V4, int NM>
+__global__ void __launch_bounds__(256, 2) oz_reconstruct(const RT* __restrict__ R, int m, int n, int nb,
                                const int* __restrict__ sigA, const int* __restrict__ sigB,
                                void* C, int64_t ldc, double alr, double ali, double ber,
                                double bei, int fill, int64_t ro, int64_t co, int tile_m, int tile_n,
                                ReconParams rp) {
   constexpr bool CPLX = dtype_is_complex(DT);
   constexpr int NV = V4 ? 4 : 1;
+  constexpr bool kBytes = sizeof(RT) == 1;
   const int64_t plane = int64_t(nb) * m;
   const bool read_c = (ber != 0.0 || bei != 0.0);
   for (int j = blockIdx.y; j < n; j += gridDim.y) {
@@ -939,13 +942,13 @@ __global__ void oz_reconstruct(const RT* __restrict__ R, int m, int n, int nb,
 #pragma unroll
           for (int t = 0; t < kMaxUsableModuli; ++t)
             if (t < rp.n) r[t] = int((wr[t] >> (8 * q)) & 255u);
-          const double xr = scale_pow2(crt_value(r, rp), e);
+          const double xr = scale_pow2(crt_value<NM, kBytes>(r, rp), e);
           double xi = 0.0;
           if (CPLX) {
 #pragma unroll
             for (int t = 0; t < kMaxUsableModuli; ++t)
               if (t < rp.n) r[t] = int((wi[t] >> (8 * q)) & 255u);
-            xi = scale_pow2(crt_value(r, rp), e);
+            xi = scale_pow2(crt_value<NM, kBytes>(r, rp), e);
           }
           store_c<DT>(C, i + int64_t(j) * ldc, xr, xi, alr, ali, ber, bei, read_c);
         }
@@ -956,19 +959,126 @@ __global__ void oz_reconstruct(const RT* __restrict__ R, int m, int n, int nb,
         for (int t = 0; t < kMaxUsableModuli; ++t)
           if (t < rp.n) r[t] = int(src[t * plane]);
         const int e = -(sigA[i] + tauj);
-        const double xr = scale_pow2(crt_value(r, rp), e);
+        const double xr = scale_pow2(crt_value<NM, kBytes>(r, rp), e);
         double xi = 0.0;
         if (CPLX) {
           src += int64_t(n) * m;
 #pragma unroll
           for (int t = 0; t < kMaxUsableModuli; ++t)
             if (t < rp.n) r[t] = int(src[t * plane]);
-          xi = scale_pow2(crt_value(r, rp), e);
+          xi = scale_pow2(crt_value<NM, kBytes>(r, rp), e);
         }
         store_c<DT>(C, i + int64_t(j) * ldc, xr, xi, alr, ali, ber, bei, read_c);
       }
     }
   }
+}
+
+// The same reconstruction for byte residues with m % 16 == 0, staged through
+// shared memory: a work item is one column j of C and a block of 1024 rows;
+// its residues (moduli x real/imaginary planes x 1024 bytes) are copied with
+// 16-byte asynchronous copies into one of two stages while the previous item
+// is reconstructed from the other, so that the CRT arithmetic does not wait
+// on the loads. Items are spread over a grid of resident blocks (item =
+// blockIdx.x + k * gridDim.x, row blocks fastest). Each thread takes four
+// consecutive rows: word threadIdx.x of each 1024-byte plane.
+constexpr int kStageRows = 1024;
+template <int DT, int NM>
+__global__ void __launch_bounds__(256, 2)
+    oz_reconstruct_staged(const unsigned char* __restrict__ R, int m, int n, int nb,
+                          const int* __restrict__ sigA, const int* __restrict__ sigB, void* C,
+                          int64_t ldc, double alr, double ali, double ber, double bei, int fill,
+                          int64_t ro, int64_t co, int tile_m, int tile_n, ReconParams rp) {
+  constexpr bool CPLX = dtype_is_complex(DT);
+  constexpr int PARTS = CPLX ? 2 : 1;
+  constexpr int NMAX = NM > 0 ? NM : kMaxUsableModuli;
+  extern __shared__ uint4 stage_smem[];
+  const int nmod = NM > 0 ? NM : rp.n;
+  const int stage_words = PARTS * nmod * (kStageRows / 4);
+  unsigned* stage = reinterpret_cast<unsigned*>(stage_smem);
+  const int64_t plane = int64_t(nb) * m;
+  const int row_blocks = (m + kStageRows - 1) / kStageRows;
+  const int64_t items = int64_t(row_blocks) * n;
+  const bool read_c = (ber != 0.0 || bei != 0.0);
+
+  auto prefetch = [&](int64_t item, int s) {
+    const int rb = int(item % row_blocks), j = int(item / row_blocks);
+    const int i0 = rb * kStageRows;
+    const int chunks = min(kStageRows, m - i0) / 16;  // m % 16 == 0
+    const int total = PARTS * nmod * chunks;
+    unsigned* dst = stage + s * stage_words;
+    for (int c = threadIdx.x; c < total; c += blockDim.x) {
+      const int pl = c / chunks, ch = c - pl * chunks;  // plane: part * nmod + t
+      const int part = pl / nmod, t = pl - part * nmod;
+      const unsigned char* src = R + t * plane + int64_t(j + part * n) * m + i0 + ch * 16;
+      cp_async_16_cg(dst + pl * (kStageRows / 4) + ch * 4, src);
+    }
+  };
+
+  int64_t item = blockIdx.x;
+  if (item < items) prefetch(item, 0);
+  cp_async_commit();
+  int s = 0;
+  for (; item < items; item += gridDim.x) {
+    const int64_t next = item + gridDim.x;
+    if (next < items) prefetch(next, s ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int rb = int(item % row_blocks), j = int(item / row_blocks);
+    const int i = rb * kStageRows + 4 * threadIdx.x;
+    bool active = i < m;
+    if (active && fill != 0) {  // tile_m is a multiple of 4: the four rows share a tile
+      const int64_t ti = (i / tile_m) * int64_t(tile_m), tj = (j / tile_n) * int64_t(tile_n);
+      active = tile_is_active(fill, ti, tj, ::min((int64_t)tile_m, (int64_t)m - ti),
+                              ::min((int64_t)tile_n, (int64_t)n - tj), ro, co);
+    }
+    if (active) {
+      const unsigned* w = stage + s * stage_words + threadIdx.x;
+      const int tauj = sigB[j];
+      const int4 sa = *reinterpret_cast<const int4*>(sigA + i);
+      const int e[4] = {-(sa.x + tauj), -(sa.y + tauj), -(sa.z + tauj), -(sa.w + tauj)};
+      double xr[4], xi[4] = {0.0, 0.0, 0.0, 0.0};
+      {
+        unsigned wr[NMAX];
+#pragma unroll
+        for (int t = 0; t < NMAX; ++t)
+          if (t < nmod) wr[t] = w[t * (kStageRows / 4)];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          int r[NMAX];
+#pragma unroll
+          for (int t = 0; t < NMAX; ++t)
+            if (t < nmod) r[t] = int((wr[t] >> (8 * q)) & 255u);
+          xr[q] = scale_pow2(crt_value<NM, true>(r, rp), e[q]);
+        }
+      }
+      if (CPLX) {
+        unsigned wi[NMAX];
+#pragma unroll
+        for (int t = 0; t < NMAX; ++t)
+          if (t < nmod) wi[t] = w[(nmod + t) * (kStageRows / 4)];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          int r[NMAX];
+#pragma unroll
+          for (int t = 0; t < NMAX; ++t)
+            if (t < nmod) r[t] = int((wi[t] >> (8 * q)) & 255u);
+          xi[q] = scale_pow2(crt_value<NM, true>(r, rp), e[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        store_c<DT>(C, i + q + int64_t(j) * ldc, xr[q], xi[q], alr, ali, ber, bei, read_c);
+    }
+    __syncthreads();  // the stage is refilled by the next iteration's prefetch
+    s ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
+inline int staged_smem_bytes(bool cplx, int nmod) {
+  return 2 * (cplx ? 2 : 1) * nmod * kStageRows;
 }
 
 // At(kk, i) <- A(i, kk): op(A) = N operands (A stored m-major) are copied
@@ -1545,14 +1655,51 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
   phase_mark(2, false, st);
   const ReconParams rp = make_recon(crt);
   // threads along the rows of C (four rows each with byte residues and
-  // m % 4 == 0), blocks along its columns (grid-stride in both, about 64
-  // blocks of 256 threads per SM)
+  // m % 4 == 0), one block row covering all of them (no partial second pass),
+  // blocks along the columns (grid-stride beyond 65535); byte residues with
+  // m % 16 == 0 take the shared-memory staged kernel instead
   const int threads = 256;
+  const bool staged = R8 && L.rowsA % 16 == 0;
   const bool v4 = R8 && L.rowsA % 4 == 0;
   const int64_t rows_per_block = int64_t(threads) * (v4 ? 4 : 1);
   const unsigned gy = unsigned(std::min<int64_t>(p.n, 65535));
-  const unsigned gx = unsigned(std::max<int64_t>(
-      1, std::min<int64_t>((p.m + rows_per_block - 1) / rows_per_block, (148 * 64 + gy - 1) / gy)));
+  const unsigned gx = unsigned(std::max<int64_t>(1, (p.m + rows_per_block - 1) / rows_per_block));
+  const bool fixed = L.nmod == (dtype_is_double(p.dtype) ? kDefaultModuli : kDefaultModuliFloat);
+  if (staged) {
+    const int smem = staged_smem_bytes(cplx, L.nmod);
+    const int64_t items = (p.m + kStageRows - 1) / kStageRows * p.n;
+    const unsigned grid = unsigned(std::min<int64_t>(items, int64_t(2) * sm_count()));
+    auto run = [&](auto kern) -> cudaError_t {
+      const cudaError_t ea = set_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
+      if (ea != cudaSuccess) return ea;
+      kern<<<grid, threads, smem, st>>>(R8, L.rowsA, int(p.n), L.nb, sigA, sigB, p.C, p.ldc,
+                                        p.alpha[0], p.alpha[1], p.beta[0], p.beta[1],
+                                        p.fill_mode, p.fill_ro, p.fill_co, BM,
+                                        cplx ? BN / 2 : BN, rp);
+      return cudaGetLastError();
+    };
+    switch (p.dtype) {
+      case kC64:
+        e = fixed ? run(oz_reconstruct_staged<kC64, kDefaultModuli>)
+                  : run(oz_reconstruct_staged<kC64, 0>);
+        break;
+      case kC32:
+        e = fixed ? run(oz_reconstruct_staged<kC32, kDefaultModuliFloat>)
+                  : run(oz_reconstruct_staged<kC32, 0>);
+        break;
+      case kR64:
+        e = fixed ? run(oz_reconstruct_staged<kR64, kDefaultModuli>)
+                  : run(oz_reconstruct_staged<kR64, 0>);
+        break;
+      default:
+        e = fixed ? run(oz_reconstruct_staged<kR32, kDefaultModuliFloat>)
+                  : run(oz_reconstruct_staged<kR32, 0>);
+        break;
+    }
+    if (e != cudaSuccess) return e;
+    phase_mark(2, true, st);
+    return cudaGetLastError();
+  }
   auto recon = [&](auto kern, const auto* Rsrc) {
     kern<<<dim3(gx, gy), threads, 0, st>>>(Rsrc, L.rowsA, int(p.n), L.nb, sigA, sigB, p.C, p.ldc,
                                            p.alpha[0], p.alpha[1], p.beta[0], p.beta[1],
@@ -1560,28 +1707,36 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
                                            cplx ? BN / 2 : BN, rp);
   };
   using u8 = unsigned char;
-  if (v4) {
+  // the default modulus counts (15 double, 9 float) run a fully unrolled
+  // reconstruction
+  auto by_dtype = [&](auto rt_tag, auto v4_tag, const auto* Rsrc) {
+    using RT = decltype(rt_tag);
+    constexpr bool V = decltype(v4_tag)::value;
     switch (p.dtype) {
-      case kC64: recon(oz_reconstruct<kC64, u8, true>, R8); break;
-      case kC32: recon(oz_reconstruct<kC32, u8, true>, R8); break;
-      case kR64: recon(oz_reconstruct<kR64, u8, true>, R8); break;
-      default: recon(oz_reconstruct<kR32, u8, true>, R8); break;
+      case kC64:
+        fixed ? recon(oz_reconstruct<kC64, RT, V, kDefaultModuli>, Rsrc)
+              : recon(oz_reconstruct<kC64, RT, V, 0>, Rsrc);
+        break;
+      case kC32:
+        fixed ? recon(oz_reconstruct<kC32, RT, V, kDefaultModuliFloat>, Rsrc)
+              : recon(oz_reconstruct<kC32, RT, V, 0>, Rsrc);
+        break;
+      case kR64:
+        fixed ? recon(oz_reconstruct<kR64, RT, V, kDefaultModuli>, Rsrc)
+              : recon(oz_reconstruct<kR64, RT, V, 0>, Rsrc);
+        break;
+      default:
+        fixed ? recon(oz_reconstruct<kR32, RT, V, kDefaultModuliFloat>, Rsrc)
+              : recon(oz_reconstruct<kR32, RT, V, 0>, Rsrc);
+        break;
     }
-  } else if (R8) {
-    switch (p.dtype) {
-      case kC64: recon(oz_reconstruct<kC64, u8, false>, R8); break;
-      case kC32: recon(oz_reconstruct<kC32, u8, false>, R8); break;
-      case kR64: recon(oz_reconstruct<kR64, u8, false>, R8); break;
-      default: recon(oz_reconstruct<kR32, u8, false>, R8); break;
-    }
-  } else {
-    switch (p.dtype) {
-      case kC64: recon(oz_reconstruct<kC64, int, false>, R); break;
-      case kC32: recon(oz_reconstruct<kC32, int, false>, R); break;
-      case kR64: recon(oz_reconstruct<kR64, int, false>, R); break;
-      default: recon(oz_reconstruct<kR32, int, false>, R); break;
-    }
-  }
+  };
+  if (v4)
+    by_dtype(u8{}, std::true_type{}, R8);
+  else if (R8)
+    by_dtype(u8{}, std::false_type{}, R8);
+  else
+    by_dtype(int{}, std::false_type{}, R);
   phase_mark(2, true, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return cudaSuccess;

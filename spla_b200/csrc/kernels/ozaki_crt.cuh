@@ -1,6 +1,7 @@
 // Chinese-remainder constants and reconstruction of the Ozaki scheme II path
-// (host and device code). The reconstruction is exact integer arithmetic on
-// 64-bit limbs; see ozaki.cu for the method.
+// (host and device code): exact integer arithmetic on 32-bit limbs up to the
+// final conversion to double, and the division-free reduction of the INT8
+// GEMM's int32 sums modulo each modulus.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -59,39 +60,6 @@ inline Crt make_crt(int n) {
   return c;
 }
 
-struct ReconParams {
-  int n;
-  int p[kMaxModuli];
-  unsigned long long w_lo[kMaxModuli], w_hi[kMaxModuli];
-  unsigned long long P_lo, P_hi;
-  double P_d, inv_P;
-};
-
-inline ReconParams make_recon(const Crt& c) {
-  ReconParams rp{};
-  rp.n = c.n;
-  for (int t = 0; t < c.n; ++t) {
-    rp.p[t] = c.p[t];
-    rp.w_lo[t] = c.w_lo[t];
-    rp.w_hi[t] = c.w_hi[t];
-  }
-  rp.P_lo = c.P_lo;
-  rp.P_hi = c.P_hi;
-  rp.P_d = c.P_d;
-  rp.inv_P = 1.0 / c.P_d;
-  return rp;
-}
-
-__host__ __device__ __forceinline__ unsigned long long mulhi64(unsigned long long a,
-                                                               unsigned long long b) {
-#ifdef __CUDA_ARCH__
-  return __umul64hi(a, b);
-#else
-  return (unsigned long long)(((unsigned __int128)a * b) >> 64);
-#endif
-}
-
-
 // v mod p in [0, p) for any int32 v and 2 <= p <= 256 without a division:
 // v = hi * 2^16 + lo, t = hi * (2^16 mod p) + lo = v (mod p) with |t| < 2^24,
 // x = t + off (off a multiple of p, >= 2^24) in [0, 2^26), and
@@ -124,117 +92,112 @@ __host__ __device__ __forceinline__ int mod_residue(int v, int p, int c16, int o
   return int(x - q * unsigned(p));
 }
 
-// Correctly rounded conversion of the signed 128-bit value x1:x0 (two's
-// complement) to double: the magnitude's top 64 bits (with a sticky bit for
-// the rest) are converted once and scaled by a power of two.
-__host__ __device__ __forceinline__ double i128_to_double(unsigned long long x1,
-                                                           unsigned long long x0) {
-  const bool neg = (long long)x1 < 0;
-  if (neg) {  // negate: ~x + 1
-    x0 = ~x0 + 1ull;
-    x1 = ~x1 + (x0 == 0 ? 1ull : 0ull);
+struct ReconParams {
+  int n;
+  int p[kMaxModuli];
+  unsigned w[kMaxModuli][4];  // CRT weights W_t < P as 32-bit limbs, least significant first
+  unsigned P[4];              // P as 32-bit limbs
+  double inv_P32;             // 2^32 / P
+};
+
+inline ReconParams make_recon(const Crt& c) {
+  ReconParams rp{};
+  rp.n = c.n;
+  for (int t = 0; t < c.n; ++t) {
+    rp.p[t] = c.p[t];
+    const unsigned long long lo = c.w_lo[t], hi = c.w_hi[t];
+    rp.w[t][0] = unsigned(lo);
+    rp.w[t][1] = unsigned(lo >> 32);
+    rp.w[t][2] = unsigned(hi);
+    rp.w[t][3] = unsigned(hi >> 32);
   }
-  double mag;
-  if (x1 == 0) {
-    mag = double(x0);
-  } else {
-#ifdef __CUDA_ARCH__
-    const int lz = __clzll((long long)x1);
-#else
-    const int lz = __builtin_clzll(x1);
-#endif
-    const unsigned long long top = lz ? ((x1 << lz) | (x0 >> (64 - lz))) : x1;
-    const unsigned long long rest = lz ? (x0 << lz) : x0;
-    const double t = double(top | (rest != 0 ? 1ull : 0ull));
-#ifdef __CUDA_ARCH__
-    mag = t * __longlong_as_double((long long)(1023 + 64 - lz) << 52);  // exact: 2^(64-lz)
-#else
-    mag = std::ldexp(t, 64 - lz);
-#endif
-  }
-  return neg ? -mag : mag;
+  rp.P[0] = unsigned(c.P_lo);
+  rp.P[1] = unsigned(c.P_lo >> 32);
+  rp.P[2] = unsigned(c.P_hi);
+  rp.P[3] = unsigned(c.P_hi >> 32);
+  rp.inv_P32 = 4294967296.0 / c.P_d;
+  return rp;
 }
 
-// X = (sum_t W_t r_t) mod P as a signed value in (-P/2, P/2], converted to double.
-// The r_t need not be reduced: any 0 <= r_t < 2^24 congruent to the residue
-// works (the INT8 GEMM hands over sums of per-chunk residues).
+// Exact conversions to double of integers below 2^32 and 2^52: the integer
+// is placed in the mantissa of 2^52 and 2^52 subtracted (one FP64 add instead
+// of an integer-to-float conversion).
+__host__ __device__ __forceinline__ double u32_to_double(unsigned x) {
+#ifdef __CUDA_ARCH__
+  return __hiloint2double(0x43300000, int(x)) - 4503599627370496.0;
+#else
+  return double(x);
+#endif
+}
+__host__ __device__ __forceinline__ double u52_to_double(unsigned long long x) {
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double((long long)(x | 0x4330000000000000ull)) - 4503599627370496.0;
+#else
+  return double(x);
+#endif
+}
+
+// X = (sum_t W_t r_t) mod P as the representative of smallest magnitude,
+// converted to double (within 1.5 units in the last place), for values with
+// |X| <= P/4: the row scaling of the Ozaki path bounds every element of the
+// scaled product by (2^Q + sqrt(K)/2)^2 with 2^(2Q) <= P/4.
+//
+// S = sum_t W_t r_t is accumulated per 32-bit limb of W_t (one 32x32->64
+// multiply-add per limb and modulus, no carries: r_t < 2^24 and at most 16
+// terms keep each limb sum below 2^60). S / P lies within 1/4 + 2^-37 of the
+// integer q = round(S / P), and the estimate S * (2^32 / P) from the top
+// three limb sums in double is off by less than 2^-20, so rounding it gives q
+// exactly. X = S - qP is formed limb by limb in signed 64-bit arithmetic,
+// carried into 32-bit limbs x0..x2 and a small signed top c, and converted by
+// Horner's rule in FP64 (exact while the partial value is below 2^53; after
+// that each of at most three steps rounds once, relative to a partial value
+// no larger than about |X|).
+//
+// N: number of moduli (0: rp.n at run time). BYTES: residues below 2^8 (the
+// limb sums are then below 2^44 and convert exactly by the mantissa method).
+template <int N, bool BYTES>
 __host__ __device__ __forceinline__ double crt_value(const int* r, const ReconParams& rp) {
-  // S = sum_t W_t r_t accumulated per 32-bit limb of W_t: each product is
-  // below 2^56 and at most 16 of them below 2^60, so the four 64-bit limb sums
-  // need no carries (one 32x32->64 multiply-add per limb and modulus)
-  // (unrolled to the usable maximum so that r stays in registers)
   unsigned long long l0 = 0, l1 = 0, l2 = 0, l3 = 0;
 #pragma unroll
-  for (int t = 0; t < kMaxUsableModuli; ++t) {
-    if (t >= rp.n) break;
-    const unsigned long long rt = (unsigned int)r[t];
-    l0 += rt * (unsigned int)rp.w_lo[t];
-    l1 += rt * (unsigned int)(rp.w_lo[t] >> 32);
-    l2 += rt * (unsigned int)rp.w_hi[t];
-    l3 += rt * (unsigned int)(rp.w_hi[t] >> 32);
+  for (int t = 0; t < (N > 0 ? N : kMaxUsableModuli); ++t) {
+    if (N == 0 && t >= rp.n) break;
+    const unsigned rt = unsigned(r[t]);
+    l0 += (unsigned long long)rt * rp.w[t][0];
+    l1 += (unsigned long long)rt * rp.w[t][1];
+    l2 += (unsigned long long)rt * rp.w[t][2];
+    l3 += (unsigned long long)rt * rp.w[t][3];
   }
-  // carry-propagate into the 192-bit S = s2:s1:s0
-  unsigned long long c = l0;
-  const unsigned long long d0 = c & 0xFFFFFFFFull;
-  c = (c >> 32) + l1;
-  const unsigned long long d1 = c & 0xFFFFFFFFull;
-  c = (c >> 32) + l2;
-  const unsigned long long d2 = c & 0xFFFFFFFFull;
-  c = (c >> 32) + l3;
-  const unsigned long long d3 = c & 0xFFFFFFFFull;
-  const unsigned long long s0 = d0 | (d1 << 32), s1 = d2 | (d3 << 32), s2 = c >> 32;
-  // q = floor(S / P) estimated in double, then S - qP. S / P < 16 * 2^24 and
-  // the estimate S_d * (1 / P_d) carries at most ~6 roundings of 2^-53
-  // relative, an absolute error below 2^-22: q is off by at most one, and one
-  // conditional add or subtract of P brings S - qP into [0, P).
-  const double S_d = double(s2) * 3.402823669209385e38 + double(s1) * 18446744073709551616.0 +
-                     double(s0);
-  unsigned long long q = (unsigned long long)floor(S_d * rp.inv_P);
-  // qP (192-bit)
-  const unsigned long long qp0 = rp.P_lo * q, qp0h = mulhi64(rp.P_lo, q);
-  const unsigned long long qp1l = rp.P_hi * q, qp1h = mulhi64(rp.P_hi, q);
-  unsigned long long t1 = qp0h + qp1l;
-  unsigned long long t2 = qp1h + (t1 < qp0h);
-  // X = S - qP (192-bit two's complement)
-  unsigned long long x0 = s0 - qp0;
-  unsigned long long br = s0 < qp0;
-  unsigned long long x1 = s1 - t1 - br;
-  unsigned long long br1 = (s1 < t1) || (s1 - t1 < br);
-  unsigned long long x2 = s2 - t2 - br1;
-  // fix-up into [0, P)
-  {
-    if ((long long)x2 < 0) {  // X < 0: X += P
-      unsigned long long n0 = x0 + rp.P_lo;
-      unsigned long long cy = n0 < x0;
-      unsigned long long n1 = x1 + rp.P_hi + cy;
-      unsigned long long cy1 = (n1 < x1) || (cy && n1 == x1);
-      x0 = n0;
-      x1 = n1;
-      x2 += cy1;
-    } else if (x2 > 0 || x1 > rp.P_hi || (x1 == rp.P_hi && x0 >= rp.P_lo)) {  // X >= P
-      unsigned long long n0 = x0 - rp.P_lo;
-      unsigned long long b0 = x0 < rp.P_lo;
-      unsigned long long n1 = x1 - rp.P_hi - b0;
-      unsigned long long b1 = (x1 < rp.P_hi) || (x1 - rp.P_hi < b0);
-      x0 = n0;
-      x1 = n1;
-      x2 -= b1;
-    }
+  // q = round(S / P) from (l1 + l2 2^32 + l3 2^64) * 2^32 / P
+  double s1, s2, s3;
+  if (BYTES) {
+    s1 = u52_to_double(l1);
+    s2 = u52_to_double(l2);
+    s3 = u52_to_double(l3);
+  } else {
+    s1 = double(l1);
+    s2 = double(l2);
+    s3 = double(l3);
   }
-  // now 0 <= X < P (x2 == 0). Symmetric: X > P/2 -> X - P.
-  const unsigned long long hP_hi = rp.P_hi >> 1,
-                           hP_lo = (rp.P_lo >> 1) | (rp.P_hi << 63);
-  const bool upper = x1 > hP_hi || (x1 == hP_hi && x0 > hP_lo);
-  if (upper) {
-    const unsigned long long n0 = x0 - rp.P_lo;
-    const unsigned long long b0 = x0 < rp.P_lo;
-    const unsigned long long n1 = x1 - rp.P_hi - b0;
-    x0 = n0;
-    x1 = n1;  // now the top limb is negative (two's complement 128-bit)
-  }
-  return i128_to_double(x1, x0);
+  const double sh = fma(s3, 18446744073709551616.0, fma(s2, 4294967296.0, s1));
+  const double qr = fma(sh, rp.inv_P32, 6755399441055744.0);  // 1.5 * 2^52: rounds to integer
+#ifdef __CUDA_ARCH__
+  const unsigned q = unsigned(__double2loint(qr));
+#else
+  const unsigned q = unsigned((unsigned long long)(qr - 6755399441055744.0));
+#endif
+  // X = S - qP, limb by limb (each difference lies in (-2^60, 2^60)), carried
+  const unsigned long long qq = q;
+  long long c = (long long)(l0 - qq * rp.P[0]);
+  const unsigned x0 = unsigned(c);
+  c = (c >> 32) + (long long)(l1 - qq * rp.P[1]);
+  const unsigned x1 = unsigned(c);
+  c = (c >> 32) + (long long)(l2 - qq * rp.P[2]);
+  const unsigned x2 = unsigned(c);
+  c = (c >> 32) + (long long)(l3 - qq * rp.P[3]);  // |c| < 2^22
+  double v = fma(double(int(c)), 4294967296.0, u32_to_double(x2));
+  v = fma(v, 4294967296.0, u32_to_double(x1));
+  return fma(v, 4294967296.0, u32_to_double(x0));
 }
-
 
 }  // namespace oz
 }  // namespace splab

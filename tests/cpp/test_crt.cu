@@ -1,11 +1,13 @@
 // CPU check of the Ozaki path's Chinese-remainder reconstruction (the same
 // host/device code the reconstruction kernel runs): random integers X with
-// |X| < P/2 are reduced modulo every modulus, reconstructed, and compared with
-// X converted to double, also with unreduced residues (r + a multiple of p,
-// below 2^24), and the division-free reduction of int32 GEMM sums modulo each
-// modulus (edges of the int32 range, around zero, random). Also checks the
-// CRT weights: W_t = 1 mod p_t and
-// 0 mod p_s (s != t). Prints "OK <cases>" on success.
+// |X| <= P/4 (the range the row scaling guarantees) are reduced modulo every
+// modulus, reconstructed, and compared with X converted to double (within
+// 1.5 units in the last place), with byte residues and with unreduced
+// residues (r + a multiple of p, below 2^24), for a run-time and a fixed
+// modulus count. Also checks the division-free reduction of int32 GEMM sums
+// modulo each modulus (edges of the int32 range, around zero, random) and the
+// CRT weights: W_t = 1 mod p_t and 0 mod p_s (s != t). Prints "OK <cases>" on
+// success.
 #include <cstdio>
 #include <cstdlib>
 #include <random>
@@ -37,36 +39,45 @@ int main() {
       }
     }
     const ReconParams rp = make_recon(c);
-    const i128 half = i128(P / 2);
+    const i128 quarter = i128(P / 4);
     for (int it = 0; it < 20000; ++it) {
       i128 X;
-      const int kind = it % 5;
-      if (kind == 0) X = half - 1 - i128(rng() % 1000);
-      else if (kind == 1) X = -half + 1 + i128(rng() % 1000);
+      const int kind = it % 6;
+      if (kind == 0) X = quarter - i128(rng() % 1000);
+      else if (kind == 1) X = -quarter + i128(rng() % 1000);
       else if (kind == 2) X = i128(int64_t(rng() % 2000001) - 1000000);
+      else if (kind == 3) X = (i128(int64_t(rng())) * i128(rng() % 4096)) % (quarter + 1);
       else {
         u128 v = (u128(rng()) << 64) | rng();
-        v %= P;
-        X = i128(v) - half;
+        v %= u128(2 * quarter + 1);
+        X = i128(v) - quarter;
       }
       int r[kMaxModuli];
       for (int t = 0; t < n; ++t) r[t] = mod_pos(X, c.p[t]);
-      const double got = crt_value(r, rp);
       const long long hi = (long long)(X >> 64);
       const unsigned long long lo = (unsigned long long)X;
       const double want = (double)((long double)hi * 18446744073709551616.0L + (long double)lo);
-      const double diff = got > want ? got - want : want - got;
-      const double tol = (want < 0 ? -want : want) * 2.3e-16 + 1e-300;
-      if (diff > tol) {
+      const double tol = (want < 0 ? -want : want) * 3.4e-16;  // 1.5 ulp
+      auto bad = [&](double got) { return (got > want ? got - want : want - got) > tol; };
+      const double got = crt_value<0, true>(r, rp);
+      if (bad(got) || bad(crt_value<0, false>(r, rp))) {
         printf("FAIL n=%d it=%d got %.17g want %.17g\n", n, it, got, want);
+        return 1;
+      }
+      if (n == 15 && bad(crt_value<15, true>(r, rp))) {
+        printf("FAIL fixed n=15 it=%d\n", it);
+        return 1;
+      }
+      if (n == 9 && bad(crt_value<9, true>(r, rp))) {
+        printf("FAIL fixed n=9 it=%d\n", it);
         return 1;
       }
       // unreduced residues (sums of per-chunk residues, below 2^24)
       for (int t = 0; t < n; ++t)
         r[t] += c.p[t] * int(rng() % ((1u << 24) / unsigned(c.p[t]) - 1));
-      const double got2 = crt_value(r, rp);
-      if (got2 != got) {
-        printf("FAIL unreduced n=%d it=%d got %.17g want %.17g\n", n, it, got2, got);
+      const double got2 = crt_value<0, false>(r, rp);
+      if (bad(got2)) {
+        printf("FAIL unreduced n=%d it=%d got %.17g want %.17g\n", n, it, got2, want);
         return 1;
       }
       ++cases;

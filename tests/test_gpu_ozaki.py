@@ -5,8 +5,9 @@ dimensions, several k-chunks (k*2 > 124928), alpha/beta with C offsets and
 ldc padding, k = 0, the modulus-count knob, the fill-mode tile skipping,
 op(A) = N (pgemm_sbs and gemm: A copied k-major first) with one k-chunk (byte
 residues) and several (int32 sums), more row tiles than one band of the unit
-raster, and the failure path of the bounded device waits (no GPU fault: the
-producer issues no copies, every wait runs into a 50 ms bound)."""
+raster, the reconstruction staged through shared memory, and the failure
+path of the bounded device waits (no GPU fault: the producer issues no
+copies, every wait runs into a 50 ms bound)."""
 import os
 import subprocess
 import sys
@@ -115,8 +116,9 @@ def test_modulus_count_out_of_range_rejected():
         ctx.set_fp64_path(spla.PATH_OZAKI, 5)
 
 
-def test_fill_lower_triangle():
-    m = n = 300
+@pytest.mark.parametrize("m", [300, 512])
+def test_fill_lower_triangle(m):
+    n = m
     k = 6000
     C0, got, ref, ldc = run_ssb(np.complex128, m, n, k, 2, fill=spla.FILL_MODE_LOWER)
     g, r = got.reshape(n, ldc).T[:m], ref.reshape(n, ldc).T[:m]
@@ -190,6 +192,19 @@ def test_tall_banded_raster(dt):
     ref = np.zeros(m * n, dtype=dt)
     assert oracle.gemm(0, 0, m, n, k, 1.0, A, m, B, k, 0.0, ref, m) == 0
     assert oracle.rel_fro(dC.cpu().numpy(), ref) <= 1e-14
+
+
+@pytest.mark.parametrize("dt,tol,m,moduli", [
+    (np.complex128, 1e-14, 3088, 0), (np.float64, 1e-14, 1040, 0),
+    (np.complex64, 1e-6, 2064, 0), (np.float32, 1e-6, 1056, 0), (np.complex128, 1e-9, 2064, 12)])
+def test_staged_reconstruction(dt, tol, m, moduli):
+    """Byte residues with m % 16 == 0 take the reconstruction staged through
+    shared memory: several blocks of 1024 rows with a partial last one, alpha
+    and beta both active, the default and a non-default modulus count."""
+    cplx = np.dtype(dt).kind == "c"
+    alpha, beta = ((0.5 + 0.25j), (-1.0 + 0.5j)) if cplx else (0.5, -1.0)
+    C0, got, ref, ldc = run_ssb(dt, m, 70, 500, 2 if cplx else 1, alpha, beta, moduli=moduli)
+    assert oracle.rel_fro(got, ref) <= tol
 
 
 def test_bounded_wait_failure_path():
