@@ -39,7 +39,8 @@ extern "C" {
 #define SPLAB_PATH_AUTO 0  /* the supported path with the least modelled time */
 #define SPLAB_PATH_DMMA 1  /* FP64 tensor cores (mma.sync f64); float inputs accumulate in FP64 */
 #define SPLAB_PATH_OZAKI 2 /* Ozaki scheme II on INT8 tcgen05 (all four dtypes) with
-                              op(A) in {T, C}, op(B) = N; other problems use DMMA */
+                              op(B) = N and any op(A) (op(A) = N: A is first copied
+                              k-major into the workspace); other problems use DMMA */
 #define SPLAB_PATH_TF32X3 3 /* float / complex float: each input split into two TF32
                                parts, three TF32 tcgen05 products, FP32 accumulation
                                drained to FP64 every 1024 reals; op(A) in {T, C},
