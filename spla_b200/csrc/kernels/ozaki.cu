@@ -231,7 +231,9 @@ __device__ __forceinline__ uint32_t pack4(float a, float b, float c, float d) {
 // mode 1: complex B rows -> u row `row` and v row `row + rows` with sign s:
 //         u = (br, -s*bi), v = (bi, s*br) interleaved.
 // TIn: double (|x| < 2^62, five digits) or float (|x| < 2^38, three digits).
-template <typename TIn, bool VEC, int NDIG, int EL>
+// NMU > 0: moduli 0 .. NMU-1 in one fully unrolled pass (the per-modulus
+// constants become fixed parameter operands); 0: t_begin .. t_end-1 in a loop.
+template <typename TIn, bool VEC, int NDIG, int EL, int NMU>
 __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
     oz_slice(const TIn* __restrict__ X, int64_t ld_doubles, int64_t len, int rows, int64_t kp,
              const int* __restrict__ sigma, int mode, int s_sign, int8_t* __restrict__ res,
@@ -284,8 +286,9 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
   }
   const unsigned long long M2 = f2_pack(kMagic, kMagic), NM2 = f2_pack(-kMagic, -kMagic);
   const unsigned long long NEG1 = f2_pack(-1.0f, -1.0f), TWO_M2 = f2_pack(2 * kMagic, 2 * kMagic);
-  int8_t* out = res + t_begin * res_mod_stride + int64_t(row) * kp + l0;
-  for (int t = t_begin; t < t_end; ++t, out += res_mod_stride) {
+  int8_t* const out0 = res + int64_t(row) * kp + l0;
+  auto modulus = [&](const int t) {
+    int8_t* out = out0 + t * res_mod_stride;
     unsigned long long rp2[EL / 2];  // MAGIC + residue of elements 2i, 2i + 1
     if (t == 0 && sc.p0 == 256.0f) {
 #pragma unroll
@@ -345,6 +348,12 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
         *reinterpret_cast<uint2*>(out_v) = make_uint2(wv[0], wv[1]);
       }
     }
+  };
+  if constexpr (NMU > 0) {
+#pragma unroll
+    for (int t = 0; t < NMU; ++t) modulus(t);
+  } else {
+    for (int t = t_begin; t < t_end; ++t) modulus(t);
   }
 }
 
@@ -1210,20 +1219,37 @@ int slice_elems() {
   return el;
 }
 
+// The default modulus count of the input type (15 for double, 9 for float)
+// over all moduli runs unrolled (SPLAB_OZAKI_SLICE_UNROLL=0 keeps the loop).
+bool slice_unroll() {
+  static const bool on = [] {
+    const char* v = std::getenv("SPLAB_OZAKI_SLICE_UNROLL");
+    return !(v && v[0] == '0');
+  }();
+  return on;
+}
+
 template <typename TIn, bool VEC, int EL>
 void launch_slice_el(int ndig, unsigned grid, cudaStream_t st, const TIn* X, int64_t ld,
                      int64_t len, int rows, int64_t kp, const int* sig, int mode, int s_sign,
                      int8_t* res, int64_t stride, const oz::SliceConsts& sc, int t0, int t1) {
   using namespace oz;
+  constexpr int kNU = sizeof(TIn) == 8 ? kDefaultModuli : kDefaultModuliFloat;
+  constexpr int kDigU = sizeof(TIn) == 8 ? 4 : 3;  // digits of the default scaling
+  if (t0 == 0 && t1 == kNU && sc.n == kNU && ndig == kDigU && slice_unroll()) {
+    oz_slice<TIn, VEC, kDigU, EL, kNU><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode,
+                                                              s_sign, res, stride, sc, t0, t1);
+    return;
+  }
   if (ndig <= 3)
-    oz_slice<TIn, VEC, 3, EL><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
-                                                     stride, sc, t0, t1);
+    oz_slice<TIn, VEC, 3, EL, 0><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign,
+                                                        res, stride, sc, t0, t1);
   else if (ndig == 4)
-    oz_slice<TIn, VEC, 4, EL><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
-                                                     stride, sc, t0, t1);
+    oz_slice<TIn, VEC, 4, EL, 0><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign,
+                                                        res, stride, sc, t0, t1);
   else
-    oz_slice<TIn, VEC, 5, EL><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign, res,
-                                                     stride, sc, t0, t1);
+    oz_slice<TIn, VEC, 5, EL, 0><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign,
+                                                        res, stride, sc, t0, t1);
 }
 
 template <typename TIn, bool VEC>
