@@ -198,7 +198,11 @@ SPLAB_API int splab_block_cyclic_info(int64_t rowsInBlock, int64_t colsInBlock, 
  * records events[2p] / events[2p+1] (cudaEvent_t handles created by the
  * caller) on its stream around phase p, for p < count:
  *   DMMA path : 0 = contraction kernel, 1 = split-K reduction
- *   Ozaki path: 0 = slicing, 1 = INT8 residue GEMMs, 2 = reconstruction
+ *   Ozaki path: 0 = slicing, 1 = INT8 residue GEMMs, 2 = reconstruction,
+ *               3 + g = GEMM launch of modulus group g; inside phase 0:
+ *               15 = k-major copy of A (op(A) = N), 16 = row norms (of A, and
+ *               of B unless they run on a side stream), 17 = residues of A,
+ *               18 = residues of B (one modulus group)
  * Pass events = NULL to stop. Returns SPLAB_OK.
  */
 SPLAB_API int splab_set_phase_events(void **events, int count);

@@ -1445,8 +1445,13 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
   // modulus-group pipeline below.
   const bool big = double(L.rowsA + L.rowsB) * double(L.K2) * dtype_bytes(p.dtype) /
                        (cplx ? 2.0 : 1.0) >= 5e8;
-  PipeStreams* ps =
-      (p.k > 0 && (groups > 1 || big) && t_side_streams) ? pipe_streams() : nullptr;
+  static const bool side_norms = [] {
+    const char* v = std::getenv("SPLAB_OZAKI_SIDE_NORMS");
+    return !(v && v[0] == '0');
+  }();
+  PipeStreams* ps = (p.k > 0 && (groups > 1 || (big && side_norms)) && t_side_streams)
+                        ? pipe_streams()
+                        : nullptr;
   std::unique_lock<std::mutex> lk;
   if (ps) lk = std::unique_lock<std::mutex>(ps->mu);
   auto scale = [&](int which, cudaStream_t s) {
@@ -1456,17 +1461,25 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
       scale_operands<float>(L, crt, p, cplx, sigA, sigB, which, s);
   };
   phase_mark(0, false, st);
-  if (L.at && p.k > 0 && (e = transpose_a(p_in, L, w + L.off_At, st)) != cudaSuccess) return e;
+  if (L.at && p.k > 0) {
+    phase_mark(15, false, st);
+    if ((e = transpose_a(p_in, L, w + L.off_At, st)) != cudaSuccess) return e;
+    phase_mark(15, true, st);
+  }
   if (p.k > 0 && ps) {
     // A's norms alone (both are pure reads and would share the bandwidth),
     // then B's norms on the side stream while A is sliced
+    phase_mark(16, false, st);
     scale(1, st);
+    phase_mark(16, true, st);
     if ((e = cudaEventRecord(ps->ev_start, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(ps->lo, ps->ev_start, 0)) != cudaSuccess) return e;
     scale(2, ps->lo);
     if ((e = cudaEventRecord(ps->ev_scaled, ps->lo)) != cudaSuccess) return e;
   } else if (p.k > 0) {
+    phase_mark(16, false, st);
     scale(3, st);
+    phase_mark(16, true, st);
   } else {
     cudaMemsetAsync(sigA, 0, sizeof(int) * L.rowsA, st);
     cudaMemsetAsync(sigB, 0, sizeof(int) * L.rowsB, st);
@@ -1638,13 +1651,14 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
     };
 
     if (groups == 1 || !ps) {
-      if (ps) {  // A on the caller's stream, B once its row norms are done
-        slice(0, L.nmod, 1, st);
-        if ((e = cudaStreamWaitEvent(st, ps->ev_scaled, 0)) != cudaSuccess) return e;
-        slice(0, L.nmod, 2, st);
-      } else {
-        slice(0, L.nmod, 3, st);
-      }
+      phase_mark(17, false, st);
+      slice(0, L.nmod, 1, st);  // A on the caller's stream
+      phase_mark(17, true, st);
+      // B once its row norms are done (on the side stream when there is one)
+      if (ps && (e = cudaStreamWaitEvent(st, ps->ev_scaled, 0)) != cudaSuccess) return e;
+      phase_mark(18, false, st);
+      slice(0, L.nmod, 2, st);
+      phase_mark(18, true, st);
       phase_mark(0, true, st);
       phase_mark(1, false, st);
       phase_mark(3, false, st);

@@ -10,7 +10,8 @@ C = op(A) B with op = conjugate transpose (complex) or transpose (real)
 unless opA is given (0 = N: A is m x k, the pgemm_sbs shape), Gaussian
 operands scaled by 1/sqrt(k). One JSON line per spec: total time,
 TFLOP/s and the phase times the path reports (scale/slice, GEMM span,
-reduction or reconstruction, then one entry per GEMM launch).
+reduction or reconstruction, then one entry per GEMM launch) and, for the
+Ozaki path, the parts of the slicing phase.
 """
 from __future__ import annotations
 
@@ -79,7 +80,9 @@ def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: i
             "resolved_path": L.splab_gemm_path(spla._dtype_of(dtype=dtype), path, op, 0, m, n, k),
             "opA": op, "m": m, "n": n, "k": k, "ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 1),
             "phases_ms": [round(x, 3) for x in ph[:3]],
-            "gemm_launch_ms": [round(x, 3) for x in ph[3:] if x > 0.05],
+            "gemm_launch_ms": [round(x, 3) for x in ph[3:15] if x > 0.05],
+            "slicing_ms": {"a_copy": round(ph[15], 3), "norms": round(ph[16], 3),
+                           "residues_a": round(ph[17], 3), "residues_b": round(ph[18], 3)},
             "workspace_GB": round(ws_bytes / 1e9, 2)}
 
 
