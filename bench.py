@@ -98,8 +98,13 @@ def cpu_model():
 # clocks
 
 
+TIMED_WINDOWS = []  # (path, host wall-clock start, end) of every timed region
+
+
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi every 20 ms; the summary keeps the samples taken inside the
+    timed regions (TIMED_WINDOWS), so idle time around them does not count."""
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -112,7 +117,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -126,7 +131,7 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, path=None):
         rows = []
         try:
             for ln in self.path.read_text().splitlines():
@@ -137,14 +142,26 @@ class ClockSampler:
             return None
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        import datetime
+
+        def inside(r):
+            try:
+                t = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                return False
+            return any(a <= t <= b for p, a, b in TIMED_WINDOWS if path is None or p == path)
+
+        timed = [r for r in rows if inside(r)]
+        use = timed or rows
+        sm = [float(r[1]) for r in use if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        loaded = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)] or sm
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
-        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+        reasons = sorted({names[i] for r in use for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(use), "samples_in_timed_regions": len(timed),
+                "sampling": "nvidia-smi every 20 ms; median over the samples inside the timed "
+                            "regions (all samples when none fell inside)"}
 
 
 # ---------------------------------------------------------------------------
@@ -242,6 +259,7 @@ def time_device_path(torch, spla, path, A, B, steps, warmup, rank):
         if torch.distributed.is_initialized():
             torch.distributed.barrier()
         torch.cuda.synchronize()
+        wall0 = time.time()
         t0.record(stream)
         for _ in range(steps):
             for e in pev:
@@ -259,6 +277,7 @@ def time_device_path(torch, spla, path, A, B, steps, warmup, rank):
                     pass
         t1.record(stream)
         torch.cuda.synchronize()
+        TIMED_WINDOWS.append((path, wall0, time.time()))
     ms = t0.elapsed_time(t1) / steps
     return dC, ms, [x / steps for x in phase_ms]
 
@@ -678,11 +697,17 @@ def main():
                 results[pname] = {"error": str(ex)}
                 continue
             ms = max_over_ranks(torch, ms, device)
-            # phases 3.. are per-launch INT8 GEMM times (Ozaki); unused ones read ~0
-            phases = phases[:3] + [x for x in phases[3:] if x > 0.05]
+            # phases 3..14 are per-launch INT8 GEMM times (Ozaki; unused ones read
+            # ~0), 15..18 the parts of the slicing phase
+            parts = dict(zip(["a_copy", "norms", "residues_a", "residues_b"], phases[15:19]))
+            phases = phases[:3] + [x for x in phases[3:15] if x > 0.05]
             results[pname] = {"ms_per_step": ms, "tflops": whole_job_tflops(FLOPS, world, ms),
                               "phase_ms": phases, "dC": dC}
-    clocks = clk.summary()
+            if pname == "ozaki":
+                results[pname]["slicing_parts_ms"] = parts
+    clocks_by_path = {p: clk.summary(names[p]) for p in results}
+    for p in results:
+        results[p]["clocks"] = clocks_by_path[p]
     for pname, r in results.items():
         if "dC" in r:
             r["rel_err_vs_oracle"] = rel_err_sampled(r.pop("dC"), A, B) if rank == 0 else None
@@ -699,6 +724,7 @@ def main():
         head = "ozaki" if int(flag.item()) else "dmma"
     hr = results[head]
     head_path = names[head]
+    clocks = clocks_by_path.get(head)
 
     e2e = None
     if not args.no_e2e:
@@ -726,18 +752,19 @@ def main():
         gemm_launch_ms = hr["phase_ms"][3:]
         k_ms = sum(gemm_launch_ms) or hr["phase_ms"][1] or hr["ms_per_step"]
         nmod = OZAKI_MODULI
-        int8_ops = 2.0 * nmod * M * (2 * N) * (2 * K)  # residue GEMMs: m x 2n x 2k per modulus
+        # residue GEMMs: three real products of m x n x k per modulus (complex)
+        int8_ops = 2.0 * nmod * 3 * M * N * K
         achieved = int8_ops / (k_ms / 1e3) / 1e12
         peak = peaks.get("int8_tops")
         # DRAM bytes of one GEMM launch of this workload (m=n=1024, k=250000), from a one-pass
-        # ncu capture of oz_gemm_pair on it: 52.89 GB read + 0.472 GB written
-        traffic = 52.89e9 + 0.472e9 if (M, N, K) == (1024, 1024, 250000) else None
+        # ncu capture of oz_gemm_pair on it
+        traffic = None
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
                 "frac": (achieved / peak) if peak else None, "traffic": traffic,
                 "traffic_source": "ncu dram__bytes_{read,write}.sum of oz_gemm_pair, one-pass "
                                   "capture of this launch (profiles/oz_gemm_pair_int8_traffic_"
                                   "zgemm_m1024_k250000.md)",
-                "algorithmic_residue_bytes": float(OZAKI_MODULI) * (M + 2 * N) * 2 * K,
+                "algorithmic_residue_bytes": float(OZAKI_MODULI) * 3 * (M + N) * K,
                 "kernel": "oz_gemm_pair (tcgen05.mma.cta_group::2.kind::i8, TMA, TMEM)",
                 "peak_source": "measured here: cuBLASLt int8 GEMM 8192^3 via torch._int_mm",
                 "algorithmic_ops_per_launch": int8_ops}

@@ -225,22 +225,26 @@ __device__ __forceinline__ uint32_t pack4(float a, float b, float c, float d) {
 }
 
 
-// Residues of one operand, written K-major: res[t][row][l] (row stride kp).
+// Residues of one operand, written K-major (row stride kp bytes).
 // Each thread handles EL (8 or 16) consecutive reals of one row.
-// mode 0: plain rows (A rows, or B rows of a real product): out row = row.
-// mode 1: complex B rows -> u row `row` and v row `row + rows` with sign s:
-//         u = (br, -s*bi), v = (bi, s*br) interleaved.
+// mode 0: real rows: res[t][row][l], l < kp.
+// mode 2: complex rows for the three-product (Karatsuba) form: complex element
+//         e = (re, im) of row `row` goes to three planes of `rows` x kp bytes,
+//         res[t][0][row][e] = r(re), res[t][1][row][e] = r(im) and
+//         res[t][2][row][e] = r(re + s_sum im) (residues are linear in the
+//         scaled integers, so the third is r(re) + s_sum r(im) reduced mod p).
+//         The input row then holds 2 kp reals (kp complex elements).
 // TIn: double (|x| < 2^62, five digits) or float (|x| < 2^38, three digits).
 // NMU > 0: moduli 0 .. NMU-1 in one fully unrolled pass (the per-modulus
 // constants become fixed parameter operands); 0: t_begin .. t_end-1 in a loop.
 template <typename TIn, bool VEC, int NDIG, int EL, int NMU>
 __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
     oz_slice(const TIn* __restrict__ X, int64_t ld_doubles, int64_t len, int rows, int64_t kp,
-             const int* __restrict__ sigma, int mode, int s_sign, int8_t* __restrict__ res,
+             const int* __restrict__ sigma, int mode, int s_sum, int8_t* __restrict__ res,
              int64_t res_mod_stride, SliceConsts sc, int t_begin, int t_end) {
   static_assert(EL == 8 || EL == 16, "8 or 16 reals per thread");
   constexpr int W = EL / 4;  // packed words per modulus
-  const int64_t groups = kp / EL;
+  const int64_t groups = (mode == 2 ? 2 * kp : kp) / EL;
   const int64_t gid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   const int row = int(gid / groups);
   if (row >= rows) return;
@@ -313,7 +317,7 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
     float r[EL];
 #pragma unroll
     for (int i = 0; i < EL / 2; ++i) f2_unpack(rp2[i], r[2 * i], r[2 * i + 1]);
-    uint32_t wu[W], wv[W];
+    uint32_t wu[W];
     if (mode == 0) {
 #pragma unroll
       for (int q = 0; q < W; ++q)
@@ -323,29 +327,37 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
       else
         *reinterpret_cast<uint2*>(out) = make_uint2(wu[0], wu[1]);
     } else {
-      // complex element e: reals (2e, 2e + 1) = (br, bi); u = (br, -s bi),
-      // v = (bi, s br). -r is MAGIC - r = 2 MAGIC - (MAGIC + r), exact.
-      float ng[EL];
+      // complex elements e = 0 .. EL/2-1: rp2[e] = (MAGIC + r(re), MAGIC + r(im));
+      // t_e = r(re) + s_sum r(im), |t_e| < 2^16, reduced to the nearest
+      // residue as in the digit path (for p = 256 the residues are the low
+      // bytes of unreduced values and the reduction gives the low byte too)
+      constexpr int NC = EL / 2;  // complex elements per thread
+      const unsigned long long np = sc.neg_p[t], ip = sc.inv_p[t];
+      const float fs = float(s_sum);
+      float tsum[NC];
 #pragma unroll
-      for (int i = 0; i < EL / 2; ++i) f2_unpack(f2_fma(rp2[i], NEG1, TWO_M2), ng[2 * i], ng[2 * i + 1]);
-#pragma unroll
-      for (int q = 0; q < W; ++q) {
-        const float br0 = r[4 * q], bi0 = r[4 * q + 1], br1 = r[4 * q + 2], bi1 = r[4 * q + 3];
-        if (s_sign < 0) {
-          wu[q] = pack4(br0, bi0, br1, bi1);
-          wv[q] = pack4(bi0, ng[4 * q], bi1, ng[4 * q + 2]);
-        } else {
-          wu[q] = pack4(br0, ng[4 * q + 1], br1, ng[4 * q + 3]);
-          wv[q] = pack4(bi0, br0, bi1, br1);
-        }
+      for (int e = 0; e < NC; ++e) {
+        float a, b;
+        f2_unpack(f2_add(rp2[e], NM2), a, b);
+        tsum[e] = fmaf(fs, b, a);
       }
-      int8_t* out_v = out + int64_t(rows) * kp;
-      if constexpr (W == 4) {
-        *reinterpret_cast<uint4*>(out) = make_uint4(wu[0], wu[1], wu[2], wu[3]);
-        *reinterpret_cast<uint4*>(out_v) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
-      } else {
-        *reinterpret_cast<uint2*>(out) = make_uint2(wu[0], wu[1]);
-        *reinterpret_cast<uint2*>(out_v) = make_uint2(wv[0], wv[1]);
+      float rs[NC];
+#pragma unroll
+      for (int e = 0; e < NC; e += 2) {
+        const unsigned long long t2 = f2_pack(tsum[e], tsum[e + 1]);
+        const unsigned long long q2 = f2_add(f2_fma(t2, ip, M2), NM2);
+        f2_unpack(f2_add(f2_fma(q2, np, t2), M2), rs[e], rs[e + 1]);
+      }
+      const int64_t plane = int64_t(rows) * kp;
+      int8_t* o = out0 - l0 + l0 / 2 + t * res_mod_stride;  // complex offset l0 / 2
+#pragma unroll
+      for (int q = 0; q < NC / 4; ++q) {
+        const uint32_t w_re = pack4(r[8 * q], r[8 * q + 2], r[8 * q + 4], r[8 * q + 6]);
+        const uint32_t w_im = pack4(r[8 * q + 1], r[8 * q + 3], r[8 * q + 5], r[8 * q + 7]);
+        const uint32_t w_s = pack4(rs[4 * q], rs[4 * q + 1], rs[4 * q + 2], rs[4 * q + 3]);
+        *reinterpret_cast<uint32_t*>(o + 4 * q) = w_re;
+        *reinterpret_cast<uint32_t*>(o + plane + 4 * q) = w_im;
+        *reinterpret_cast<uint32_t*>(o + 2 * plane + 4 * q) = w_s;
       }
     }
   };
@@ -366,8 +378,9 @@ struct GemmParams {
   int kblocks;       // kp / 128
   int nchunks;       // ceil(kblocks / kChunkBlocks)
   int chunk_blocks;  // k-blocks per chunk: ceil(kblocks / nchunks) <= kChunkBlocks
-  int nmod;
-  int t0;            // first modulus of this launch (units cover t0 ..)
+  int nmod;          // products: moduli x nsub (the A/B/R planes in order)
+  int nsub;          // products per modulus (3 complex, 1 real): modulus = product / nsub
+  int t0;            // first product of this launch (units cover t0 ..)
   int tiles_m, tiles_n;
   int total_units;   // moduli of the launch * nchunks * tiles
   int* R;            // accumulated residues [nmod][nb][m] (int32), or
@@ -550,8 +563,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
       const Unit w = decode_unit(u, g);
       if (!mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)) break;
       tc_fence_after();
-      const int p = g.p[w.t], c16 = g.c16[w.t], off = g.off[w.t];
-      const unsigned M = g.M[w.t];
+      const int mt = w.t / g.nsub;  // modulus of this product
+      const int p = g.p[mt], c16 = g.c16[mt], off = g.off[mt];
+      const unsigned M = g.M[mt];
       const int i = w.tm * BM + row;
       const int j0 = w.tn * BN;
       int* Rt = g.R + int64_t(w.t) * g.nb * g.m;
@@ -795,8 +809,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, 1)
       unit_of(u, t, c, tm, tn);
       if (!mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)) break;
       tc_fence_after();
-      const int p = g.p[t], c16 = g.c16[t], off = g.off[t];
-      const unsigned M = g.M[t];
+      const int mt = t / g.nsub;  // modulus of this product
+      const int p = g.p[mt], c16 = g.c16[mt], off = g.off[mt];
+      const unsigned M = g.M[mt];
       const int i = tm * 256 + row;
       const int jw = tn * (256 * NT) + half * kCols;
       const int64_t plane = int64_t(t) * g.nb * g.m;
@@ -900,194 +915,66 @@ __device__ __forceinline__ void store_c(void* C, int64_t ci, double xr, double x
   }
 }
 
-// C(i, j) <- alpha * 2^(-sigma_i - tau_j) * X + beta * C(i, j); complex: real
-// part from R row j, imaginary part from R row n + j. R holds int32 sums of
-// per-chunk residues or, with one k-chunk, the residues as bytes (RT). Threads
-// run along i (contiguous in R and C), blocks along j: no index division.
-// V4 (byte residues, m % 4 == 0): each thread takes four consecutive rows and
-// loads their residues of one modulus as one 32-bit word. NM: the number of
-// moduli when fixed at compile time (the defaults), 0 for rp.n.
-template <int DT, typename RT, bool V4, int NM>
-__global__ void __launch_bounds__(256, 2) oz_reconstruct(const RT* __restrict__ R, int m, int n, int nb,
-                               const int* __restrict__ sigA, const int* __restrict__ sigB,
-                               void* C, int64_t ldc, double alr, double ali, double ber,
-                               double bei, int fill, int64_t ro, int64_t co, int tile_m, int tile_n,
-                               ReconParams rp) {
+// Residues of element (i, j) of the real result (real types) or of Re and Im
+// (complex: three product planes per modulus combined by combine3), for
+// modulus t. src points at plane 0 of modulus t, element (i, j); planes of
+// one product are `plane` elements apart. off: p for byte residues, off24 for
+// int32 sums.
+template <bool CPLX, typename RT>
+__device__ __forceinline__ void product_residues(const RT* src, int64_t plane, int off, int conj,
+                                                 int& re, int& im) {
+  if (CPLX) {
+    combine3(int(src[0]), int(src[plane]), int(src[2 * plane]), off, conj, re, im);
+  } else {
+    re = int(src[0]);
+    im = 0;
+  }
+}
+
+// C(i, j) <- alpha * 2^(-sigma_i - tau_j) * X + beta * C(i, j), X the CRT
+// value of the product (complex: of Re and Im). R holds, per product plane,
+// int32 sums of per-chunk residues or, with one k-chunk, the residues as
+// bytes (RT). Threads run along i (contiguous in R and C), blocks along j: no
+// index division. NM: the number of moduli when fixed at compile time (the
+// defaults), 0 for rp.n.
+template <int DT, typename RT, int NM>
+__global__ void __launch_bounds__(256, 2) oz_reconstruct(const RT* __restrict__ R, int m, int n,
+                                                         int nb, const int* __restrict__ sigA,
+                                                         const int* __restrict__ sigB, void* C,
+                                                         int64_t ldc, double alr, double ali,
+                                                         double ber, double bei, int fill,
+                                                         int64_t ro, int64_t co, int tile_m,
+                                                         int tile_n, ReconParams rp) {
   constexpr bool CPLX = dtype_is_complex(DT);
-  constexpr int NV = V4 ? 4 : 1;
+  constexpr int NSUB = CPLX ? 3 : 1;
   constexpr bool kBytes = sizeof(RT) == 1;
+  constexpr int NMAX = NM > 0 ? NM : kMaxUsableModuli;
+  const int nmod = NM > 0 ? NM : rp.n;
   const int64_t plane = int64_t(nb) * m;
   const bool read_c = (ber != 0.0 || bei != 0.0);
   for (int j = blockIdx.y; j < n; j += gridDim.y) {
     const int tauj = sigB[j];
     const int64_t tj = (j / tile_n) * int64_t(tile_n);
-    for (int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * NV; i0 < m;
-         i0 += gridDim.x * blockDim.x * NV) {
-      if (fill != 0) {  // tile_m is a multiple of 4: the NV rows share a tile
-        const int64_t ti = (i0 / tile_m) * int64_t(tile_m);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+      if (fill != 0) {
+        const int64_t ti = (i / tile_m) * int64_t(tile_m);
         if (!tile_is_active(fill, ti, tj, ::min((int64_t)tile_m, (int64_t)m - ti),
                             ::min((int64_t)tile_n, (int64_t)n - tj), ro, co))
           continue;
       }
-      const RT* src = R + int64_t(j) * m + i0;
-      if constexpr (V4) {
-        unsigned wr[kMaxUsableModuli], wi[kMaxUsableModuli];
-        const unsigned* s4 = reinterpret_cast<const unsigned*>(src);
-        const int64_t p4 = plane / 4;
+      int rr[NMAX], ri[NMAX];
+      const RT* src = R + int64_t(j) * m + i;
 #pragma unroll
-        for (int t = 0; t < kMaxUsableModuli; ++t)
-          if (t < rp.n) wr[t] = s4[t * p4];
-        if (CPLX) {
-          const unsigned* s4i = s4 + int64_t(n) * m / 4;
-#pragma unroll
-          for (int t = 0; t < kMaxUsableModuli; ++t)
-            if (t < rp.n) wi[t] = s4i[t * p4];
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int i = i0 + q;
-          const int e = -(sigA[i] + tauj);
-          int r[kMaxUsableModuli];
-#pragma unroll
-          for (int t = 0; t < kMaxUsableModuli; ++t)
-            if (t < rp.n) r[t] = int((wr[t] >> (8 * q)) & 255u);
-          const double xr = scale_pow2(crt_value<NM, kBytes>(r, rp), e);
-          double xi = 0.0;
-          if (CPLX) {
-#pragma unroll
-            for (int t = 0; t < kMaxUsableModuli; ++t)
-              if (t < rp.n) r[t] = int((wi[t] >> (8 * q)) & 255u);
-            xi = scale_pow2(crt_value<NM, kBytes>(r, rp), e);
-          }
-          store_c<DT>(C, i + int64_t(j) * ldc, xr, xi, alr, ali, ber, bei, read_c);
-        }
-      } else {
-        const int i = i0;
-        int r[kMaxUsableModuli];
-#pragma unroll
-        for (int t = 0; t < kMaxUsableModuli; ++t)
-          if (t < rp.n) r[t] = int(src[t * plane]);
-        const int e = -(sigA[i] + tauj);
-        const double xr = scale_pow2(crt_value<NM, kBytes>(r, rp), e);
-        double xi = 0.0;
-        if (CPLX) {
-          src += int64_t(n) * m;
-#pragma unroll
-          for (int t = 0; t < kMaxUsableModuli; ++t)
-            if (t < rp.n) r[t] = int(src[t * plane]);
-          xi = scale_pow2(crt_value<NM, kBytes>(r, rp), e);
-        }
-        store_c<DT>(C, i + int64_t(j) * ldc, xr, xi, alr, ali, ber, bei, read_c);
-      }
+      for (int t = 0; t < NMAX; ++t)
+        if (t < nmod)
+          product_residues<CPLX>(src + t * NSUB * plane, plane, kBytes ? rp.p[t] : rp.off24[t],
+                                 rp.conj, rr[t], ri[t]);
+      const int e = -(sigA[i] + tauj);
+      const double xr = scale_pow2(crt_value<NM, kBytes>(rr, rp), e);
+      const double xi = CPLX ? scale_pow2(crt_value<NM, kBytes>(ri, rp), e) : 0.0;
+      store_c<DT>(C, i + int64_t(j) * ldc, xr, xi, alr, ali, ber, bei, read_c);
     }
   }
-}
-
-// The same reconstruction for byte residues with m % 16 == 0, staged through
-// shared memory: a work item is one column j of C and a block of 1024 rows;
-// its residues (moduli x real/imaginary planes x 1024 bytes) are copied with
-// 16-byte asynchronous copies into one of two stages while the previous item
-// is reconstructed from the other, so that the CRT arithmetic does not wait
-// on the loads. Items are spread over a grid of resident blocks (item =
-// blockIdx.x + k * gridDim.x, row blocks fastest). Each thread takes four
-// consecutive rows: word threadIdx.x of each 1024-byte plane.
-constexpr int kStageRows = 1024;
-template <int DT, int NM>
-__global__ void __launch_bounds__(256, 2)
-    oz_reconstruct_staged(const unsigned char* __restrict__ R, int m, int n, int nb,
-                          const int* __restrict__ sigA, const int* __restrict__ sigB, void* C,
-                          int64_t ldc, double alr, double ali, double ber, double bei, int fill,
-                          int64_t ro, int64_t co, int tile_m, int tile_n, ReconParams rp) {
-  constexpr bool CPLX = dtype_is_complex(DT);
-  constexpr int PARTS = CPLX ? 2 : 1;
-  constexpr int NMAX = NM > 0 ? NM : kMaxUsableModuli;
-  extern __shared__ uint4 stage_smem[];
-  const int nmod = NM > 0 ? NM : rp.n;
-  const int stage_words = PARTS * nmod * (kStageRows / 4);
-  unsigned* stage = reinterpret_cast<unsigned*>(stage_smem);
-  const int64_t plane = int64_t(nb) * m;
-  const int row_blocks = (m + kStageRows - 1) / kStageRows;
-  const int64_t items = int64_t(row_blocks) * n;
-  const bool read_c = (ber != 0.0 || bei != 0.0);
-
-  auto prefetch = [&](int64_t item, int s) {
-    const int rb = int(item % row_blocks), j = int(item / row_blocks);
-    const int i0 = rb * kStageRows;
-    const int chunks = min(kStageRows, m - i0) / 16;  // m % 16 == 0
-    const int total = PARTS * nmod * chunks;
-    unsigned* dst = stage + s * stage_words;
-    for (int c = threadIdx.x; c < total; c += blockDim.x) {
-      const int pl = c / chunks, ch = c - pl * chunks;  // plane: part * nmod + t
-      const int part = pl / nmod, t = pl - part * nmod;
-      const unsigned char* src = R + t * plane + int64_t(j + part * n) * m + i0 + ch * 16;
-      cp_async_16_cg(dst + pl * (kStageRows / 4) + ch * 4, src);
-    }
-  };
-
-  int64_t item = blockIdx.x;
-  if (item < items) prefetch(item, 0);
-  cp_async_commit();
-  int s = 0;
-  for (; item < items; item += gridDim.x) {
-    const int64_t next = item + gridDim.x;
-    if (next < items) prefetch(next, s ^ 1);
-    cp_async_commit();
-    cp_async_wait<1>();
-    __syncthreads();
-    const int rb = int(item % row_blocks), j = int(item / row_blocks);
-    const int i = rb * kStageRows + 4 * threadIdx.x;
-    bool active = i < m;
-    if (active && fill != 0) {  // tile_m is a multiple of 4: the four rows share a tile
-      const int64_t ti = (i / tile_m) * int64_t(tile_m), tj = (j / tile_n) * int64_t(tile_n);
-      active = tile_is_active(fill, ti, tj, ::min((int64_t)tile_m, (int64_t)m - ti),
-                              ::min((int64_t)tile_n, (int64_t)n - tj), ro, co);
-    }
-    if (active) {
-      const unsigned* w = stage + s * stage_words + threadIdx.x;
-      const int tauj = sigB[j];
-      const int4 sa = *reinterpret_cast<const int4*>(sigA + i);
-      const int e[4] = {-(sa.x + tauj), -(sa.y + tauj), -(sa.z + tauj), -(sa.w + tauj)};
-      double xr[4], xi[4] = {0.0, 0.0, 0.0, 0.0};
-      {
-        unsigned wr[NMAX];
-#pragma unroll
-        for (int t = 0; t < NMAX; ++t)
-          if (t < nmod) wr[t] = w[t * (kStageRows / 4)];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          int r[NMAX];
-#pragma unroll
-          for (int t = 0; t < NMAX; ++t)
-            if (t < nmod) r[t] = int((wr[t] >> (8 * q)) & 255u);
-          xr[q] = scale_pow2(crt_value<NM, true>(r, rp), e[q]);
-        }
-      }
-      if (CPLX) {
-        unsigned wi[NMAX];
-#pragma unroll
-        for (int t = 0; t < NMAX; ++t)
-          if (t < nmod) wi[t] = w[(nmod + t) * (kStageRows / 4)];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          int r[NMAX];
-#pragma unroll
-          for (int t = 0; t < NMAX; ++t)
-            if (t < nmod) r[t] = int((wi[t] >> (8 * q)) & 255u);
-          xi[q] = scale_pow2(crt_value<NM, true>(r, rp), e[q]);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        store_c<DT>(C, i + q + int64_t(j) * ldc, xr[q], xi[q], alr, ali, ber, bei, read_c);
-    }
-    __syncthreads();  // the stage is refilled by the next iteration's prefetch
-    s ^= 1;
-  }
-  cp_async_wait<0>();
-}
-
-inline int staged_smem_bytes(bool cplx, int nmod) {
-  return 2 * (cplx ? 2 : 1) * nmod * kStageRows;
 }
 
 // At(kk, i) <- A(i, kk): op(A) = N operands (A stored m-major) are copied
@@ -1114,13 +1001,121 @@ __global__ void oz_transpose(const E* __restrict__ A, int64_t lda, int m, int64_
   }
 }
 
+// The same reconstruction for byte residues with m % 16 == 0, staged through
+// shared memory: a work item is one column j of C and a block of 1024 rows;
+// its residues (moduli x product planes x 1024 bytes) are copied with 16-byte
+// asynchronous copies into one of two stages while the previous item is
+// reconstructed from the other, so that the CRT arithmetic does not wait on
+// the loads. Items are spread over a grid of resident blocks (item =
+// blockIdx.x + k * gridDim.x, row blocks fastest). Each thread takes four
+// consecutive rows: byte q of word threadIdx.x of each 1024-byte plane.
+constexpr int kStageRows = 1024;
+template <int DT, int NM>
+__global__ void __launch_bounds__(256, 2)
+    oz_reconstruct_staged(const unsigned char* __restrict__ R, int m, int n, int nb,
+                          const int* __restrict__ sigA, const int* __restrict__ sigB, void* C,
+                          int64_t ldc, double alr, double ali, double ber, double bei, int fill,
+                          int64_t ro, int64_t co, int tile_m, int tile_n, ReconParams rp) {
+  constexpr bool CPLX = dtype_is_complex(DT);
+  constexpr int NSUB = CPLX ? 3 : 1;
+  constexpr int NMAX = NM > 0 ? NM : kMaxUsableModuli;
+  constexpr int WPP = kStageRows / 4;  // 32-bit words per staged plane
+  extern __shared__ uint4 stage_smem[];
+  const int nmod = NM > 0 ? NM : rp.n;
+  const int stage_words = NSUB * nmod * WPP;
+  unsigned* stage = reinterpret_cast<unsigned*>(stage_smem);
+  const int64_t plane = int64_t(nb) * m;
+  const int row_blocks = (m + kStageRows - 1) / kStageRows;
+  const int64_t items = int64_t(row_blocks) * n;
+  const bool read_c = (ber != 0.0 || bei != 0.0);
+
+  // staged plane pl = t * NSUB + s holds product s of modulus t
+  auto prefetch = [&](int64_t item, int s) {
+    const int rb = int(item % row_blocks), j = int(item / row_blocks);
+    const int i0 = rb * kStageRows;
+    const int chunks = min(kStageRows, m - i0) / 16;  // m % 16 == 0
+    const int total = NSUB * nmod * chunks;
+    unsigned* dst = stage + s * stage_words;
+    for (int c = threadIdx.x; c < total; c += blockDim.x) {
+      const int pl = c / chunks, ch = c - pl * chunks;
+      const unsigned char* src = R + pl * plane + int64_t(j) * m + i0 + ch * 16;
+      cp_async_16_cg(dst + pl * WPP + ch * 4, src);
+    }
+  };
+
+  int64_t item = blockIdx.x;
+  if (item < items) prefetch(item, 0);
+  cp_async_commit();
+  int s = 0;
+  for (; item < items; item += gridDim.x) {
+    const int64_t next = item + gridDim.x;
+    if (next < items) prefetch(next, s ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int rb = int(item % row_blocks), j = int(item / row_blocks);
+    const int i = rb * kStageRows + 4 * threadIdx.x;
+    bool active = i < m;
+    if (active && fill != 0) {  // tile_m is a multiple of 4: the four rows share a tile
+      const int64_t ti = (i / tile_m) * int64_t(tile_m), tj = (j / tile_n) * int64_t(tile_n);
+      active = tile_is_active(fill, ti, tj, ::min((int64_t)tile_m, (int64_t)m - ti),
+                              ::min((int64_t)tile_n, (int64_t)n - tj), ro, co);
+    }
+    if (active) {
+      const unsigned* w = stage + s * stage_words + threadIdx.x;
+      const int tauj = sigB[j];
+      // residues of Re (part 0) or Im (part 1) of row i + q, from the staged
+      // bytes (the arrays of the two parts are built one after the other)
+      auto part_residues = [&](int q, int part, int (&r)[NMAX]) {
+#pragma unroll
+        for (int t = 0; t < NMAX; ++t) {
+          if (t < nmod) {
+            const unsigned* wt = w + t * NSUB * WPP;
+            const int r0 = int((wt[0] >> (8 * q)) & 255u);
+            if (CPLX) {
+              const int r1 = int((wt[WPP] >> (8 * q)) & 255u);
+              const int r2 = int((wt[2 * WPP] >> (8 * q)) & 255u);
+              int re, im;
+              combine3(r0, r1, r2, rp.p[t], rp.conj, re, im);
+              r[t] = part ? im : re;
+            } else {
+              r[t] = r0;
+            }
+          }
+        }
+      };
+#pragma unroll 1
+      for (int q = 0; q < 4; ++q) {  // rolled: one row's chain at a time keeps registers
+        const int e = -(sigA[i + q] + tauj);
+        int r[NMAX];
+        part_residues(q, 0, r);
+        const double xr = scale_pow2(crt_value<NM, true>(r, rp), e);
+        double xi = 0.0;
+        if (CPLX) {
+          part_residues(q, 1, r);
+          xi = scale_pow2(crt_value<NM, true>(r, rp), e);
+        }
+        store_c<DT>(C, i + q + int64_t(j) * ldc, xr, xi, alr, ali, ber, bei, read_c);
+      }
+    }
+    __syncthreads();  // the stage is refilled by the next iteration's prefetch
+    s ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
+inline int staged_smem_bytes(bool cplx, int nmod) {
+  return 2 * (cplx ? 3 : 1) * nmod * kStageRows;
+}
+
 // --------------------------------------------------------------------------
 // host orchestration
 
 struct Layout {
   int nmod;
-  int64_t K2, kp;          // real depth, padded to 128
-  int rowsA, rowsB, nb;    // A rows, B source rows, B residue rows
+  int nsub;                // products per modulus: 3 (complex, Karatsuba) or 1 (real)
+  int64_t K2, kp;          // reals per operand row; residue row length (k padded to 128)
+  int rowsA, rowsB, nb;    // A rows, B rows, B residue rows per product
   bool at;                 // op(A) = N: A is first copied k-major into At
   bool r8;                 // one k-chunk: the residues of C are stored as bytes
   int64_t ldAt;            // leading dimension of At (elements of A's type)
@@ -1134,11 +1129,12 @@ Layout layout_of(const GemmProblem& p, int moduli) {
   L.nmod = moduli > 0 ? std::min(moduli, kMaxUsableModuli)
                       : (dtype_is_double(p.dtype) ? kDefaultModuli : kDefaultModuliFloat);
   const bool cplx = dtype_is_complex(p.dtype);
+  L.nsub = cplx ? 3 : 1;
   L.K2 = cplx ? 2 * p.k : p.k;
-  L.kp = (L.K2 + BKB - 1) / BKB * BKB;
+  L.kp = (p.k + BKB - 1) / BKB * BKB;
   L.rowsA = int(p.m);
   L.rowsB = int(p.n);
-  L.nb = cplx ? int(2 * p.n) : int(p.n);
+  L.nb = int(p.n);
   L.at = p.opA == 0;
   L.r8 = (L.kp / BKB + kChunkBlocks - 1) / kChunkBlocks == 1;
   L.ldAt = L.at ? (p.k + 7) / 8 * 8 : 0;
@@ -1148,11 +1144,11 @@ Layout layout_of(const GemmProblem& p, int moduli) {
   L.off_sigB = off;
   off = align256(off + sizeof(int) * L.rowsB);
   L.off_resA = off;
-  off = align256(off + size_t(L.nmod) * L.rowsA * L.kp);
+  off = align256(off + size_t(L.nmod) * L.nsub * L.rowsA * L.kp);
   L.off_resB = off;
-  off = align256(off + size_t(L.nmod) * L.nb * L.kp);
+  off = align256(off + size_t(L.nmod) * L.nsub * L.nb * L.kp);
   L.off_R = off;
-  off = align256(off + (L.r8 ? 1 : sizeof(int)) * size_t(L.nmod) * L.nb * L.rowsA);
+  off = align256(off + (L.r8 ? 1 : sizeof(int)) * size_t(L.nmod) * L.nsub * L.nb * L.rowsA);
   L.off_At = off;
   off = align256(off + size_t(dtype_bytes(p.dtype)) * size_t(L.rowsA) * size_t(L.ldAt));
   L.off_status = off;
@@ -1257,7 +1253,8 @@ void launch_slice(int ndig, cudaStream_t st, const TIn* X, int64_t ld, int64_t l
                   int64_t kp, const int* sig, int mode, int s_sign, int8_t* res, int64_t stride,
                   const oz::SliceConsts& sc, int t0, int t1) {
   const int el = slice_elems();
-  const unsigned grid = unsigned((int64_t(rows) * (kp / el) + 255) / 256);
+  const int64_t kreal = mode == 2 ? 2 * kp : kp;  // reals per row a thread group covers
+  const unsigned grid = unsigned((int64_t(rows) * (kreal / el) + 255) / 256);
   if (el == 16)
     launch_slice_el<TIn, VEC, 16>(ndig, grid, st, X, ld, len, rows, kp, sig, mode, s_sign, res,
                                   stride, sc, t0, t1);
@@ -1314,20 +1311,24 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
   const int vec_elems = 16 / int(sizeof(TIn));
   const bool vecA = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (ldA % vec_elems == 0);
   const bool vecB = (reinterpret_cast<uintptr_t>(B) % 16 == 0) && (ldB % vec_elems == 0);
-  const int s_sign = p.opA == 2 ? -1 : 1;
-  const int64_t strideA = int64_t(L.rowsA) * L.kp, strideB = int64_t(L.nb) * L.kp;
+  // complex: three planes per modulus, A's third is re(a) - im(a) for A^H
+  // (conj(a) b: Im = r2 - r0 + r1) and re(a) + im(a) otherwise; B's is re + im
+  const int mode = cplx ? 2 : 0;
+  const int sumA = p.opA == 2 ? -1 : 1;
+  const int64_t strideA = int64_t(L.nsub) * L.rowsA * L.kp;
+  const int64_t strideB = int64_t(L.nsub) * L.nb * L.kp;
   if ((which & 1) && vecA)
-    launch_slice<TIn, true>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA, strideA, sc,
-                            t0, t1);
+    launch_slice<TIn, true>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, mode, sumA, resA,
+                            strideA, sc, t0, t1);
   else if (which & 1)
-    launch_slice<TIn, false>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, 0, 1, resA, strideA,
-                             sc, t0, t1);
+    launch_slice<TIn, false>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, mode, sumA, resA,
+                             strideA, sc, t0, t1);
   if ((which & 2) && vecB)
-    launch_slice<TIn, true>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0, s_sign,
-                            resB, strideB, sc, t0, t1);
+    launch_slice<TIn, true>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, mode, 1, resB, strideB,
+                            sc, t0, t1);
   else if (which & 2)
-    launch_slice<TIn, false>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, cplx ? 1 : 0, s_sign,
-                             resB, strideB, sc, t0, t1);
+    launch_slice<TIn, false>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, mode, 1, resB, strideB,
+                             sc, t0, t1);
 }
 
 // Side streams may be used by this host thread (off while a batch captures
@@ -1501,8 +1502,8 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
         slice_operands<float>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, which, s);
     };
     CUtensorMap mapA, mapB;
-    if (!make_map(&mapA, resA, L.kp, int64_t(L.nmod) * L.rowsA, BM) ||
-        !make_map(&mapB, resB, L.kp, int64_t(L.nmod) * L.nb, BN))
+    if (!make_map(&mapA, resA, L.kp, int64_t(L.nmod) * L.nsub * L.rowsA, BM) ||
+        !make_map(&mapB, resB, L.kp, int64_t(L.nmod) * L.nsub * L.nb, BN))
       return cudaErrorNotSupported;
     GemmParams g{};
     g.m = L.rowsA;
@@ -1511,7 +1512,8 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
     g.nchunks = (g.kblocks + kChunkBlocks - 1) / kChunkBlocks;
     // equal chunks (each within the exact INT32 bound): equal work units
     g.chunk_blocks = std::max(1, (g.kblocks + g.nchunks - 1) / std::max(1, g.nchunks));
-    g.nmod = L.nmod;
+    g.nmod = L.nmod * L.nsub;
+    g.nsub = L.nsub;
     g.tiles_m = (L.rowsA + BM - 1) / BM;
     g.tiles_n = (L.nb + BN - 1) / BN;
     g.total_units = g.nmod * g.nchunks * g.tiles_m * g.tiles_n;
@@ -1570,35 +1572,19 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
       g.total_units = g.nmod * g.nchunks * g.tiles_m * g.tiles_n;
       if (p.fill_mode != 0) {
         // compute only the pair tiles that cover an element the reconstruction
-        // writes: its tiles are BM x (BN/2 complex | BN real) of C
+        // writes: its tiles are BM x (BN/2 complex | BN real) of C; a pair tile
+        // covers rows r0 .. r1-1 and columns b0 .. b1-1 of C (B rows = columns)
         const int rt_m = BM, rt_n = cplx ? BN / 2 : BN;
         std::vector<int> act;
         for (int tn = 0; tn < g.tiles_n; ++tn)
           for (int tm = 0; tm < g.tiles_m; ++tm) {
             const int64_t r0 = int64_t(tm) * 256, r1 = std::min<int64_t>(r0 + 256, L.rowsA);
             const int64_t b0 = int64_t(tn) * tile_nb, b1 = std::min<int64_t>(b0 + tile_nb, L.nb);
-            // complex columns covered by the B rows (u rows j, v rows n + j)
-            int64_t cr[2][2] = {{0, 0}, {0, 0}};
-            int ncr = 0;
-            if (!cplx) {
-              cr[ncr][0] = b0;
-              cr[ncr++][1] = b1;
-            } else {
-              if (b0 < p.n) {
-                cr[ncr][0] = b0;
-                cr[ncr++][1] = std::min<int64_t>(b1, p.n);
-              }
-              if (b1 > p.n) {
-                cr[ncr][0] = std::max<int64_t>(b0, p.n) - p.n;
-                cr[ncr++][1] = b1 - p.n;
-              }
-            }
             bool on = false;
-            for (int q = 0; q < ncr && !on; ++q)
-              for (int64_t ti = (r0 / rt_m) * rt_m; ti < r1 && !on; ti += rt_m)
-                for (int64_t tj = (cr[q][0] / rt_n) * rt_n; tj < cr[q][1] && !on; tj += rt_n)
-                  on = tile_is_active(p.fill_mode, ti, tj, std::min<int64_t>(rt_m, p.m - ti),
-                                      std::min<int64_t>(rt_n, p.n - tj), p.fill_ro, p.fill_co);
+            for (int64_t ti = (r0 / rt_m) * rt_m; ti < r1 && !on; ti += rt_m)
+              for (int64_t tj = (b0 / rt_n) * rt_n; tj < b1 && !on; tj += rt_n)
+                on = tile_is_active(p.fill_mode, ti, tj, std::min<int64_t>(rt_m, p.m - ti),
+                                    std::min<int64_t>(rt_n, p.n - tj), p.fill_ro, p.fill_co);
             if (on) act.push_back(tm + tn * g.tiles_m);
           }
         if (act.empty()) act.push_back(0);  // keep the launch well formed
@@ -1616,15 +1602,15 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
           (e = set_dynamic_smem(reinterpret_cast<const void*>(oz_gemm_pair<2>),
                                 PairCfg<2>::SMEM)) != cudaSuccess)
         return e;
-      if (!make_map(&mapA2, resA, L.kp, int64_t(L.nmod) * L.rowsA, 128) ||
-          !make_map(&mapB2, resB, L.kp, int64_t(L.nmod) * L.nb, 128))
+      if (!make_map(&mapA2, resA, L.kp, int64_t(L.nmod) * L.nsub * L.rowsA, 128) ||
+          !make_map(&mapB2, resB, L.kp, int64_t(L.nmod) * L.nsub * L.nb, 128))
         return cudaErrorNotSupported;
     }
-    const int units_per_mod = g.total_units / g.nmod;
+    const int units_per_mod = g.total_units / L.nmod;  // all products of one modulus
     // the INT8 GEMM over moduli t0 .. t1-1 on stream s
     auto launch_gemm = [&](int t0, int t1, cudaStream_t s) -> cudaError_t {
       GemmParams gg = g;
-      gg.t0 = t0;
+      gg.t0 = t0 * L.nsub;
       gg.total_units = (t1 - t0) * units_per_mod;
       if (pair) {
         const int pairs = std::max(1, std::min(gg.total_units, sm_count() / 2));
@@ -1693,17 +1679,16 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
 
   phase_mark(2, false, st);
-  const ReconParams rp = make_recon(crt);
-  // threads along the rows of C (four rows each with byte residues and
-  // m % 4 == 0), one block row covering all of them (no partial second pass),
-  // blocks along the columns (grid-stride beyond 65535); byte residues with
-  // m % 16 == 0 take the shared-memory staged kernel instead
+  ReconParams rp = make_recon(crt);
+  rp.conj = p.opA == 2 ? 1 : 0;
+  // threads along the rows of C, one block row covering all of them (no
+  // partial second pass), blocks along the columns (grid-stride beyond
+  // 65535); byte residues with m % 16 == 0 take the shared-memory staged
+  // kernel instead
   const int threads = 256;
   const bool staged = R8 && L.rowsA % 16 == 0;
-  const bool v4 = R8 && L.rowsA % 4 == 0;
-  const int64_t rows_per_block = int64_t(threads) * (v4 ? 4 : 1);
   const unsigned gy = unsigned(std::min<int64_t>(p.n, 65535));
-  const unsigned gx = unsigned(std::max<int64_t>(1, (p.m + rows_per_block - 1) / rows_per_block));
+  const unsigned gx = unsigned(std::max<int64_t>(1, (p.m + threads - 1) / threads));
   const bool fixed = L.nmod == (dtype_is_double(p.dtype) ? kDefaultModuli : kDefaultModuliFloat);
   if (staged) {
     const int smem = staged_smem_bytes(cplx, L.nmod);
@@ -1749,34 +1734,31 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
   using u8 = unsigned char;
   // the default modulus counts (15 double, 9 float) run a fully unrolled
   // reconstruction
-  auto by_dtype = [&](auto rt_tag, auto v4_tag, const auto* Rsrc) {
+  auto by_dtype = [&](auto rt_tag, const auto* Rsrc) {
     using RT = decltype(rt_tag);
-    constexpr bool V = decltype(v4_tag)::value;
     switch (p.dtype) {
       case kC64:
-        fixed ? recon(oz_reconstruct<kC64, RT, V, kDefaultModuli>, Rsrc)
-              : recon(oz_reconstruct<kC64, RT, V, 0>, Rsrc);
+        fixed ? recon(oz_reconstruct<kC64, RT, kDefaultModuli>, Rsrc)
+              : recon(oz_reconstruct<kC64, RT, 0>, Rsrc);
         break;
       case kC32:
-        fixed ? recon(oz_reconstruct<kC32, RT, V, kDefaultModuliFloat>, Rsrc)
-              : recon(oz_reconstruct<kC32, RT, V, 0>, Rsrc);
+        fixed ? recon(oz_reconstruct<kC32, RT, kDefaultModuliFloat>, Rsrc)
+              : recon(oz_reconstruct<kC32, RT, 0>, Rsrc);
         break;
       case kR64:
-        fixed ? recon(oz_reconstruct<kR64, RT, V, kDefaultModuli>, Rsrc)
-              : recon(oz_reconstruct<kR64, RT, V, 0>, Rsrc);
+        fixed ? recon(oz_reconstruct<kR64, RT, kDefaultModuli>, Rsrc)
+              : recon(oz_reconstruct<kR64, RT, 0>, Rsrc);
         break;
       default:
-        fixed ? recon(oz_reconstruct<kR32, RT, V, kDefaultModuliFloat>, Rsrc)
-              : recon(oz_reconstruct<kR32, RT, V, 0>, Rsrc);
+        fixed ? recon(oz_reconstruct<kR32, RT, kDefaultModuliFloat>, Rsrc)
+              : recon(oz_reconstruct<kR32, RT, 0>, Rsrc);
         break;
     }
   };
-  if (v4)
-    by_dtype(u8{}, std::true_type{}, R8);
-  else if (R8)
-    by_dtype(u8{}, std::false_type{}, R8);
+  if (R8)
+    by_dtype(u8{}, R8);
   else
-    by_dtype(int{}, std::false_type{}, R);
+    by_dtype(int{}, R);
   phase_mark(2, true, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return cudaSuccess;

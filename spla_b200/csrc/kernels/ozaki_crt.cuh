@@ -95,16 +95,36 @@ __host__ __device__ __forceinline__ int mod_residue(int v, int p, int c16, int o
 struct ReconParams {
   int n;
   int p[kMaxModuli];
+  int off24[kMaxModuli];      // p * ceil(2^24 / p): a multiple of p above any int32 residue sum
   unsigned w[kMaxModuli][4];  // CRT weights W_t < P as 32-bit limbs, least significant first
   unsigned P[4];              // P as 32-bit limbs
   double inv_P32;             // 2^32 / P
+  int conj;                   // complex products: A^H B (1) or A^T B / A B (0)
 };
+
+// Residues of Re and Im of a complex product from the residues of the three
+// real products P0 = re(a) re(b), P1 = im(a) im(b), P2 = (re(a) + s im(a))
+// (re(b) + im(b)) with s = -1 for A^H B (conj(a) b: Re = P0 + P1,
+// Im = P2 - P0 + P1) and s = +1 otherwise (Re = P0 - P1, Im = P2 - P0 - P1).
+// off is a multiple of p not below any r (p for bytes, off24 for int32 sums),
+// so the results are non-negative and below 3 off.
+__host__ __device__ __forceinline__ void combine3(int r0, int r1, int r2, int off, int conj,
+                                                  int& re, int& im) {
+  if (conj) {
+    re = r0 + r1;
+    im = r2 + r1 + (off - r0);
+  } else {
+    re = r0 + (off - r1);
+    im = r2 + (off - r0) + (off - r1);
+  }
+}
 
 inline ReconParams make_recon(const Crt& c) {
   ReconParams rp{};
   rp.n = c.n;
   for (int t = 0; t < c.n; ++t) {
     rp.p[t] = c.p[t];
+    rp.off24[t] = c.p[t] * (((1 << 24) + c.p[t] - 1) / c.p[t]);
     const unsigned long long lo = c.w_lo[t], hi = c.w_hi[t];
     rp.w[t][0] = unsigned(lo);
     rp.w[t][1] = unsigned(lo >> 32);
@@ -143,8 +163,8 @@ __host__ __device__ __forceinline__ double u52_to_double(unsigned long long x) {
 // scaled product by (2^Q + sqrt(K)/2)^2 with 2^(2Q) <= P/4.
 //
 // S = sum_t W_t r_t is accumulated per 32-bit limb of W_t (one 32x32->64
-// multiply-add per limb and modulus, no carries: r_t < 2^24 and at most 16
-// terms keep each limb sum below 2^60). S / P lies within 1/4 + 2^-37 of the
+// multiply-add per limb and modulus, no carries: r_t < 2^26 and at most 16
+// terms keep each limb sum below 2^62). S / P lies within 1/4 + 2^-37 of the
 // integer q = round(S / P), and the estimate S * (2^32 / P) from the top
 // three limb sums in double is off by less than 2^-20, so rounding it gives q
 // exactly. X = S - qP is formed limb by limb in signed 64-bit arithmetic,
@@ -153,8 +173,8 @@ __host__ __device__ __forceinline__ double u52_to_double(unsigned long long x) {
 // that each of at most three steps rounds once, relative to a partial value
 // no larger than about |X|).
 //
-// N: number of moduli (0: rp.n at run time). BYTES: residues below 2^8 (the
-// limb sums are then below 2^44 and convert exactly by the mantissa method).
+// N: number of moduli (0: rp.n at run time). BYTES: residues below 2^10 (the
+// limb sums are then below 2^46 and convert exactly by the mantissa method).
 template <int N, bool BYTES>
 __host__ __device__ __forceinline__ double crt_value(const int* r, const ReconParams& rp) {
   unsigned long long l0 = 0, l1 = 0, l2 = 0, l3 = 0;
@@ -185,7 +205,7 @@ __host__ __device__ __forceinline__ double crt_value(const int* r, const ReconPa
 #else
   const unsigned q = unsigned((unsigned long long)(qr - 6755399441055744.0));
 #endif
-  // X = S - qP, limb by limb (each difference lies in (-2^60, 2^60)), carried
+  // X = S - qP, limb by limb (each difference lies in (-2^62, 2^62)), carried
   const unsigned long long qq = q;
   long long c = (long long)(l0 - qq * rp.P[0]);
   const unsigned x0 = unsigned(c);

@@ -126,14 +126,15 @@ double dmma_ms(const GemmProblem& p) {
 double ozaki_ms(const GemmProblem& p) {
   const bool c = dtype_is_complex(p.dtype);
   const int nmod = dtype_is_double(p.dtype) ? 15 : 9;
-  const double K2 = c ? 2.0 * p.k : double(p.k), nb = c ? 2.0 * p.n : double(p.n);
-  const double kp = std::ceil(K2 / 128.0) * 128.0;
+  const double nsub = c ? 3.0 : 1.0;  // complex: three real products per modulus
+  const double K2 = c ? 2.0 * p.k : double(p.k);
+  const double kp = std::ceil(p.k / 128.0) * 128.0;
   const double reals = double(p.m + p.n) * K2;
   const double slice = 6.0e-13 * reals * nmod + reals * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12;
-  const double tiles = std::ceil(p.m / 256.0) * std::ceil(nb / 256.0);
+  const double tiles = std::ceil(p.m / 256.0) * std::ceil(p.n / 256.0) * nsub;
   const double chunks = std::ceil(kp / 128.0 / 976.0);
-  const double gemm = 2.0 * nmod * p.m * nb * kp / (2.8e15 * fill(nmod * chunks * tiles));
-  const double recon = 3e-12 * p.m * nb * nmod;
+  const double gemm = 2.0 * nmod * nsub * p.m * p.n * kp / (2.8e15 * fill(nmod * chunks * tiles));
+  const double recon = 3e-12 * p.m * (c ? 2.0 * p.n : double(p.n)) * nmod;
   // op(A) = N: A is first copied k-major (one read, one write)
   const double transpose =
       p.opA == 0 ? 2.0 * p.m * K2 * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12 : 0.0;

@@ -8,6 +8,7 @@
 // modulo each modulus (edges of the int32 range, around zero, random) and the
 // CRT weights: W_t = 1 mod p_t and 0 mod p_s (s != t). Prints "OK <cases>" on
 // success.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <random>
@@ -72,12 +73,43 @@ int main() {
         printf("FAIL fixed n=9 it=%d\n", it);
         return 1;
       }
-      // unreduced residues (sums of per-chunk residues, below 2^24)
+      // unreduced residues (combinations of per-chunk residue sums, below 2^26)
       for (int t = 0; t < n; ++t)
-        r[t] += c.p[t] * int(rng() % ((1u << 24) / unsigned(c.p[t]) - 1));
+        r[t] += c.p[t] * int(rng() % ((1u << 26) / unsigned(c.p[t]) - 1));
       const double got2 = crt_value<0, false>(r, rp);
       if (bad(got2)) {
         printf("FAIL unreduced n=%d it=%d got %.17g want %.17g\n", n, it, got2, want);
+        return 1;
+      }
+      ++cases;
+    }
+    // complex products from three real ones: random P0, P1 (|Re| < 2^57), Im
+    // with |Im| <= P/4 and P2 chosen to match; residues combined per modulus
+    // (byte residues, or unreduced int32 sums with the off24 offsets)
+    for (int it = 0; it < 4000; ++it) {
+      const int conj = it & 1;
+      const i128 im = (i128(int64_t(rng())) * i128(rng() % 64)) % (quarter + 1);
+      const i128 P0 = i128(int64_t(rng() >> 8)), P1 = i128(int64_t(rng() >> 8));
+      // conj: Re = P0 + P1, Im = P2 - P0 + P1; else Re = P0 - P1, Im = P2 - P0 - P1
+      const i128 P2 = conj ? im + P0 - P1 : im + P0 + P1;
+      const i128 re_x = conj ? P0 + P1 : P0 - P1;
+      int rr[kMaxModuli], ri[kMaxModuli];
+      for (int t = 0; t < n; ++t) {
+        const int pt = c.p[t];
+        const bool bytes = (it >> 1) & 1;
+        const int off = bytes ? pt : rp.off24[t];
+        // byte residues, or unreduced sums below 2^24
+        const int extra = bytes ? 0 : pt * int(rng() % ((1u << 24) / unsigned(pt) - 1));
+        combine3(mod_pos(P0, pt) + (bytes ? 0 : extra), mod_pos(P1, pt), mod_pos(P2, pt), off, conj,
+                 rr[t], ri[t]);
+      }
+      const double want_im = double((long double)im);
+      const double g_re = crt_value<0, false>(rr, rp), g_im = crt_value<0, false>(ri, rp);
+      const double w_re = double((long double)re_x);
+      if (std::fabs(g_re - w_re) > std::fabs(w_re) * 3.4e-16 ||
+          std::fabs(g_im - want_im) > std::fabs(want_im) * 3.4e-16) {
+        printf("FAIL combine n=%d it=%d re %.17g/%.17g im %.17g/%.17g\n", n, it, g_re, w_re,
+               g_im, want_im);
         return 1;
       }
       ++cases;
