@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
   // 2^sg as a double when representable, else ldexp per element
   const bool direct = sg > -1000 && sg < 1000;
   const double scale = direct ? __longlong_as_double((long long)(sg + 1023) << 52) : 1.0;
-  unsigned long long dp[EL / 2][5];  // digits of elements 2i, 2i + 1
+  unsigned long long dp[EL / 2][5];  // digits of the element pairs (see below)
   {
     double v[EL];
     if (VEC && l0 + EL <= len) {
@@ -278,6 +278,18 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
     } else {
 #pragma unroll
       for (int i = 0; i < EL; ++i) v[i] = (l0 + i < len) ? double(x[i]) : 0.0;
+    }
+    // pairs (2i, 2i + 1) in mode 0; in mode 2 the real parts pair up first,
+    // then the imaginary parts: (re0, re1), (re2, re3), ..., (im0, im1), ...
+    if (mode == 2) {
+      double u[EL];
+#pragma unroll
+      for (int i = 0; i < EL / 2; ++i) {
+        u[i] = v[2 * i];
+        u[EL / 2 + i] = v[2 * i + 1];
+      }
+#pragma unroll
+      for (int i = 0; i < EL; ++i) v[i] = u[i];
     }
 #pragma unroll
     for (int i = 0; i < EL / 2; ++i) {
@@ -327,37 +339,36 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
       else
         *reinterpret_cast<uint2*>(out) = make_uint2(wu[0], wu[1]);
     } else {
-      // complex elements e = 0 .. EL/2-1: rp2[e] = (MAGIC + r(re), MAGIC + r(im));
-      // t_e = r(re) + s_sum r(im), |t_e| < 2^16, reduced to the nearest
-      // residue as in the digit path (for p = 256 the residues are the low
-      // bytes of unreduced values and the reduction gives the low byte too)
-      constexpr int NC = EL / 2;  // complex elements per thread
+      // rp2[h] = MAGIC + residues of (re_2h, re_2h+1), rp2[H + h] those of the
+      // imaginary parts. Third plane: t = r(re) + s_sum r(im) (|t| < 2^16):
+      // MAGIC + t exactly in one FMA, t, its nearest quotient by p and
+      // MAGIC + (t - q p) = (MAGIC + t) - q p (for p = 256 the residues are
+      // unreduced low bytes and the reduction gives the low byte of the sum)
+      constexpr int H = EL / 4;  // pairs of complex elements
       const unsigned long long np = sc.neg_p[t], ip = sc.inv_p[t];
-      const float fs = float(s_sum);
-      float tsum[NC];
+      const unsigned long long S2 = f2_pack(float(s_sum), float(s_sum));
+      unsigned long long sm2[H];
 #pragma unroll
-      for (int e = 0; e < NC; ++e) {
-        float a, b;
-        f2_unpack(f2_add(rp2[e], NM2), a, b);
-        tsum[e] = fmaf(fs, b, a);
-      }
-      float rs[NC];
-#pragma unroll
-      for (int e = 0; e < NC; e += 2) {
-        const unsigned long long t2 = f2_pack(tsum[e], tsum[e + 1]);
+      for (int h = 0; h < H; ++h) {
+        const unsigned long long tM = f2_fma(S2, f2_add(rp2[H + h], NM2), rp2[h]);
+        const unsigned long long t2 = f2_add(tM, NM2);
         const unsigned long long q2 = f2_add(f2_fma(t2, ip, M2), NM2);
-        f2_unpack(f2_add(f2_fma(q2, np, t2), M2), rs[e], rs[e + 1]);
+        sm2[h] = f2_fma(q2, np, tM);
       }
       const int64_t plane = int64_t(rows) * kp;
       int8_t* o = out0 - l0 + l0 / 2 + t * res_mod_stride;  // complex offset l0 / 2
 #pragma unroll
-      for (int q = 0; q < NC / 4; ++q) {
-        const uint32_t w_re = pack4(r[8 * q], r[8 * q + 2], r[8 * q + 4], r[8 * q + 6]);
-        const uint32_t w_im = pack4(r[8 * q + 1], r[8 * q + 3], r[8 * q + 5], r[8 * q + 7]);
-        const uint32_t w_s = pack4(rs[4 * q], rs[4 * q + 1], rs[4 * q + 2], rs[4 * q + 3]);
-        *reinterpret_cast<uint32_t*>(o + 4 * q) = w_re;
-        *reinterpret_cast<uint32_t*>(o + plane + 4 * q) = w_im;
-        *reinterpret_cast<uint32_t*>(o + 2 * plane + 4 * q) = w_s;
+      for (int w = 0; w < H / 2; ++w) {
+        float a0, a1, a2, a3;
+        f2_unpack(rp2[2 * w], a0, a1);
+        f2_unpack(rp2[2 * w + 1], a2, a3);
+        *reinterpret_cast<uint32_t*>(o + 4 * w) = pack4(a0, a1, a2, a3);
+        f2_unpack(rp2[H + 2 * w], a0, a1);
+        f2_unpack(rp2[H + 2 * w + 1], a2, a3);
+        *reinterpret_cast<uint32_t*>(o + plane + 4 * w) = pack4(a0, a1, a2, a3);
+        f2_unpack(sm2[2 * w], a0, a1);
+        f2_unpack(sm2[2 * w + 1], a2, a3);
+        *reinterpret_cast<uint32_t*>(o + 2 * plane + 4 * w) = pack4(a0, a1, a2, a3);
       }
     }
   };
