@@ -1498,7 +1498,8 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
   }
   // byte residues are stored, not accumulated: every element the
   // reconstruction reads is written by the GEMM
-  if (!L.r8) cudaMemsetAsync(R, 0, sizeof(int) * size_t(L.nmod) * L.nb * L.rowsA, st);
+  if (!L.r8)
+    cudaMemsetAsync(R, 0, sizeof(int) * size_t(L.nmod) * L.nsub * L.nb * L.rowsA, st);
   cudaMemsetAsync(status, 0, sizeof(int), st);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (p.k <= 0) {

@@ -1,7 +1,8 @@
 """Ozaki scheme II path (INT8 tcgen05) against the double-double oracle.
 
-Covers: complex A^H B and A^T B, real A^T B, partial tiles in both
-dimensions, several k-chunks (k*2 > 124928), alpha/beta with C offsets and
+Covers: complex A^H B and A^T B (three real products per modulus), real
+A^T B, partial tiles in both dimensions, several k-chunks (k > 124928), the
+workspace reused by a second call, alpha/beta with C offsets and
 ldc padding, k = 0, the modulus-count knob, the fill-mode tile skipping,
 op(A) = N (pgemm_sbs and gemm: A copied k-major first) with one k-chunk (byte
 residues) and several (int32 sums), more row tiles than one band of the unit
@@ -51,7 +52,7 @@ def block(x, ldc, m, n, ro, co):
 
 @pytest.mark.parametrize("opA", [2, 1])
 def test_complex_multi_chunk_partial_tiles(opA):
-    m, n, k = 300, 150, 150000  # 2k = 300000 -> 3 k-chunks; 3 x 2 tiles, partial
+    m, n, k = 300, 150, 150000  # rows of 150016 bytes -> 2 k-chunks; partial tiles
     C0, got, ref, ldc = run_ssb(np.complex128, m, n, k, opA)
     err = oracle.rel_fro(got, ref)
     assert err <= 1e-14, err
@@ -72,7 +73,7 @@ def test_pair_tile_widths(nt, monkeypatch):
     """Both INT8 GEMM tile widths (CTA pair 256 x 256 and 256 x 512) on a
     problem with partial tiles in both dimensions and two k-chunks."""
     monkeypatch.setenv("SPLAB_OZAKI_NT", nt)
-    m, n, k = 333, 291, 70000  # real form 333 x 582, 2k = 140000 -> 2 chunks
+    m, n, k = 333, 291, 130000  # residue rows of 130048 bytes -> 2 chunks
     C0, got, ref, ldc = run_ssb(np.complex128, m, n, k, 2)
     assert oracle.rel_fro(got, ref) <= 1e-14
 
@@ -157,9 +158,9 @@ def test_sbs_op_n(dt, tol):
 
 
 def test_gemm_op_n_multi_chunk():
-    """gemm(N, N) on the Ozaki path with 2k > 124928 (two k-chunks: the
+    """gemm(N, N) on the Ozaki path with k > 124928 (two k-chunks: the
     residues are int32 sums) and a padded A."""
-    m, n, k, lda = 90, 40, 70000, 97
+    m, n, k, lda = 90, 40, 130000, 97
     alpha, beta = 1.0 - 0.5j, -0.5 + 0.25j
     A = buffer(np.complex128, lda, k, 41, "gauss_k", k)
     B = buffer(np.complex128, k, n, 42, "gauss_k", k)
@@ -205,6 +206,28 @@ def test_staged_reconstruction(dt, tol, m, moduli):
     alpha, beta = ((0.5 + 0.25j), (-1.0 + 0.5j)) if cplx else (0.5, -1.0)
     C0, got, ref, ldc = run_ssb(dt, m, 70, 500, 2 if cplx else 1, alpha, beta, moduli=moduli)
     assert oracle.rel_fro(got, ref) <= tol
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.float64])
+def test_workspace_reused_across_calls(dt):
+    """Two multi-chunk calls (int32 residue sums) through one context reuse its
+    workspace: the sums of the second call must start from zero in every
+    product plane, so both results match the oracle."""
+    import torch
+    cplx = np.dtype(dt).kind == "c"
+    m, n, k = 130, 70, 140000  # residue rows of 140032 bytes: 2 k-chunks
+    ctx = spla.Context(spla.PU_GPU)
+    ctx.set_fp64_path(spla.PATH_OZAKI)
+    d = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128, 128)
+    for seed in (71, 72):
+        A = buffer(dt, k, m, seed, "gauss_k", k)
+        B = buffer(dt, k, n, seed + 10, "gauss_k", k)
+        dC = torch.zeros(m * n, dtype=torch.complex128 if cplx else torch.float64, device="cuda")
+        spla.pgemm_ssb(m, n, k, 2 if cplx else 1, 1.0, _dev(A), k, _dev(B), k, 0.0, dC, m, 0, 0,
+                       d, ctx)
+        ref = np.zeros(m * n, dtype=dt)
+        assert oracle.pgemm_ssb(m, n, k, 2 if cplx else 1, 1.0, A, k, B, k, 0.0, ref, m, 0, 0) == 0
+        assert oracle.rel_fro(dC.cpu().numpy(), ref) <= 1e-14, seed
 
 
 def test_bounded_wait_failure_path():
