@@ -1,34 +1,39 @@
 // Ozaki scheme II contraction on INT8 tensor cores (tcgen05, sm_100a).
 //
-// C <- alpha * op(A) * op(B) + beta * C for double / complex double with
-// op(A) in {T, C} and op(B) = N (the layout of pgemm_ssb: both operands
-// K-major, reference src/pgemm_ssb/pgemm_ssb_host.cpp:168-171).
+// C <- alpha * op(A) * B + beta * C for float / double / complex with
+// op(A) in {N, T, C} (the layouts of pgemm_ssb, K-major operands, reference
+// src/pgemm_ssb/pgemm_ssb_host.cpp:168-171, and of pgemm_sbs / gemm N N:
+// op(A) = N is first copied K-major).
 //
 // Method (Ozaki, Uchino & Imamura, "Ozaki Scheme II: A GEMM-oriented emulation
 // of floating-point matrix multiplication using an integer modular
 // technique", 2025), restated here in our own formulation:
-//   1. Real form. A complex product is one real GEMM of twice the depth: row i
-//      of op(A) read as 2k reals (its interleaved memory), against two real
-//      rows per column j of B, u_j = (br, -s bi) and v_j = (bi, s br)
-//      interleaved, s = -1 for A^H, +1 for A^T:  Re C_ij = a_i . u_j,
-//      Im C_ij = a_i . v_j.
-//   2. Scaling. Every row x is scaled by 2^sigma so that ||2^sigma x||_2 < 2^Q
-//      and rounded to integers A', B' (exact in double, |.| < 2^Q).
-//      Then |(A' B'^T)_ij| <= ||A'_i|| ||B'_j|| < 2^(2Q) by Cauchy-Schwarz.
-//   3. Residues. For pairwise coprime moduli p_t <= 256 with product
-//      P > 2^(2Q+1), the residues A' mod p_t, B' mod p_t (symmetric, int8)
-//      are multiplied exactly on the INT8 tensor cores with INT32
-//      accumulation (k-chunks of at most 124928 so that 128*128*chunk < 2^31),
-//      reduced mod p_t and accumulated over chunks.
-//   4. Reconstruction. The Chinese remainder theorem gives X = A' B'^T exactly
-//      (|X| < P/2); C = 2^(-sigma_i - tau_j) X, then alpha/beta.
+//   1. Complex products as three real ones (Karatsuba): with a = ar + i ai
+//      and b = br + i bi, P0 = ar.br, P1 = ai.bi, P2 = (ar + s ai).(br + bi),
+//      s = -1 for A^H (Re = P0 + P1, Im = P2 - P0 + P1) and +1 otherwise
+//      (Re = P0 - P1, Im = P2 - P0 - P1). Each is a real GEMM of depth k;
+//      the combination happens on the residues, before the reconstruction.
+//   2. Scaling. Every row x (complex: its interleaved reals) is scaled by
+//      2^sigma so that ||2^sigma x||_2 < 2^Q and rounded to integers A', B'
+//      (exact in double). By Cauchy-Schwarz every entry of the real product,
+//      and Re and Im of the complex one, is below 2^(2Q) <= P/4.
+//   3. Residues. For pairwise coprime moduli p_t <= 256 with product P, the
+//      residues of A', B' mod p_t (symmetric, int8; the third complex plane
+//      is the reduced sum of the first two) are multiplied exactly on the
+//      INT8 tensor cores with INT32 accumulation (k-chunks of at most 124928
+//      so that 128*128*chunk < 2^31), reduced mod p_t and summed over chunks.
+//   4. Reconstruction. The Chinese remainder theorem gives X exactly (|X| <=
+//      P/4, so the quotient S/P rounds to the right integer without
+//      correction); C = 2^(-sigma_i - tau_j) X, then alpha/beta.
 // The only rounding is the integer rounding of step 2 (relative to each row's
 // 2-norm, 2^-Q) and the final conversion of X to double.
 //
-// Kernels: oz_row_scale (row norms -> sigma), oz_slice (scaled residues, int8,
-// K-major, one matrix per modulus), oz_gemm (tcgen05.mma kind::i8, TMA-fed,
-// TMEM accumulators, warp-specialised persistent kernel), oz_reconstruct (CRT +
-// scaling + alpha/beta + fill-mode tile skipping into C).
+// Kernels: oz_transpose (op(A) = N), oz_row_scale (row norms -> sigma),
+// oz_slice (scaled residues, int8, K-major, one plane per modulus and
+// product), oz_gemm_pair / oz_gemm (tcgen05.mma kind::i8, TMA-fed, TMEM
+// accumulators, warp-specialised persistent kernels), oz_reconstruct /
+// oz_reconstruct_staged (CRT + scaling + alpha/beta + fill-mode tile skipping
+// into C).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
