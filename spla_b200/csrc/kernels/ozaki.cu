@@ -1563,20 +1563,21 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
     const char* gk = std::getenv("SPLAB_OZAKI_GEMM");
     const bool pair = !(gk && gk[0] == '1');  // "1sm" selects the single-CTA kernel
     CUtensorMap mapA2, mapB2;
-    // pair tile 256 x 256 (two accumulator buffers: the epilogue of one unit
-    // overlaps the next unit's MMAs) unless the 256 x 512 tile (one A tile for
-    // two MMAs, one 512-column accumulator) needs fewer rounds of work units;
-    // with equal k-chunks the two measured within a few percent of each other
-    // per operation (SPLAB_OZAKI_NT=1|2 overrides)
+    // pair tile 256 x 512 (one A tile for two MMAs, one 512-column
+    // accumulator drained once per unit) when the units are long enough to
+    // hide the drain (128 k-blocks or more) and it needs at most 5 % more
+    // rounds of work units than the double-buffered 256 x 256 tile; measured
+    // 9 % faster on the INT8 GEMM of m = n = 1024, k = 250000 (complex double
+    // and float) under the power cap (SPLAB_OZAKI_NT=1|2 overrides)
     int nt = 1;
-    if (L.nb >= 512) {
+    if (L.nb >= 512 && g.chunk_blocks >= 128) {
       const int pairs = std::max(1, sm_count() / 2);
       auto rounds = [&](int w) {
         const long long units = (long long)g.nmod * g.nchunks * ((L.rowsA + 255) / 256) *
                                 ((L.nb + 256 * w - 1) / (256 * w));
         return double((units + pairs - 1) / pairs);
       };
-      nt = rounds(2) * 2.0 < rounds(1) ? 2 : 1;
+      nt = rounds(2) * 2.0 <= rounds(1) * 1.05 ? 2 : 1;
     }
     if (const char* v = std::getenv("SPLAB_OZAKI_NT")) {
       if (v[0] == '1') nt = 1;
