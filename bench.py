@@ -757,8 +757,8 @@ def main():
         achieved = int8_ops / (k_ms / 1e3) / 1e12
         peak = peaks.get("int8_tops")
         # DRAM bytes of one GEMM launch of this workload (m=n=1024, k=250000), from a one-pass
-        # ncu capture of oz_gemm_pair on it: 29.99 GB read + 0.290 GB written
-        traffic = 29.99e9 + 0.290e9 if (M, N, K) == (1024, 1024, 250000) else None
+        # ncu capture of oz_gemm_pair on it: 28.32 GB read + 0.229 GB written
+        traffic = 28.32e9 + 0.229e9 if (M, N, K) == (1024, 1024, 250000) else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
                 "frac": (achieved / peak) if peak else None, "traffic": traffic,
                 "traffic_source": "ncu dram__bytes_{read,write}.sum of oz_gemm_pair, one-pass "
