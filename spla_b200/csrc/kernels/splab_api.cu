@@ -130,11 +130,13 @@ double ozaki_ms(const GemmProblem& p) {
   const double K2 = c ? 2.0 * p.k : double(p.k);
   const double kp = std::ceil(p.k / 128.0) * 128.0;
   const double reals = double(p.m + p.n) * K2;
-  const double slice = 6.0e-13 * reals * nmod + reals * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12;
+  // per real element and modulus: complex rows feed three residue planes
+  const double slice =
+      (c ? 6.0e-13 : 4.0e-13) * reals * nmod + reals * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12;
   const double tiles = std::ceil(p.m / 256.0) * std::ceil(p.n / 256.0) * nsub;
   const double chunks = std::ceil(kp / 128.0 / 976.0);
   const double gemm = 2.0 * nmod * nsub * p.m * p.n * kp / (2.8e15 * fill(nmod * chunks * tiles));
-  const double recon = 3e-12 * p.m * (c ? 2.0 * p.n : double(p.n)) * nmod;
+  const double recon = (c ? 3e-12 * 2.0 : 2e-12) * p.m * double(p.n) * nmod;
   // op(A) = N: A is first copied k-major (one read, one write)
   const double transpose =
       p.opA == 0 ? 2.0 * p.m * K2 * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12 : 0.0;
