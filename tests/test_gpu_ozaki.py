@@ -195,6 +195,25 @@ def test_tall_banded_raster(dt):
     assert oracle.rel_fro(dC.cpu().numpy(), ref) <= 1e-14
 
 
+@pytest.mark.parametrize("dt,tol", [(np.complex128, 1e-14), (np.float32, 1e-6)])
+def test_fill_lower_wide_tile(dt, tol, monkeypatch):
+    """Lower fill mode on the 256 x 512 pair tile (the default for long units,
+    forced here): every element of the triangle is computed, the rest is
+    either computed or unchanged."""
+    monkeypatch.setenv("SPLAB_OZAKI_NT", "2")
+    m = n = 520
+    k = 16500  # residue rows of 16512 bytes: 129 k-blocks
+    C0, got, ref, ldc = run_ssb(dt, m, n, k, 2 if np.dtype(dt).kind == "c" else 1,
+                                fill=spla.FILL_MODE_LOWER)
+    g, r = got.reshape(n, ldc).T[:m], ref.reshape(n, ldc).T[:m]
+    c0 = C0.reshape(n, ldc).T[:m]
+    tri = np.tril(np.ones((m, n), bool))
+    assert oracle.rel_fro(g[tri], r[tri]) <= tol
+    off = ~tri
+    ok = np.isclose(g[off], r[off], rtol=1e-5, atol=1e-7) | (g[off] == c0[off])
+    assert ok.all()
+
+
 @pytest.mark.parametrize("dt,tol,m,moduli", [
     (np.complex128, 1e-14, 3088, 0), (np.float64, 1e-14, 1040, 0),
     (np.complex64, 1e-6, 2064, 0), (np.float32, 1e-6, 1056, 0), (np.complex128, 1e-9, 2064, 12)])
