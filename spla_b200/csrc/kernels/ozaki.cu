@@ -94,29 +94,101 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_
 // 1. row scale exponents
 
 // One block per row: sigma = Q - e where ||row||_2 = f 2^e, f in [0.5, 1).
-// Rows of zeros get sigma = 0.
+// Rows of zeros get sigma = 0, rows holding a NaN or an infinity get
+// kSigmaNonFinite (the reconstruction then writes NaN where they contribute).
+// The sum of squares is kept as S 2^(2E) with E the largest exponent seen
+// (rescaled by exact powers of two when it grows), so rows of any finite
+// magnitude, 1e-300 or 1e300, neither underflow nor overflow.
+constexpr int kSigmaNonFinite = -(1 << 30);
+
+// frexp-style exponent of |v| (v = f 2^e, f in [0.5, 1)); subnormals and
+// zero as -1022, infinities and NaN as 1025
+__device__ __forceinline__ int exponent_of(double v) {
+  const int b = int((__double_as_longlong(v) >> 52) & 0x7FF);
+  return (b == 0 ? 1 : b) - 1022;
+}
+
+__device__ __forceinline__ void scaled_add(double& S, int& E, double S2, int E2) {
+  if (E2 > E) {
+    S = ldexp(S, 2 * (E - E2)) + S2;
+    E = E2;
+  } else {
+    S += ldexp(S2, 2 * (E2 - E));
+  }
+}
+
 template <typename TIn>
 __global__ void oz_row_scale(const TIn* __restrict__ X, int64_t ld_elems, int64_t len, int rows,
                              int q_bits, int* __restrict__ sigma) {
   const int row = blockIdx.x;
   if (row >= rows) return;
   const TIn* x = X + int64_t(row) * ld_elems;
-  double s = 0.0;
-  for (int64_t l = threadIdx.x; l < len; l += blockDim.x) {
-    const double v = double(x[l]);
-    s = fma(v, v, s);
+  double S = 0.0, inv = 0.0;  // sum of (v 2^-E)^2, and 2^-E
+  int E = -2100;              // below any exponent: the first batch sets it
+  // batches of 8 independent loads (memory-level parallelism), one exponent
+  // check per batch
+  const int64_t step = blockDim.x;
+  int64_t l = threadIdx.x;
+  for (; l + 7 * step < len; l += 8 * step) {
+    double v[8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) v[b] = double(x[l + b * step]);
+    int em = exponent_of(v[0]);
+#pragma unroll
+    for (int b = 1; b < 8; ++b) em = max(em, exponent_of(v[b]));
+    if (em > E) {  // rare: rescale the sum to the new largest exponent
+      S = ldexp(S, 2 * (E - em));
+      E = em;
+      inv = ldexp(1.0, -E);
+    }
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const double w = v[b] * inv;
+      S = fma(w, w, S);
+    }
   }
-  __shared__ double red[32];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  for (; l < len; l += step) {
+    const double v = double(x[l]);
+    const int ev = exponent_of(v);
+    if (ev > E) {
+      S = ldexp(S, 2 * (E - ev));
+      E = ev;
+      inv = ldexp(1.0, -E);
+    }
+    const double w = v * inv;
+    S = fma(w, w, S);
+  }
+  __shared__ double redS[32];
+  __shared__ int redE[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    const double S2 = __shfl_xor_sync(0xffffffffu, S, o);
+    const int E2 = __shfl_xor_sync(0xffffffffu, E, o);
+    scaled_add(S, E, S2, E2);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    redS[threadIdx.x >> 5] = S;
+    redE[threadIdx.x >> 5] = E;
+  }
   __syncthreads();
   if (threadIdx.x < 32) {
-    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const bool have = threadIdx.x < (blockDim.x >> 5);
+    S = have ? redS[threadIdx.x] : 0.0;
+    E = have ? redE[threadIdx.x] : -2100;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double S2 = __shfl_xor_sync(0xffffffffu, S, o);
+      const int E2 = __shfl_xor_sync(0xffffffffu, E, o);
+      scaled_add(S, E, S2, E2);
+    }
     if (threadIdx.x == 0) {
-      int e = 0;
-      if (s > 0.0) frexp(sqrt(s), &e);
-      sigma[row] = s > 0.0 ? q_bits - e : 0;
+      if (!(S < 1e300)) {  // NaN or infinite input
+        sigma[row] = kSigmaNonFinite;
+      } else if (S > 0.0) {
+        int e0 = 0;
+        frexp(sqrt(S), &e0);
+        sigma[row] = q_bits - (e0 + E);
+      } else {
+        sigma[row] = 0;
+      }
     }
   }
 }
@@ -893,6 +965,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, 1)
 // --------------------------------------------------------------------------
 // 4. reconstruction
 
+constexpr long long kNaNBits = 0x7FF8000000000000ll;  // quiet NaN
+
 // x * 2^e, correctly rounded: a multiplication by the power of two when the
 // result stays normal (|x| is an integer below 2^128 or zero), ldexp otherwise.
 __device__ __forceinline__ double scale_pow2(double x, int e) {
@@ -985,9 +1059,11 @@ __global__ void __launch_bounds__(256, 2) oz_reconstruct(const RT* __restrict__ 
         if (t < nmod)
           product_residues<CPLX>(src + t * NSUB * plane, plane, kBytes ? rp.p[t] : rp.off24[t],
                                  rp.conj, rr[t], ri[t]);
-      const int e = -(sigA[i] + tauj);
-      const double xr = scale_pow2(crt_value<NM, kBytes>(rr, rp), e);
-      const double xi = CPLX ? scale_pow2(crt_value<NM, kBytes>(ri, rp), e) : 0.0;
+      const int si = sigA[i];
+      const int e = -(si + tauj);
+      double xr = scale_pow2(crt_value<NM, kBytes>(rr, rp), e);
+      double xi = CPLX ? scale_pow2(crt_value<NM, kBytes>(ri, rp), e) : 0.0;
+      if (si == kSigmaNonFinite || tauj == kSigmaNonFinite) xr = xi = __longlong_as_double(kNaNBits);
       store_c<DT>(C, i + int64_t(j) * ldc, xr, xi, alr, ali, ber, bei, read_c);
     }
   }
@@ -1102,15 +1178,17 @@ __global__ void __launch_bounds__(256, 2)
       };
 #pragma unroll 1
       for (int q = 0; q < 4; ++q) {  // rolled: one row's chain at a time keeps registers
-        const int e = -(sigA[i + q] + tauj);
+        const int si = sigA[i + q];
+        const int e = -(si + tauj);
         int r[NMAX];
         part_residues(q, 0, r);
-        const double xr = scale_pow2(crt_value<NM, true>(r, rp), e);
+        double xr = scale_pow2(crt_value<NM, true>(r, rp), e);
         double xi = 0.0;
         if (CPLX) {
           part_residues(q, 1, r);
           xi = scale_pow2(crt_value<NM, true>(r, rp), e);
         }
+        if (si == kSigmaNonFinite || tauj == kSigmaNonFinite) xr = xi = __longlong_as_double(kNaNBits);
         store_c<DT>(C, i + q + int64_t(j) * ldc, xr, xi, alr, ali, ber, bei, read_c);
       }
     }

@@ -6,7 +6,8 @@ workspace reused by a second call, alpha/beta with C offsets and
 ldc padding, k = 0, the modulus-count knob, the fill-mode tile skipping,
 op(A) = N (pgemm_sbs and gemm: A copied k-major first) with one k-chunk (byte
 residues) and several (int32 sums), more row tiles than one band of the unit
-raster, the reconstruction staged through shared memory, and the failure
+raster, the reconstruction staged through shared memory, rows of extreme
+magnitude, NaN/Inf propagation, and the failure
 path of the bounded device waits (no GPU fault: the producer issues no
 copies, every wait runs into a 50 ms bound)."""
 import os
@@ -247,6 +248,63 @@ def test_workspace_reused_across_calls(dt):
         ref = np.zeros(m * n, dtype=dt)
         assert oracle.pgemm_ssb(m, n, k, 2 if cplx else 1, 1.0, A, k, B, k, 0.0, ref, m, 0, 0) == 0
         assert oracle.rel_fro(dC.cpu().numpy(), ref) <= 1e-14, seed
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.float64])
+def test_extreme_row_magnitudes(dt):
+    """Rows of A scaled to 1e-170 and 1e150 (their squared norms would
+    underflow or overflow in plain double): each row of C matches the oracle
+    to 1e-14 of its own norm."""
+    import torch
+    cplx = np.dtype(dt).kind == "c"
+    m, n, k = 64, 40, 3000
+    A = buffer(dt, k, m, 81, "gauss_k", k)
+    B = buffer(dt, k, n, 82, "gauss_k", k)
+    scale = np.ones(m)
+    scale[:16] = 1e-170
+    scale[16:32] = 1e150
+    A = np.ascontiguousarray((A.reshape(m, k) * scale[:, None]).ravel())
+    ctx = spla.Context(spla.PU_GPU)
+    ctx.set_fp64_path(spla.PATH_OZAKI)
+    d = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128, 128)
+    dC = torch.zeros(m * n, dtype=torch.complex128 if cplx else torch.float64, device="cuda")
+    op = 2 if cplx else 1
+    spla.pgemm_ssb(m, n, k, op, 1.0, _dev(A), k, _dev(B), k, 0.0, dC, m, 0, 0, d, ctx)
+    ref = np.zeros(m * n, dtype=dt)
+    assert oracle.pgemm_ssb(m, n, k, op, 1.0, A, k, B, k, 0.0, ref, m, 0, 0) == 0
+    g, r = dC.cpu().numpy().reshape(n, m).T, ref.reshape(n, m).T
+    for i in range(m):
+        mx = np.abs(r[i]).max()  # norm without underflow or overflow of the squares
+        assert np.abs(g[i] - r[i]).max() <= 1e-14 * mx * np.linalg.norm(r[i] / mx), i
+
+
+def test_nan_and_inf_propagate():
+    """A NaN in row 3 of A and an infinity in column 5 of B: that row and
+    column of C come out NaN, every other element matches the oracle."""
+    import torch
+    dt = np.complex128
+    m, n, k = 40, 24, 2000
+    A = buffer(dt, k, m, 91, "gauss_k", k)
+    B = buffer(dt, k, n, 92, "gauss_k", k)
+    A[3 * k + 17] = complex(np.nan, 0.0)
+    B[5 * k + 100] = complex(np.inf, 1.0)
+    ctx = spla.Context(spla.PU_GPU)
+    ctx.set_fp64_path(spla.PATH_OZAKI)
+    d = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128, 128)
+    dC = torch.zeros(m * n, dtype=torch.complex128, device="cuda")
+    spla.pgemm_ssb(m, n, k, 2, 1.0, _dev(A), k, _dev(B), k, 0.0, dC, m, 0, 0, d, ctx)
+    g = dC.cpu().numpy().reshape(n, m).T
+    assert np.isnan(g[3, :]).all() and np.isnan(g[:, 5]).all()
+    A2, B2 = A.copy(), B.copy()
+    A2[3 * k + 17] = 0.0
+    B2[5 * k + 100] = 0.0
+    ref = np.zeros(m * n, dtype=dt)
+    assert oracle.pgemm_ssb(m, n, k, 2, 1.0, A2, k, B2, k, 0.0, ref, m, 0, 0) == 0
+    r = ref.reshape(n, m).T
+    mask = np.ones((m, n), bool)
+    mask[3, :] = False
+    mask[:, 5] = False
+    assert oracle.rel_fro(g[mask], r[mask]) <= 1e-14
 
 
 def test_bounded_wait_failure_path():
