@@ -197,8 +197,8 @@ __global__ void oz_row_scale(const TIn* __restrict__ X, int64_t ld_elems, int64_
 // 2. residues
 
 // Per-modulus constants of the slicer, each stored twice (both halves of an
-// f32x2 operand): -p, 1/p and the digit weights 2^(13 i) mod p in symmetric
-// form, i = 1..4.
+// f32x2 operand): -p, 1/p and the digit weights b^i mod p in symmetric form,
+// i = 1..4 (digit base b = 2^15 with four digits, else 2^13).
 struct SliceConsts {
   int n;
   float p0;  // first modulus (256: residue = low byte of the lowest digit)
@@ -461,8 +461,8 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
 // 3. INT8 residue GEMM on tcgen05
 
 struct GemmParams {
-  int m;             // rows of A per modulus
-  int nb;            // rows of B per modulus
+  int m;             // rows of A per product plane
+  int nb;            // rows of B per product plane
   int kblocks;       // kp / 128
   int nchunks;       // ceil(kblocks / kChunkBlocks)
   int chunk_blocks;  // k-blocks per chunk: ceil(kblocks / nchunks) <= kChunkBlocks
@@ -488,7 +488,7 @@ struct Unit {
   int t, c, tm, tn;
 };
 
-// Tile raster within one (modulus, k-chunk): bands of kBandTiles row tiles,
+// Tile raster within one (product, k-chunk): bands of kBandTiles row tiles,
 // row tiles fastest within a band. The units in flight at one time cover a
 // few row tiles of A and a few column tiles of B, so that each A tile is
 // read from DRAM once even when A is much taller than L2 holds (a plain
