@@ -307,6 +307,17 @@ def test_nan_and_inf_propagate():
     assert oracle.rel_fro(g[mask], r[mask]) <= 1e-14
 
 
+@pytest.mark.parametrize("dt,m,n,k,opA", [(np.complex128, 130, 70, 140000, 2),
+                                          (np.float64, 200, 120, 3000, 1)])
+def test_single_cta_gemm(dt, m, n, k, opA, monkeypatch):
+    """The single-CTA INT8 GEMM kept beside the CTA-pair one
+    (SPLAB_OZAKI_GEMM=1sm): two k-chunks (int32 sums) and one (byte
+    residues)."""
+    monkeypatch.setenv("SPLAB_OZAKI_GEMM", "1sm")
+    C0, got, ref, ldc = run_ssb(dt, m, n, k, opA)
+    assert oracle.rel_fro(got, ref) <= 1e-14
+
+
 def test_bounded_wait_failure_path():
     """The INT8 GEMM's barrier waits are bounded: with the test hook the
     producer issues no copies, the waits give up after 50 ms, the kernel frees
