@@ -1,0 +1,49 @@
+"""bench.py's clock record (host logic, CPU): nvidia-smi samples are kept only
+when they fall inside the timed region of the path asked for, their median SM
+clock and the throttle reasons seen there are reported, and all samples are
+used when none fell inside."""
+import datetime
+import sys
+from pathlib import Path
+
+sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+
+import bench  # noqa: E402
+
+
+def _line(t, mhz, power_cap):
+    ts = datetime.datetime.fromtimestamp(t).strftime("%Y/%m/%d %H:%M:%S.%f")[:-3]
+    cap = "Active" if power_cap else "Not Active"
+    return f"{ts}, {mhz}, 1965, 700.0, 0x4, Not Active, Not Active, Not Active, {cap}"
+
+
+def test_samples_inside_the_path_window(tmp_path, monkeypatch):
+    t0 = 1_800_000_000.0
+    lines = [_line(t0 + 0.00, 1965, False),   # before the timed regions
+             _line(t0 + 1.00, 1965, False),   # DMMA window
+             _line(t0 + 1.02, 1965, False),
+             _line(t0 + 2.00, 1425, True),    # Ozaki window
+             _line(t0 + 2.02, 1500, True),
+             _line(t0 + 2.04, 1455, True),
+             _line(t0 + 3.00, 1965, False)]   # after
+    clk = bench.ClockSampler(0)
+    clk.path = tmp_path / "clocks.csv"
+    clk.path.write_text("\n".join(lines) + "\n")
+    monkeypatch.setattr(bench, "TIMED_WINDOWS", [(1, t0 + 0.9, t0 + 1.1), (2, t0 + 1.9, t0 + 2.1)])
+    oz = clk.summary(2)
+    assert oz["samples_in_timed_regions"] == 3
+    assert oz["sm_mhz"] == 1455
+    assert oz["reasons"] == ["sw_power_cap"]
+    assert oz["sm_max_mhz"] == 1965
+    dm = clk.summary(1)
+    assert dm["samples_in_timed_regions"] == 2 and dm["sm_mhz"] == 1965 and dm["reasons"] == []
+
+
+def test_all_samples_when_none_inside(tmp_path, monkeypatch):
+    t0 = 1_800_000_000.0
+    clk = bench.ClockSampler(0)
+    clk.path = tmp_path / "clocks.csv"
+    clk.path.write_text(_line(t0, 1700, False) + "\n" + _line(t0 + 0.02, 1800, False) + "\n")
+    monkeypatch.setattr(bench, "TIMED_WINDOWS", [(2, t0 + 5.0, t0 + 6.0)])
+    s = clk.summary(2)
+    assert s["samples_in_timed_regions"] == 0 and s["samples"] == 2 and s["sm_mhz"] == 1750
