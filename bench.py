@@ -51,6 +51,12 @@ def set_shape(m, k):
     K = k
     FLOPS = 8.0 * M * N * K
 OZAKI_MODULI = 15  # default modulus count of the library (<= 1e-14 at this k)
+HEADLINE_METRIC = "ZGEMM-SSB TFLOP/s: Ozaki-INT8 vs FP64-DMMA at ≤1e-14 rel err, 1 B200"
+
+
+def workload_name():
+    return (f"pzgemm_ssb C=A^H B complex double m=n={M} k={K}, 1x1 grid 128x128 blocks, "
+            "beta=0")
 
 
 def max_over_ranks(torch, ms, device):
@@ -67,8 +73,12 @@ def whole_job_tflops(flops_per_rank, world, ms_max):
 
 
 def cpu_env():
-    """Thread count and an explicit OpenBLAS core type (must precede loading BLAS)."""
-    n = os.cpu_count() or 1
+    """Thread count (the CPUs this process may run on) and an explicit OpenBLAS
+    core type (must precede loading BLAS)."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        n = os.cpu_count() or 1
     os.environ.setdefault("OPENBLAS_NUM_THREADS", str(n))
     os.environ.setdefault("OMP_NUM_THREADS", str(n))
     try:
@@ -217,7 +227,7 @@ def measured_peaks(torch, device):
 
 
 def rel_err_sampled(dC, A, B, cols=None):
-    """Relative Frobenius error of columns `cols` of C against the Dot2 oracle."""
+    """Relative Frobenius error of columns `cols` of C against the CPU Dot2 oracle."""
     import numpy as np
     import oracle
     cols = cols or (0, N // 2, N - 1)
@@ -225,8 +235,26 @@ def rel_err_sampled(dC, A, B, cols=None):
     Bs = B[list(cols)].cpu().numpy().ravel()
     ref = np.zeros(M * len(cols), np.complex128)
     assert oracle.gemm(2, 0, M, len(cols), K, 1.0, An, K, Bs, K, 0.0, ref, M) == 0
-    got = dC.view(N, M)[list(cols)].cpu().numpy().ravel()
+    got = dC.reshape(N, M)[list(cols)].cpu().numpy().ravel()
     return oracle.rel_fro(got, ref)
+
+
+def dd_reference(torch, spla, A, B):
+    """The whole C = A^H B in double-double on the device (splab_gemm_dd, the
+    device form of the compensated oracle), rounded to complex128, (N, M)."""
+    R = torch.zeros((N, M), dtype=torch.complex128, device=A.device)
+    rc = spla.gemm_dd(3, 2, 0, M, N, K, A, K, B, K, R, M,
+                      stream=torch.cuda.current_stream(A.device).cuda_stream)
+    if rc != 0:
+        raise RuntimeError(f"splab_gemm_dd: status {rc}")
+    torch.cuda.synchronize()
+    return R
+
+
+def rel_err_full(torch, C, R):
+    """||C - R||_F / ||R||_F over the whole C (device or host tensor)."""
+    C = C.to(R.device).reshape(R.shape)
+    return float(torch.linalg.vector_norm(C - R) / torch.linalg.vector_norm(R))
 
 
 def time_device_path(torch, spla, path, A, B, steps, warmup, rank):
@@ -310,19 +338,54 @@ def e2e_public_api(torch, spla, path, A, B, steps, warmup):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    return ms, hC
+    return ms, hC, hA, hB
 
 
-def cpu_reference_run(steps, warmup, budget_s=12.0):
-    """The reference's CPU path on a bounded sample of the workload (same m, n;
-    k reduced), all host threads. Returns (TFLOP/s, info)."""
+def gauss_host(rows, cols, seed, scale, threads):
+    """Column-major complex128 rows x cols buffer, re and im N(0, scale^2),
+    filled by `threads` seeded generators in parallel (one per chunk)."""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+    out = np.empty(rows * cols, np.complex128)
+    flat = out.view(np.float64)
+    nch = 4 * max(1, threads)
+    bounds = np.linspace(0, flat.size, nch + 1).astype(np.int64)
+    gens = [np.random.default_rng(s) for s in np.random.SeedSequence(seed).spawn(nch)]
+
+    def fill(i):
+        part = flat[bounds[i]:bounds[i + 1]]
+        gens[i].standard_normal(out=part)
+        part *= scale
+
+    with ThreadPoolExecutor(max(1, threads)) as ex:
+        list(ex.map(fill, range(nch)))
+    return out
+
+
+def host_load():
+    try:
+        return [float(x) for x in Path("/proc/loadavg").read_text().split()[:3]]
+    except OSError:
+        return None
+
+
+def cpu_reference_run(steps, warmup, A=None, B=None):
+    """The reference's CPU path on the whole workload: one step is one full
+    pzgemm_ssb call (m = n = M, k = K, op = C, beta = 0) through the C ABI of
+    the reference library built from its sources (oracle/_ref), else of the
+    oracle's C restatement, with every host thread this process may run on.
+    `warmup` untimed calls, then `steps` timed calls (as the reference's own
+    benchmark: tests/programs/benchmark.cpp:53-66). A and B: host column-major
+    K x M / K x N complex128 buffers (generated here when None).
+    Returns (TFLOP/s, ms per call, info)."""
     import numpy as np
     cores = cpu_env()
-    from inputs import buffer
     import oracle
-    ksamp = 16384
-    A = buffer(np.complex128, ksamp, M, SEED, "gauss_k", K)
-    B = buffer(np.complex128, ksamp, N, SEED + 1, "gauss_k", K)
+    load_before = host_load()
+    if A is None:
+        s = (1.0 / (2.0 * K)) ** 0.5
+        A = gauss_host(K, M, SEED, s, cores)
+        B = gauss_host(K, N, SEED + 1, s, cores)
     C = np.zeros(M * N, np.complex128)
     if oracle.REF_LIB.exists():
         from capi import SplaCAPI
@@ -331,29 +394,37 @@ def cpu_reference_run(steps, warmup, budget_s=12.0):
         _, dist = ref.block_cyclic(1, 1, 128, 128)
 
         def call():
-            assert ref.pgemm_ssb(np.complex128, M, N, ksamp, 2, 1.0, A, ksamp, B, ksamp, 0.0, C,
-                                 M, 0, 0, dist, ctx) == 0
+            assert ref.pgemm_ssb(np.complex128, M, N, K, 2, 1.0, A, K, B, K, 0.0, C, M, 0, 0,
+                                 dist, ctx) == 0
         kind = "reference"
     else:
         def call():
-            assert oracle.pgemm_ssb(M, N, ksamp, 2, 1.0, A, ksamp, B, ksamp, 0.0, C, M, 0, 0) == 0
+            assert oracle.pgemm_ssb(M, N, K, 2, 1.0, A, K, B, K, 0.0, C, M, 0, 0) == 0
         kind = "port"
-    for _ in range(max(1, warmup)):
+    for _ in range(max(0, warmup)):
         call()
     times = []
-    t_end = time.perf_counter() + budget_s
-    for i in range(max(1, steps)):
+    t_all = time.perf_counter()
+    for _ in range(max(1, steps)):
         t0 = time.perf_counter()
         call()
         times.append(time.perf_counter() - t0)
-        if time.perf_counter() > t_end and i >= 0:
-            break
-    t = statistics.median(times)
-    flops = 8.0 * M * N * ksamp
-    return flops / t / 1e12, dict(kind=kind, cores=cores, sample=(
-        f"pzgemm_ssb m=n={M} k={ksamp} (k sampled from {K}), op=C, {len(times)} timed calls, "
-        f"median {t * 1e3:.1f} ms, OPENBLAS_CORETYPE={os.environ.get('OPENBLAS_CORETYPE')}, "
-        f"cpu={cpu_model()}"))
+    ms = (time.perf_counter() - t_all) * 1e3 / len(times)
+    flops = 8.0 * M * N * K
+    try:
+        quota = Path("/sys/fs/cgroup/cpu.max").read_text().strip()
+    except OSError:
+        quota = None
+    info = dict(kind=kind, cores=cores, sample=(
+        f"pzgemm_ssb m=n={M} k={K} op=C beta=0 (the whole workload each call), "
+        f"{warmup} warm-up + {len(times)} timed calls, mean {ms:.0f} ms, "
+        f"OPENBLAS_NUM_THREADS={os.environ.get('OPENBLAS_NUM_THREADS')}, "
+        f"OPENBLAS_CORETYPE={os.environ.get('OPENBLAS_CORETYPE')}, cpu={cpu_model()}"),
+        call_ms={"min": min(times) * 1e3, "median": statistics.median(times) * 1e3,
+                 "max": max(times) * 1e3},
+        host={"cpus_usable": cores, "cpus_online": os.cpu_count(), "cgroup_cpu_max": quota,
+              "loadavg_before": load_before, "loadavg_after": host_load()})
+    return flops / (ms / 1e3) / 1e12, ms, info
 
 
 # ---------------------------------------------------------------------------
@@ -661,12 +732,14 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        value, info = cpu_reference_run(args.steps, 1)
-        line = {"metric": "ZGEMM-SSB TFLOP/s (reference CPU path)", "value": value,
-                "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": 1,
-                "higher_is_better": True, "impl": "reference", "dtype": "complex128",
-                "data": "synthetic", "config": {"workload": "pzgemm_ssb m=n=1024 k=250000 op=C",
-                                                "sample": info["sample"]},
+        value, ms, info = cpu_reference_run(args.steps, args.warmup)
+        line = {"metric": HEADLINE_METRIC, "value": value, "unit": "TFLOP/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "impl": "reference", "dtype": "complex128 (f64)",
+                "data": "synthetic: complex Gaussian / sqrt(k), seeded",
+                "config": {"workload": workload_name(), "path": "reference CPU path (BLAS)",
+                           "sample": info["sample"]},
                 "cpu_baseline": {"value": value, "unit": "TFLOP/s", **info},
                 "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}, "vs_baseline": None}
@@ -708,9 +781,14 @@ def main():
     clocks_by_path = {p: clk.summary(names[p]) for p in results}
     for p in results:
         results[p]["clocks"] = clocks_by_path[p]
+    # accuracy on the whole C against the device double-double reference, which is
+    # itself checked against the CPU Dot2 oracle on three columns
+    R = dd_reference(torch, spla, A, B)
+    dd_check = rel_err_sampled(R, A, B) if rank == 0 and not args.no_cpu else None
     for pname, r in results.items():
         if "dC" in r:
-            r["rel_err_vs_oracle"] = rel_err_sampled(r.pop("dC"), A, B) if rank == 0 else None
+            r["rel_err_vs_oracle"] = rel_err_full(torch, r.pop("dC"), R)
+            r["rel_err_scope"] = "whole C vs the device double-double reference (splab_gemm_dd)"
 
     # headline: Ozaki if it ran and met the accuracy bar (checked on rank 0 and
     # broadcast, so that every rank takes the same steps), else DMMA
@@ -727,12 +805,18 @@ def main():
     clocks = clocks_by_path.get(head)
 
     e2e = None
+    hA = hB = None
     if not args.no_e2e:
-        ms_e2e, _ = e2e_public_api(torch, spla, head_path, A, B, max(1, min(args.steps, 3)), 1)
+        ms_e2e, hC, hA, hB = e2e_public_api(torch, spla, head_path, A, B,
+                                            max(1, min(args.steps, 3)), 1)
         ms_e2e = max_over_ranks(torch, ms_e2e, device)
         e2e = {"value": whole_job_tflops(FLOPS, world, ms_e2e), "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(16 * K * (M + N)), "d2h_bytes_per_step": int(16 * M * N),
-               "ms_per_step": ms_e2e, "operands": "pinned host memory, streamed in k-chunks"}
+               "ms_per_step": ms_e2e, "operands": "pinned host memory, streamed in k-chunks",
+               "rel_err_vs_oracle": rel_err_full(torch, hC, R),
+               "rel_err_scope": "whole C of the last timed call vs the device double-double "
+                                "reference"}
+    del R
 
     if rank != 0:
         torch.distributed.destroy_process_group() if world > 1 else None
@@ -780,17 +864,22 @@ def main():
 
     cpu = None
     if not args.no_cpu and world >= 1:
-        v, info = cpu_reference_run(3, 1)
-        cpu = {"value": v, "unit": "TFLOP/s", **info}
+        # the reference's CPU path on the same workload: 1 warm-up + 3 full calls
+        # (about 10 s on 16 host cores), on the pinned host copies of A and B
+        v, ms_cpu, info = cpu_reference_run(
+            3, 1, None if hA is None else hA.numpy().ravel(),
+            None if hB is None else hB.numpy().ravel())
+        cpu = {"value": v, "unit": "TFLOP/s", "ms_per_call": ms_cpu, **info}
+    if dd_check is not None:
+        hr["dd_reference_vs_cpu_dot2_3cols"] = dd_check
 
     line = {
-        "metric": "ZGEMM-SSB TFLOP/s: Ozaki-INT8 vs FP64-DMMA at <=1e-14 rel err, 1 B200",
+        "metric": HEADLINE_METRIC,
         "value": hr["tflops"], "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": warmup, "ms_per_step": hr["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)",
         "data": "synthetic: complex Gaussian / sqrt(k), seeded",
-        "config": {"workload": f"pzgemm_ssb C=A^H B complex double m=n={M} k={K}, 1x1 grid "
-                               "128x128 blocks, beta=0", "path": head,
+        "config": {"workload": workload_name(), "path": head,
                    "l2": "inputs (8.2 GB) larger than L2, no flush",
                    "parallelism": f"replicas x{world}"},
         "paths": {k: {kk: vv for kk, vv in v.items()} for k, v in results.items()},

@@ -104,15 +104,18 @@ SPLAB_API int splab_gemm_check(int dtype, int path, int opA, int opB, int64_t m,
  * cap, and latency-critical loops that cannot take the device synchronisation
  * of cudaMalloc / cudaFree. It allocates nothing: the split-K partials live
  * in one static device array of SPLAB_NOALLOC_SCRATCH_BYTES (64 MiB) that
- * every GPU loading the library holds until exit. Problems with
- * m * n * e > 32 MiB (e = 16 bytes for complex, 8 for real dtypes: one FP64
- * partial of C; two must fit) are rejected with SPLAB_ERR_WORKSPACE; the
- * others use fewer k-splits than splab_gemm when the partials would not fit.
- * The first call on a device looks up the array's device address (with that
- * device current); make that first call before any stream capture. All calls
- * share the array: calls that overlap on the GPU race and must be serialised
- * by the caller. Inputs and outputs are passed by the caller as for
- * splab_gemm; alpha/beta are host pointers.
+ * every GPU loading the library holds until exit. A problem that splab_gemm
+ * would run with one k-split (small k, or k = 0) needs no partials and runs at
+ * any size. One that splab_gemm splits along k needs one FP64 partial of C
+ * per split, m * n * e bytes (e = 16 for complex, 8 for real dtypes): it runs
+ * with as many splits as fit in the array (fewer than splab_gemm when needed)
+ * and is rejected with SPLAB_ERR_WORKSPACE when not even two fit
+ * (m * n * e > 32 MiB). The first call on a device, and the first after a
+ * device reset, looks up the array's device address (with that device
+ * current); make that first call before any stream capture. All calls share
+ * the array: calls that overlap on the GPU race and must be serialised by the
+ * caller. Inputs and outputs are passed by the caller as for splab_gemm;
+ * alpha/beta are host pointers.
  */
 #define SPLAB_NOALLOC_SCRATCH_BYTES (64u << 20)
 SPLAB_API int splab_gemm_dmma_noalloc(int dtype, int opA, int opB, int64_t m, int64_t n, int64_t k,
@@ -191,6 +194,20 @@ SPLAB_API int splab_block_cyclic_info(int64_t rowsInBlock, int64_t colsInBlock, 
                             int64_t gridCols, int64_t globalRows, int64_t globalCols,
                             int64_t rowOffset, int64_t colOffset, const int64_t *blockIdx,
                             int64_t count, int64_t *out, void *stream);
+
+/*
+ * Double-double reference product for verification (no reference counterpart;
+ * it is the device form of the compensated CPU oracle and sits on no
+ * contraction path): R = op(A) * op(B) with every product split exactly
+ * (TwoProduct) and summed with TwoSum (Ogita-Rump-Oishi Dot2), as accurate as
+ * a dot product in twice the working precision. A and B of any dtype (read
+ * as double); Rhi and, when non-null, Rlo are DEVICE double buffers (complex:
+ * interleaved re, im) with leading dimension ldr in elements. Asynchronous
+ * on `stream`. Lets results be checked on the whole C at full problem sizes.
+ */
+SPLAB_API int splab_gemm_dd(int dtype, int opA, int opB, int64_t m, int64_t n, int64_t k,
+                            const void *A, int64_t lda, const void *B, int64_t ldb, double *Rhi,
+                            double *Rlo, int64_t ldr, void *stream);
 
 /*
  * Phase timing for measurement harnesses (no reference counterpart). When

@@ -373,6 +373,19 @@ def splab_gemm(dtype, path, opA, opB, m, n, k, alpha, A, lda, B, ldb, beta, C, l
                             ro, co, moduli, _addr(workspace)[0], workspace_bytes, stream)
 
 
+def gemm_dd(dtype, opA, opB, m, n, k, A, lda, B, ldb, R_hi, ldr, R_lo=None, stream=0):
+    """Double-double reference product R = op(A) op(B) on the device
+    (splab_gemm_dd; verification only). R_hi / R_lo: device float64 (real) or
+    complex128 (complex) buffers. Returns the status code."""
+    L = lib()
+    L.splab_gemm_dd.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_int64, ct.c_int64, ct.c_int64,
+                                ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_int64, ct.c_void_p,
+                                ct.c_void_p, ct.c_int64, ct.c_void_p]
+    L.splab_gemm_dd.restype = ct.c_int
+    return L.splab_gemm_dd(_dtype_of(dtype=dtype), opA, opB, m, n, k, _addr(A)[0], lda,
+                           _addr(B)[0], ldb, _addr(R_hi)[0], _addr(R_lo)[0], ldr, stream)
+
+
 def splab_gemm_workspace_size(dtype, path, opA, opB, m, n, k, moduli=0):
     return lib().splab_gemm_workspace_size(_dtype_of(dtype=dtype), path, opA, opB, m, n, k,
                                            moduli)

@@ -100,9 +100,14 @@ ContextInternal::ContextInternal(SplaProcessingUnit pu)
   const cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count < 1) {
     cudaGetLastError();
-    throw GPUNoDeviceError();
+    // A host context is created without touching a device, as the
+    // reference's (context_internal.hpp:58-73: device id 0); its
+    // contractions, which run on the GPU here, report the missing device.
+    if (pu != SPLA_PU_HOST) throw GPUNoDeviceError();
+  } else {
+    check_cuda(cudaGetDevice(&deviceId_));
+    hasDevice_ = true;
   }
-  check_cuda(cudaGetDevice(&deviceId_));
   fp64Path_ = path_from_env();
   if (const char* v = std::getenv("SPLA_B200_OZAKI_MODULI")) {
     const int m = std::atoi(v);  // valid: 8 .. 16; anything else keeps the default
@@ -126,6 +131,7 @@ ContextInternal::ContextInternal(SplaProcessingUnit pu)
 }
 
 ContextInternal::~ContextInternal() {
+  if (!hasDevice_) return;  // nothing was allocated or created on a device
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(deviceId_);

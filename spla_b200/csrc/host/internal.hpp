@@ -110,6 +110,7 @@ private:
   int tileSizeGPU_ = 2048;
   int opThresholdGPU_ = 2000000;
   int deviceId_ = 0;
+  bool hasDevice_ = false;  // a device was present at construction
   int fp64Path_ = 0;
   int ozakiModuli_ = 0;
   std::unique_ptr<ScratchPool> host_, pinned_, device_;

@@ -22,6 +22,8 @@
 // Fill mode: tiles of C that do not intersect the requested triangle are
 // skipped (C left unchanged), with the reference's block predicate
 // (src/block_generation/block.hpp:58-66) applied per tile.
+#include <cuda.h>
+
 #include <algorithm>
 #include <climits>
 #include <mutex>
@@ -567,8 +569,8 @@ cudaError_t reduce_partials(const GemmProblem& pr, const void* P, int splits, in
 //
 // The array's host-side symbol is only a stand-in: its device address is
 // looked up with cudaGetSymbolAddress, once per device, by the first call on
-// that device (with that device current). Make that first call before any
-// stream capture. All calls share the array and it keeps the last call's
+// that device (with that device current), and again after a device reset
+// (a new context). Make that first call before any stream capture. All calls share the array and it keeps the last call's
 // contents; nothing in it has to start at zero (every split overwrites its
 // partial tile before the reduction reads it). Calls whose execution overlaps
 // on the GPU (different streams, or different host threads) race on the
@@ -578,35 +580,76 @@ static __device__ __align__(256) unsigned char noalloc_scratch[SPLAB_NOALLOC_SCR
 
 namespace {
 std::mutex noalloc_mutex;
-void* noalloc_ptr[64] = {nullptr};
+struct NoallocSlot {
+  unsigned long long context_id = 0;  // the CUDA context the address belongs to
+  void* ptr = nullptr;
+};
+NoallocSlot noalloc_slot[64];
 
+// Unique id of the calling thread's current CUDA context, 0 when it cannot be
+// read. A device reset (cudaDeviceReset) destroys the context and the module
+// with the array; the next context loads the module anew and the array may
+// sit at another address, so the address is cached per device AND context.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+    cudaGetLastError();
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext c = nullptr;
+  if (get_current(&c) != CUDA_SUCCESS || c == nullptr) return 0;
+  unsigned long long id = 0;
+  return get_id(c, &id) == CUDA_SUCCESS ? id : 0;
+}
+
+// Device address of noalloc_scratch on the current device, looked up once per
+// device and context (with that device current); the lookup allocates nothing.
 cudaError_t noalloc_scratch_address(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(noalloc_mutex);
-  if (!noalloc_ptr[dev]) {
+  NoallocSlot& slot = noalloc_slot[dev];
+  const unsigned long long id = current_context_id();
+  if (slot.ptr == nullptr || id == 0 || id != slot.context_id) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, noalloc_scratch);
     if (e != cudaSuccess) return e;
-    noalloc_ptr[dev] = p;
+    slot.ptr = p;
+    slot.context_id = current_context_id();  // the lookup made the context current
   }
-  *out = noalloc_ptr[dev];
+  *out = slot.ptr;
   return cudaSuccess;
 }
 }  // namespace
 
 int dmma_gemm_noalloc(const GemmProblem& pr, int num_sms, cudaStream_t st) {
   if (pr.m <= 0 || pr.n <= 0) return 0;
-  // one k-split's partials are m * n FP64 (complex: pairs); two must fit
+  // The planner's split count first: a plan with one k-split (small k, or
+  // k = 0) needs no partials and runs at any size. Otherwise one split's
+  // partials are m * n FP64 (complex: pairs); with fewer splits than the
+  // planner chose they are made to fit the static array, and problems where
+  // not even two fit are refused.
   const size_t per_split = size_t(pr.m) * size_t(pr.n) * (dtype_is_complex(pr.dtype) ? 16 : 8);
-  if (2 * per_split > SPLAB_NOALLOC_SCRATCH_BYTES) return 2;
   DmmaPlan plan = dmma_plan(pr, num_sms);
   if (plan.workspace_bytes > SPLAB_NOALLOC_SCRATCH_BYTES) {
-    // fewer k-splits so that the partials fit the static array
-    const int fit = int(size_t(SPLAB_NOALLOC_SCRATCH_BYTES) / per_split);
-    plan = dmma_plan(pr, num_sms, fit);
+    const size_t fit = size_t(SPLAB_NOALLOC_SCRATCH_BYTES) / per_split;
+    if (fit < 2) return 2;
+    plan = dmma_plan(pr, num_sms, int(std::min<size_t>(fit, 4096)));
     if (plan.workspace_bytes > SPLAB_NOALLOC_SCRATCH_BYTES) return 2;
   }
   void* scratch = nullptr;

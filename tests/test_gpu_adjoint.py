@@ -14,6 +14,11 @@ Checks:
     loss (see _fd_check); the plain two-evaluation difference, whose accuracy
     at h = 1e-6 is bounded by the FP64 rounding of the forwards, agrees to
     <= 2e-3;
+  * the plain two-evaluation difference over a range of h (1e-6 ... 1e-2):
+    for this quadratic loss the central difference has no truncation error,
+    so its discrepancy is rounding alone and falls as 1/h, reaching <= 1e-6
+    at h >= 1e-3 (the measured table is printed and written to
+    fd_vs_h.json in the pytest temporary directory);
   * the Ozaki path's gradient equals the FP64 DMMA path's.
 """
 import math
@@ -126,6 +131,39 @@ def test_finite_differences(setup, which):
     stable, raw = _fd_check(torch, spla, A, B, ctx, which, gA, gB)
     assert stable <= 1e-6, stable
     assert raw <= 2e-3, raw
+
+
+def test_plain_central_difference_vs_h(setup, tmp_path):
+    """(L(X + hV) - L(X - hV)) / 2 with two forwards only, against Re<grad, dX>,
+    for h from 1e-6 to 1e-2 on 8 random unit directions of A: the worst
+    relative discrepancy times h stays about constant (rounding of the
+    forwards, no truncation term), and the plain form meets 1e-6 once h is
+    large enough for the rounding to be below it."""
+    import json
+    torch, spla, A, B, ctx = setup
+    from spla_b200.autograd import ssb
+    gA, _ = grads(torch, spla, A, B, ctx)
+    rng = np.random.default_rng(19)
+    dirs = []
+    for _ in range(8):
+        V = torch.from_numpy(rng.standard_normal(A.shape) + 1j * rng.standard_normal(A.shape)).to(
+            A.device)
+        dirs.append(V / V.norm())
+    table = {}
+    for h in (1e-6, 1e-5, 1e-4, 1e-3, 1e-2):
+        worst = 0.0
+        for V in dirs:
+            Xp, Xm = A + h * V, A - h * V
+            an = float((gA.conj() * (Xp - Xm)).sum().real)
+            raw = loss_exact(ssb(Xp, B, ctx)) - loss_exact(ssb(Xm, B, ctx))
+            worst = max(worst, abs(raw - an) / abs(an))
+        table[h] = worst
+    print("plain central difference, worst relative discrepancy by h:", table)
+    (tmp_path / "fd_vs_h.json").write_text(json.dumps({str(h): v for h, v in table.items()}))
+    assert table[1e-6] <= 2e-3
+    assert table[1e-3] <= 1e-6 and table[1e-2] <= 1e-6, table
+    # rounding-limited: the discrepancy falls with h (within a factor for noise)
+    assert table[1e-2] < table[1e-6] / 100, table
 
 
 def test_ozaki_forward_gradient_matches_dmma(setup):

@@ -6,7 +6,12 @@ Checks per case: computed elements within tolerance of the reference's result
 block bit-unchanged (exact C layout, ldc padding untouched), and for
 pgemm_ssbtr every element either the reference's value or unchanged.
 Operands are passed as device pointers and, for a subset, as host pointers
-(the streamed path)."""
+(the streamed path). Every case runs on the automatic path choice and with
+each contraction path forced (FP64 DMMA, Ozaki INT8, 3xTF32), so the
+reference's own outputs pin the tensor-core paths directly; a forced path
+that does not support a case (3xTF32 on double dtypes) runs DMMA, and each
+test checks that the forced path took some of its cases."""
+import ctypes as ct
 import json
 
 import numpy as np
@@ -23,11 +28,36 @@ def ours(spla_lib):
     return SplaCAPI(spla_lib.LIB_PATH)
 
 
-@pytest.fixture(scope="module")
-def ctx(ours):
+PATHS = {0: "auto", 1: "dmma", 2: "ozaki", 3: "tf32x3"}
+
+
+@pytest.fixture(scope="module", params=list(PATHS), ids=list(PATHS.values()))
+def ctx(ours, request):
     h = ours.ctx(1)
+    ours.lib.spla_b200_ctx_set_fp64_path.argtypes = [ct.c_void_p, ct.c_int, ct.c_int]
+    assert ours.lib.spla_b200_ctx_set_fp64_path(h, request.param, 0) == 0
+    h.path = request.param
     yield h
     ours.destroy_ctx(h)
+
+
+class PathCount:
+    """How many cases the forced path itself computed (splab_gemm_path)."""
+
+    def __init__(self, lib, ctx):
+        self.lib, self.path, self.taken, self.total = lib, ctx.path, 0, 0
+        lib.splab_gemm_path.argtypes = [ct.c_int] * 4 + [ct.c_int64] * 3
+        lib.splab_gemm_path.restype = ct.c_int
+
+    def add(self, dt, opA, opB, m, n, k):
+        self.total += 1
+        code = {np.float32: 0, np.float64: 1, np.complex64: 2, np.complex128: 3}[dt]
+        if self.path and self.lib.splab_gemm_path(code, self.path, opA, opB, m, n, k) == self.path:
+            self.taken += 1
+
+    def check(self, expect_taken=True):
+        if self.path in (2, 3) and expect_taken:
+            assert self.taken > 0, f"path {self.path} took none of {self.total} cases"
 
 
 def dev(x):
@@ -73,8 +103,10 @@ def check_case(name, c, dt, A, B, C0, Cout, mask_fn=None):
 def test_gemm_grid(ours, ctx, use_host):
     cases, _ = gc.load("gemm")
     sel = cases if not use_host else cases[::5]
+    count = PathCount(ours.lib, ctx)
     for c in sel:
         dt, A, B, C = gc.gemm_inputs(c)
+        count.add(dt, c["opA"], c["opB"], c["m"], c["n"], c["k"])
         C0 = C.copy()
         if use_host:
             rc = ours.gemm(dt, c["opA"], c["opB"], c["m"], c["n"], c["k"], c["alpha"], A, c["lda"],
@@ -88,6 +120,7 @@ def test_gemm_grid(ours, ctx, use_host):
         assert rc == 0, (c, rc)
         check_case("gemm", c, dt, A, B, C0, out,
                    mask_fn=lambda idx, c=c: (_block_mask(c, idx), _block_mask(c, idx)))
+    count.check()
 
 
 def _block_mask(c, idx):
@@ -100,8 +133,10 @@ def _block_mask(c, idx):
 def test_ssb_and_ssbtr(ours, ctx, use_host):
     cases, _ = gc.load("ssb")
     sel = cases if not use_host else cases[::4]
+    count = PathCount(ours.lib, ctx)
     for c in sel:
         dt, A, B, C = gc.ssb_inputs(c)
+        count.add(dt, c["opA"], 0, c["m"], c["n"], c["k"])
         C0 = C.copy()
         rcd, dist = ours.block_cyclic(1, 1, 64, 64)
         alpha, beta = gc.scalar(c["alpha"], dt), gc.scalar(c["beta"], dt)
@@ -123,14 +158,17 @@ def test_ssb_and_ssbtr(ours, ctx, use_host):
             return inside, gc.fill_mask(c, idx)
 
         check_case("ssb", c, dt, A, B, C0, out, mask_fn=masks)
+    count.check()
 
 
 @pytest.mark.parametrize("use_host", [False, True])
 def test_sbs(ours, ctx, use_host):
     cases, _ = gc.load("sbs")
     sel = cases if not use_host else cases[::3]
+    count = PathCount(ours.lib, ctx)
     for c in sel:
         dt, A, B, C = gc.sbs_inputs(c)
+        count.add(dt, 0, 0, c["mloc"], c["n"], c["k"])
         C0 = C.copy()
         rcd, dist = ours.block_cyclic(1, 1, 128, 128)
         alpha, beta = gc.scalar(c["alpha"], dt), gc.scalar(c["beta"], dt)
@@ -151,6 +189,7 @@ def test_sbs(ours, ctx, use_host):
             return inside, inside
 
         check_case("sbs", c, dt, A, B, C0, out, mask_fn=masks)
+    count.check(expect_taken=ctx.path == 2)  # 3xTF32 takes op(A) in {T, C} only
 
 
 def test_error_codes(ours, ctx):
