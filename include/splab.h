@@ -38,13 +38,14 @@ extern "C" {
 /* Compute paths for the contraction. */
 #define SPLAB_PATH_AUTO 0  /* the supported path with the least modelled time */
 #define SPLAB_PATH_DMMA 1  /* FP64 tensor cores (mma.sync f64); float inputs accumulate in FP64 */
-#define SPLAB_PATH_OZAKI 2 /* Ozaki scheme II on INT8 tcgen05 (all four dtypes) with
-                              op(B) = N and any op(A) (op(A) = N: A is first copied
-                              k-major into the workspace); other problems use DMMA */
+#define SPLAB_PATH_OZAKI 2 /* Ozaki scheme II on INT8 tcgen05 (all four dtypes), any
+                              op pair: op(A) = N and op(B) in {T, C} are first copied
+                              k-major into the workspace (conjugated for C) */
 #define SPLAB_PATH_TF32X3 3 /* float / complex float: each input split into two TF32
                                parts, three TF32 tcgen05 products, FP32 accumulation
-                               drained to FP64 every 1024 reals; op(A) in {T, C},
-                               op(B) = N; other problems use DMMA */
+                               in 64-real windows folded into double-float sums; any
+                               op pair (k-major copies as for Ozaki); double dtypes
+                               use DMMA */
 
 #define SPLAB_OK 0
 #define SPLAB_ERR_INVALID 1     /* bad argument (sizes, leading dimensions, dtype, path) */

@@ -458,6 +458,322 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
 }
 
 // --------------------------------------------------------------------------
+// 2b. residues of complex double rows with the digit sums on the tensor cores
+//
+// The digit sums above are a small integer matrix product. Written in
+// balanced base-256 digits, x = sum_j d_j 256^j with d_j in [-128, 127]
+// (eight digits cover |x| < 2^62), the residue of x mod p is that of
+// sum_j d_j w_j with w_j = 256^j mod p in symmetric form (|w_j| <= 127). A
+// complex element has 16 digits (8 of re, 8 of im), and its three planes are
+// three such sums: re uses w on the re digits, im w on the im digits, the
+// sum plane w on re and s_sum w on im. One tcgen05.mma kind::i8 (exact INT32)
+//   D[128 x 256] = W[128 x K] . Dig[K x 256]
+// computes them for G groups of 256 elements at once: the 16 digit bytes of
+// group g's element n are K bytes 16 g .. 16 g + 15 of B row n, and row
+// (g, t, q) of W holds the weights of modulus t and plane q on group g's
+// bytes; (nmod - 1) * 3 * G <= 128 rows (G = 3 for the default 15 moduli:
+// 126 rows, two K-steps of 32 bytes). The modulus 256 is the low byte of x and
+// is written by the producers directly. The epilogue reduces each sum
+// (|s| < 16 * 128 * 127 < 2^18) mod p on the FP32 pipe with 4 operations
+// per residue (against 7 for the digit-sum form plus 3 for the sum plane),
+// stages the bytes of its 256-element row segment in shared memory and writes
+// it with one bulk copy.
+//
+// Warps 0-3: epilogue (warp w reads TMEM lanes 32 w .. 32 w + 31, one
+// (group, modulus, plane) row each); warps 4-7: producers (row scaling,
+// digits into the 128-byte-swizzled B tile, modulus-256 bytes); warp 8: TMEM
+// allocation and the MMA issue. Digits and accumulators are double-buffered;
+// every wait is bounded and a give-up sets *status.
+struct SliceTcParams {
+  const double* X;        // rows of interleaved complex doubles
+  int64_t ld;             // row stride in doubles
+  int64_t len;            // complex elements per row
+  int rows;
+  int64_t kp;             // residue row length (complex elements, multiple of 128)
+  const int* sigma;       // row scale exponents
+  int s_sum;              // sign of im in the third plane
+  int8_t* res;            // res[t][q][row][e]
+  int64_t mod_stride;     // bytes between moduli
+  int64_t plane;          // bytes between the planes of one modulus
+  int nmod;               // moduli, p[0] = 256
+  int groups;             // groups of 256 elements per unit
+  int ksteps;             // K-steps of 32 bytes per unit
+  int units_per_row;
+  long long total_units;
+  int p[kMaxModuli];
+  int* status;
+  unsigned long long wait_limit_ns;
+};
+
+constexpr int TC_THREADS = 288;
+constexpr int TC_W_BYTES = 128 * 128;            // weights: 128 rows x 128 B (SW128)
+constexpr int TC_D_BYTES = 256 * 128;            // digits: 256 rows x 128 B (SW128)
+constexpr int TC_ROW_STAGE = 256 + 16;           // one staged row segment (padded)
+constexpr int TC_S_BYTES = 128 * TC_ROW_STAGE;   // staging of the 128 epilogue rows
+constexpr int TC_SMEM = TC_W_BYTES + 2 * TC_D_BYTES + 2 * TC_S_BYTES + 256 + 1024;
+
+__device__ __forceinline__ int sw128_chunk(int row, int chunk) {
+  return (row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4);
+}
+
+// round(y) as a 64-bit integer for |y| < 2^62, without conversion
+// instructions: y = xh 2^30 + xl_d, both parts read from the bits of
+// (value + 1.5 2^52).
+__device__ __forceinline__ long long round_to_int64(double y) {
+  constexpr double kM52 = 6755399441055744.0;  // 1.5 * 2^52: ulp 1
+  constexpr long long kM52Bits = 0x4338000000000000ll;
+  const double t = fma(y, 1.0 / 1073741824.0, kM52);   // kM52 + round(y 2^-30)
+  const double xl_d = fma(t - kM52, -1073741824.0, y);  // exact, |xl_d| <= 2^29
+  const long long xh = __double_as_longlong(t) - kM52Bits;
+  const int xl = int(__double2loint(xl_d + kM52));
+  return xh * 1073741824ll + xl;
+}
+
+// Balanced base-256 digits of x as bytes: d_j = byte_j(x + 0x0080..80) - 128
+// for j < 7 (the XOR flips the offset back), d_7 the signed top byte.
+__device__ __forceinline__ unsigned long long balanced_digits(long long x) {
+  constexpr unsigned long long kOff = 0x0080808080808080ull;
+  return (static_cast<unsigned long long>(x) + kOff) ^ kOff;
+}
+
+__device__ __forceinline__ void bulk_store(void* gdst, uint32_t ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst),
+               "r"(ssrc), "r"(bytes)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) oz_slice_tc(const __grid_constant__ SliceTcParams P) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw_addr = smem_u32(smem_raw);
+  const uint32_t base = (raw_addr + 1023u) & ~1023u;
+  unsigned char* bp = smem_raw + (base - raw_addr);
+  unsigned char* Wt = bp;
+  unsigned char* Dg = bp + TC_W_BYTES;
+  unsigned char* St = Dg + 2 * TC_D_BYTES;
+  const uint32_t w_addr = base, d_addr = base + TC_W_BYTES, s_addr = d_addr + 2 * TC_D_BYTES;
+  const uint32_t bar_base = s_addr + 2 * TC_S_BYTES;
+  auto dfull = [&](int b) { return bar_base + 8u * b; };
+  auto dempty = [&](int b) { return bar_base + 8u * (2 + b); };
+  auto accf = [&](int b) { return bar_base + 8u * (4 + b); };
+  auto acce = [&](int b) { return bar_base + 8u * (6 + b); };
+  const uint32_t drain_bar = bar_base + 64;
+  unsigned char* tail = St + 2 * TC_S_BYTES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tail + 128);
+  volatile int* abort = reinterpret_cast<volatile int*>(tail + 136);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int R3 = 3 * (P.nmod - 1);
+  const int wrows = P.groups * R3;
+
+  // weights: row L = (group g, modulus t >= 1, plane q), K byte k
+  for (int i = threadIdx.x; i < 128 * 128; i += blockDim.x) {
+    const int L = i >> 7, k = i & 127;
+    int w = 0;
+    if (L < wrows) {
+      const int g = L / R3, j = L - g * R3, t = 1 + j / 3, q = j - 3 * (j / 3);
+      const int kg = k - 16 * g;
+      if (kg >= 0 && kg < 16) {
+        const int part = kg >> 3, dj = kg & 7;  // part 0: re digits, 1: im digits
+        const int pt = P.p[t];
+        int c = 1;
+        for (int s = 0; s < dj; ++s) c = (c * 256) % pt;
+        if (c > pt / 2) c -= pt;
+        if (q == 0) w = part == 0 ? c : 0;
+        else if (q == 1) w = part == 1 ? c : 0;
+        else w = part == 0 ? c : P.s_sum * c;
+      }
+    }
+    Wt[sw128_chunk(L, k >> 4) + (k & 15)] = static_cast<unsigned char>(static_cast<signed char>(w));
+  }
+  // digit tiles start at zero: the bytes beyond the groups are read by the
+  // last K-step (against zero weights) and never written
+  for (int i = threadIdx.x; i < 2 * TC_D_BYTES / 16; i += blockDim.x)
+    reinterpret_cast<uint4*>(Dg)[i] = make_uint4(0u, 0u, 0u, 0u);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(dfull(b), 128);
+      mbar_init(dempty(b), 1);
+      mbar_init(accf(b), 1);
+      mbar_init(acce(b), 128);
+    }
+    mbar_init(drain_bar, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 8) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                     smem_u32(tmem_slot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const int unit_elems = 256 * P.groups;
+
+  if (warp >= 4 && warp < 8) {
+    // ---- producers: 2 G elements per thread and unit, consecutive threads
+    // on consecutive elements (coalesced 16-byte loads)
+    const int pt = threadIdx.x - 128;
+    const int per = 2 * P.groups;
+    // the elements of unit u, loaded one unit ahead of their use
+    auto load = [&](long long u, double2 (&v)[8]) {
+      const int row = int(u / P.units_per_row);
+      const int64_t e0 = (u - int64_t(row) * P.units_per_row) * unit_elems;
+      const double2* xr = reinterpret_cast<const double2*>(P.X + int64_t(row) * P.ld);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        if (r < per) {
+          const int64_t e = e0 + pt + 128 * r;
+          v[r] = e < P.len ? __ldcs(xr + e) : make_double2(0.0, 0.0);
+        }
+      }
+    };
+    double2 v[8], vn[8];
+    if (blockIdx.x < P.total_units) load(blockIdx.x, vn);
+    for (long long u = blockIdx.x, it = 0; u < P.total_units; u += gridDim.x, ++it) {
+      const int b = int(it & 1);
+      const uint32_t par = uint32_t((it >> 1) & 1);
+      const int row = int(u / P.units_per_row);
+      const int64_t e0 = (u - int64_t(row) * P.units_per_row) * unit_elems;
+      const int sg = P.sigma[row];
+      const bool direct = sg > -1000 && sg < 1000;
+      const double scale = direct ? __longlong_as_double((long long)(sg + 1023) << 52) : 1.0;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) v[r] = vn[r];
+      if (u + gridDim.x < P.total_units) load(u + gridDim.x, vn);
+      if (!mbar_wait(dempty(b), par ^ 1u, abort, P.wait_limit_ns)) break;
+      unsigned char* dg = Dg + b * TC_D_BYTES;
+      int8_t* r256 = P.res + int64_t(row) * P.kp;  // modulus 0 (256), plane 0
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        if (r < per) {
+          const int el = pt + 128 * r;
+          const int64_t e = e0 + el;
+          const double yr = direct ? v[r].x * scale : ldexp(v[r].x, sg);
+          const double yi = direct ? v[r].y * scale : ldexp(v[r].y, sg);
+          const long long x_re = round_to_int64(yr), x_im = round_to_int64(yi);
+          const unsigned long long dr = balanced_digits(x_re), di = balanced_digits(x_im);
+          *reinterpret_cast<uint4*>(dg + sw128_chunk(el & 255, el >> 8)) =
+              make_uint4(unsigned(dr), unsigned(dr >> 32), unsigned(di), unsigned(di >> 32));
+          if (e < P.kp) {
+            r256[e] = static_cast<int8_t>(x_re);
+            r256[P.plane + e] = static_cast<int8_t>(x_im);
+            r256[2 * P.plane + e] = static_cast<int8_t>(x_re + P.s_sum * x_im);
+          }
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(dfull(b));
+    }
+  } else if (warp == 8) {
+    if (lane == 0) {
+      // ---- MMA issuer
+      bool ok = true;
+      for (long long u = blockIdx.x, it = 0; u < P.total_units; u += gridDim.x, ++it) {
+        const int b = int(it & 1);
+        const uint32_t par = uint32_t((it >> 1) & 1);
+        if (!mbar_wait(dfull(b), par, abort, P.wait_limit_ns) ||
+            !mbar_wait(acce(b), par ^ 1u, abort, P.wait_limit_ns)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + uint32_t(b * 256);
+        for (int kk = 0; kk < P.ksteps; ++kk)
+          umma_i8(d, umma_desc_sw128(w_addr + kk * 32),
+                  umma_desc_sw128(d_addr + b * TC_D_BYTES + kk * 32), kk > 0 ? 1u : 0u);
+        umma_commit(dempty(b));
+        umma_commit(accf(b));
+      }
+      if (!ok) {
+        umma_commit(drain_bar);  // MMAs may be in flight: wait (bounded) until they retire
+        const unsigned long long t0 = globaltimer();
+        while (!mbar_try_wait(drain_bar, 0) && globaltimer() - t0 < 1000000ull) {
+        }
+      }
+    }
+  } else if (warp < 4) {
+    // ---- epilogue: TMEM lane L = (group, modulus, plane) row
+    const int L = warp * 32 + lane;
+    const bool active = L < wrows;
+    int g = 0, t = 1, q = 0;
+    if (active) {
+      g = L / R3;
+      const int j = L - g * R3;
+      t = 1 + j / 3;
+      q = j - 3 * (j / 3);
+    }
+    const float pf = float(P.p[t]);
+    const unsigned long long NP2 = f2_pack(-pf, -pf);
+    const unsigned long long IP2 = f2_pack(1.0f / pf, 1.0f / pf);
+    const unsigned long long M2 = f2_pack(kMagic, kMagic), NM2 = f2_pack(-kMagic, -kMagic);
+    const uint32_t row_stage = uint32_t(L) * TC_ROW_STAGE;
+    for (long long u = blockIdx.x, it = 0; u < P.total_units; u += gridDim.x, ++it) {
+      const int b = int(it & 1);
+      const uint32_t par = uint32_t((it >> 1) & 1);
+      if (!mbar_wait(accf(b), par, abort, P.wait_limit_ns)) break;
+      tc_fence_after();
+      // the staging slot of this unit was last read by the bulk copy of unit it - 2
+      if (active) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+      unsigned char* st = St + b * TC_S_BYTES + row_stage;
+#pragma unroll 1
+      for (int c0 = 0; c0 < 256; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32(tmem_base + (uint32_t(warp * 32) << 16) + uint32_t(b * 256 + c0), v);
+        if (active) {
+          uint32_t wv[8];
+#pragma unroll
+          for (int h = 0; h < 8; ++h) {
+            float r[4];
+#pragma unroll
+            for (int e2 = 0; e2 < 2; ++e2) {
+              const int c = 4 * h + 2 * e2;
+              // MAGIC + s exactly (|s| < 2^22), s, its nearest quotient by p,
+              // MAGIC + s - q p = MAGIC + (s mod p)
+              const unsigned long long tM = f2_pack(__int_as_float(0x4B400000 + int(v[c])),
+                                                    __int_as_float(0x4B400000 + int(v[c + 1])));
+              const unsigned long long t2 = f2_add(tM, NM2);
+              const unsigned long long q2 = f2_add(f2_fma(t2, IP2, M2), NM2);
+              f2_unpack(f2_fma(q2, NP2, tM), r[2 * e2], r[2 * e2 + 1]);
+            }
+            wv[h] = pack4(r[0], r[1], r[2], r[3]);
+          }
+          *reinterpret_cast<uint4*>(st + c0) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+          *reinterpret_cast<uint4*>(st + c0 + 16) = make_uint4(wv[4], wv[5], wv[6], wv[7]);
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(acce(b));
+      if (active) {
+        const int row = int(u / P.units_per_row);
+        const int64_t e = (u - int64_t(row) * P.units_per_row) * unit_elems + 256 * g;
+        const int64_t n = P.kp - e < 256 ? P.kp - e : 256;  // a multiple of 128, or <= 0
+        if (n > 0) {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          bulk_store(P.res + t * P.mod_stride + q * P.plane + int64_t(row) * P.kp + e,
+                     s_addr + uint32_t(b * TC_S_BYTES) + row_stage, uint32_t(n));
+        }
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+      }
+    }
+    if (active) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (*abort && threadIdx.x == 0) atomicExch(P.status, 1);
+  if (warp == 8) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base)
+                 : "memory");
+  }
+}
+
+// --------------------------------------------------------------------------
 // 3. INT8 residue GEMM on tcgen05
 
 struct GemmParams {
@@ -1372,16 +1688,75 @@ void scale_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
                                                L.rowsB, crt.q_bits, sigB);
 }
 
+// Residue slicing of complex double rows with the digit sums on the tensor
+// cores (oz_slice_tc): used for all moduli at once when the modulus 256 comes
+// first and the rows are 16-byte aligned; SPLAB_OZAKI_SLICE_TC=0 selects the
+// FP32 digit-sum slicer instead.
+bool slice_tc_enabled() {  // read per call: tests compare both slicers in one process
+  const char* v = std::getenv("SPLAB_OZAKI_SLICE_TC");
+  return !(v && v[0] == '0');
+}
+
+cudaError_t launch_slice_tc(const double* X, int64_t ld, int64_t len, int rows, int64_t kp,
+                            const int* sig, int s_sum, int8_t* res, int64_t mod_stride,
+                            int64_t plane, const oz::Crt& crt, int nmod, int* status,
+                            cudaStream_t st) {
+  using namespace oz;
+  SliceTcParams P{};
+  P.X = X;
+  P.ld = ld;
+  P.len = len;
+  P.rows = rows;
+  P.kp = kp;
+  P.sigma = sig;
+  P.s_sum = s_sum;
+  P.res = res;
+  P.mod_stride = mod_stride;
+  P.plane = plane;
+  P.nmod = nmod;
+  const int r3 = 3 * (nmod - 1);
+  P.groups = std::min(4, 128 / r3);
+  P.ksteps = (16 * P.groups + 31) / 32;
+  P.units_per_row = int((kp + 256 * P.groups - 1) / (256 * P.groups));
+  P.total_units = (long long)rows * P.units_per_row;
+  for (int t = 0; t < nmod; ++t) P.p[t] = crt.p[t];
+  P.status = status;
+  P.wait_limit_ns = kWaitLimitNs;
+  if (P.total_units <= 0) return cudaSuccess;
+  cudaError_t e = set_dynamic_smem(reinterpret_cast<const void*>(oz_slice_tc), TC_SMEM);
+  if (e != cudaSuccess) return e;
+  const long long grid = std::min<long long>(P.total_units, sm_count());
+  oz_slice_tc<<<unsigned(grid), TC_THREADS, TC_SMEM, st>>>(P);
+  return cudaGetLastError();
+}
+
 // Residues of moduli t0 .. t1-1 of A (which & 1) and B (which & 2).
 template <typename TIn>
 void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
                     const int* sigA, const int* sigB, int8_t* resA, int8_t* resB, int t0, int t1,
-                    int which, cudaStream_t st) {
+                    int which, cudaStream_t st, int* status) {
   using namespace oz;
   const TIn* A = static_cast<const TIn*>(p.A);
   const TIn* B = static_cast<const TIn*>(p.B);
   const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in real elements
   const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
+  if (std::is_same<TIn, double>::value && cplx && t0 == 0 && t1 == L.nmod && crt.p[0] == 256 &&
+      L.nmod >= 2 && slice_tc_enabled()) {
+    const double* Ad = reinterpret_cast<const double*>(A);
+    const double* Bd = reinterpret_cast<const double*>(B);
+    const bool okA = reinterpret_cast<uintptr_t>(Ad) % 16 == 0;
+    const bool okB = reinterpret_cast<uintptr_t>(Bd) % 16 == 0;
+    if ((!(which & 1) || okA) && (!(which & 2) || okB)) {
+      const int64_t planeA = int64_t(L.rowsA) * L.kp, planeB = int64_t(L.nb) * L.kp;
+      if (which & 1)
+        launch_slice_tc(Ad, ldA, p.k, L.rowsA, L.kp, sigA, p.opA == 2 ? -1 : 1, resA,
+                        int64_t(L.nsub) * planeA, planeA, crt, L.nmod, status, st);
+      if (which & 2)
+        launch_slice_tc(Bd, ldB, p.k, L.rowsB, L.kp, sigB, 1, resB, int64_t(L.nsub) * planeB,
+                        planeB, crt, L.nmod, status, st);
+      return;
+    }
+  }
   SliceConsts sc{};
   sc.n = L.nmod;
   sc.p0 = float(crt.p[0]);
@@ -1592,9 +1967,11 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
   } else {
     auto slice = [&](int t0, int t1, int which, cudaStream_t s) {
       if (dbl)
-        slice_operands<double>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, which, s);
+        slice_operands<double>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, which, s,
+                               status);
       else
-        slice_operands<float>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, which, s);
+        slice_operands<float>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, which, s,
+                              status);
     };
     CUtensorMap mapA, mapB;
     if (!make_map(&mapA, resA, L.kp, int64_t(L.nmod) * L.nsub * L.rowsA, BM) ||

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <mutex>
 #include <set>
+#include <type_traits>
 #include <utility>
 
 #include "../../../include/splab.h"
@@ -171,23 +172,154 @@ size_t device_total_memory() {
   return total;
 }
 
+// Operand normalisation for the tensor-core paths, whose kernels contract
+// k-major operands (op(B) = N; on 3xTF32 also op(A) in {T, C}): op(B) in
+// {T, C} is first copied k-major (conjugated for C) into the head of the
+// workspace, and on 3xTF32 so is A when op(A) = N. The path then runs on the
+// normalised problem with the rest of the workspace. The local gemm() takes
+// every op pair (reference include/spla/gemm.hpp:66-97,
+// src/gemm/gemm_gpu.cpp:59-174).
+struct Normalized {
+  GemmProblem p;  // the problem the path runs (pointers to the copies set at run time)
+  bool copyA = false, copyB = false;
+  int64_t ldAn = 0, ldBn = 0;
+  size_t offA = 0, offB = 0, prefix = 0;  // byte offsets of the copies; the path's workspace
+};
+
+size_t align_up256(size_t x) { return (x + 255) & ~size_t(255); }
+
+Normalized normalize(const GemmProblem& p, int rp) {
+  Normalized N;
+  N.p = p;
+  if (rp != SPLAB_PATH_OZAKI && rp != SPLAB_PATH_TF32X3) return N;
+  const size_t esz = size_t(dtype_bytes(p.dtype));
+  const int64_t kn = (std::max<int64_t>(p.k, 1) + 7) / 8 * 8;  // 16-byte aligned rows
+  size_t off = 0;
+  if (p.opB != 0) {
+    N.copyB = true;
+    N.ldBn = kn;
+    N.offB = off;
+    off = align_up256(off + esz * size_t(p.n) * size_t(kn));
+    N.p.opB = 0;
+    N.p.ldb = kn;
+  }
+  if (rp == SPLAB_PATH_TF32X3 && p.opA == 0) {
+    N.copyA = true;
+    N.ldAn = kn;
+    N.offA = off;
+    off = align_up256(off + esz * size_t(p.m) * size_t(kn));
+    N.p.opA = 1;
+    N.p.lda = kn;
+  }
+  N.prefix = off;
+  return N;
+}
+
+// The k-major view a tensor-core path would run (for support checks).
+GemmProblem k_major_view(const GemmProblem& p, bool copy_a) {
+  GemmProblem q = p;
+  q.opB = 0;
+  if (copy_a && q.opA == 0) q.opA = 1;
+  return q;
+}
+
+// Y (k x rows, column-major, ldy) <- X (rows x k, column-major, ldx),
+// conjugated when `conj` (complex element types): a 32 x 32 tile through
+// shared memory, reads coalesced along rows, writes along k.
+template <typename E>
+__global__ void to_k_major(const E* __restrict__ X, int64_t ldx, int64_t rows, int64_t k,
+                           int conj, E* __restrict__ Y, int64_t ldy) {
+  __shared__ E tile[32][33];
+  const int64_t r0 = int64_t(blockIdx.x) * 32;
+  for (int64_t k0 = int64_t(blockIdx.y) * 32; k0 < k; k0 += int64_t(gridDim.y) * 32) {
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+      const int64_t r = r0 + threadIdx.x, kk = k0 + j;
+      if (r < rows && kk < k) tile[j][threadIdx.x] = X[r + kk * ldx];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+      const int64_t r = r0 + j, kk = k0 + threadIdx.x;
+      if (r < rows && kk < k) {
+        E v = tile[threadIdx.x][j];
+        if constexpr (sizeof(E) == 8 && !std::is_same<E, double>::value) {
+          if (conj) v.y = -v.y;
+        } else if constexpr (sizeof(E) == 16) {
+          if (conj) v.y = -v.y;
+        }
+        Y[kk + r * ldy] = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_to_k_major(int dtype, const void* X, int64_t ldx, int64_t rows, int64_t k,
+                              bool conj, void* Y, int64_t ldy, cudaStream_t st) {
+  if (rows <= 0 || k <= 0) return cudaSuccess;
+  const dim3 block(32, 8);
+  const dim3 grid(unsigned((rows + 31) / 32), unsigned(std::min<int64_t>((k + 31) / 32, 65535)));
+  auto go = [&](auto tag) {
+    using E = decltype(tag);
+    to_k_major<E><<<grid, block, 0, st>>>(static_cast<const E*>(X), ldx, rows, k, conj ? 1 : 0,
+                                          static_cast<E*>(Y), ldy);
+  };
+  switch (dtype) {
+    case kR32: go(float{}); break;
+    case kR64: go(double{}); break;
+    case kC32: go(float2{}); break;
+    default: go(double2{}); break;
+  }
+  return cudaGetLastError();
+}
+
+// The copies of a normalised problem, on `st`; redirects N.p's operands.
+cudaError_t run_normalization(Normalized& N, const GemmProblem& p, char* ws, cudaStream_t st) {
+  cudaError_t e = cudaSuccess;
+  if (N.copyB) {
+    // op(B) is k x n: B holds n x k (column-major, ldb)
+    e = launch_to_k_major(p.dtype, p.B, p.ldb, p.n, p.k, p.opB == 2, ws + N.offB, N.ldBn, st);
+    if (e != cudaSuccess) return e;
+    N.p.B = ws + N.offB;
+  }
+  if (N.copyA) {
+    e = launch_to_k_major(p.dtype, p.A, p.lda, p.m, p.k, false, ws + N.offA, N.ldAn, st);
+    if (e != cudaSuccess) return e;
+    N.p.A = ws + N.offA;
+  }
+  return e;
+}
+
+size_t path_workspace(const GemmProblem& p, int rp, int moduli) {
+  if (rp == SPLAB_PATH_TF32X3 || rp == SPLAB_PATH_OZAKI) {
+    const Normalized N = normalize(p, rp);
+    return N.prefix + (rp == SPLAB_PATH_TF32X3 ? tf32x3_workspace_bytes(N.p)
+                                               : ozaki_workspace_bytes(N.p, moduli));
+  }
+  return dmma_plan(p, num_sms()).workspace_bytes;
+}
+
 int resolve_path(const GemmProblem& p, int path, int moduli) {
-  const bool oz = ozaki_supported(p), tf = tf32x3_supported(p);
+  const bool oz = ozaki_supported(k_major_view(p, false));
+  const bool tf = tf32x3_supported(k_major_view(p, true));
   if (path == SPLAB_PATH_TF32X3) return tf ? SPLAB_PATH_TF32X3 : SPLAB_PATH_DMMA;
   if (path == SPLAB_PATH_OZAKI) return oz ? SPLAB_PATH_OZAKI : SPLAB_PATH_DMMA;
   if (path == SPLAB_PATH_DMMA || p.m <= 0 || p.n <= 0 || p.k <= 0) return SPLAB_PATH_DMMA;
   const size_t cap = device_total_memory() / 4;
+  // the k-major copies of a normalised problem: one read and one write each
+  const double esz = dtype_bytes(p.dtype);
+  const double copyB = p.opB != 0 ? 2.0 * p.n * p.k * esz / 6e12 * 1e3 : 0.0;
+  const double copyA = p.opA == 0 ? 2.0 * p.m * p.k * esz / 6e12 * 1e3 : 0.0;
   int best = SPLAB_PATH_DMMA;
   double best_ms = model::dmma_ms(p);
-  if (oz && ozaki_workspace_bytes(p, moduli) <= cap) {
-    const double t = model::ozaki_ms(p);
+  if (oz && path_workspace(p, SPLAB_PATH_OZAKI, moduli) <= cap) {
+    const double t = model::ozaki_ms(k_major_view(p, false)) + copyB;
     if (t < 0.9 * best_ms) {
       best = SPLAB_PATH_OZAKI;
       best_ms = t;
     }
   }
-  if (tf && tf32x3_workspace_bytes(p) <= cap) {
-    const double t = model::tf32x3_ms(p);
+  if (tf && path_workspace(p, SPLAB_PATH_TF32X3, moduli) <= cap) {
+    const double t = model::tf32x3_ms(k_major_view(p, true)) + copyB + copyA;
     if (t < 0.9 * best_ms) best = SPLAB_PATH_TF32X3;
   }
   return best;
@@ -265,10 +397,7 @@ size_t splab_gemm_workspace_size(int dtype, int path, int opA, int opB, int64_t 
   p.m = m;
   p.n = n;
   p.k = k;
-  const int rp = resolve_path(p, path, ozakiModuli);
-  if (rp == SPLAB_PATH_TF32X3) return tf32x3_workspace_bytes(p);
-  if (rp == SPLAB_PATH_OZAKI) return ozaki_workspace_bytes(p, ozakiModuli);
-  return dmma_plan(p, num_sms()).workspace_bytes;
+  return path_workspace(p, resolve_path(p, path, ozakiModuli), ozakiModuli);
 }
 
 int splab_gemm_check(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int64_t k,
@@ -284,10 +413,12 @@ int splab_gemm_check(int dtype, int path, int opA, int opB, int64_t m, int64_t n
   if (cudaStreamSynchronize(st) != cudaSuccess) return SPLAB_ERR_LAUNCH;
   if (m <= 0 || n <= 0 || !workspace) return SPLAB_OK;
   const int rp = resolve_path(p, path, ozakiModuli);
+  const Normalized N = normalize(p, rp);
+  void* pw = static_cast<char*>(workspace) + N.prefix;
   if (rp == SPLAB_PATH_TF32X3)
-    return tf32x3_status(p, workspace, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
+    return tf32x3_status(N.p, pw, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
   if (rp != SPLAB_PATH_OZAKI) return SPLAB_OK;
-  return ozaki_status(p, ozakiModuli, workspace, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
+  return ozaki_status(N.p, ozakiModuli, pw, st) ? SPLAB_ERR_TIMEOUT : SPLAB_OK;
 }
 
 int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int64_t k,
@@ -304,14 +435,16 @@ int splab_gemm(int dtype, int path, int opA, int opB, int64_t m, int64_t n, int6
   cudaError_t err;
   if (ozakiModuli != 0 && (ozakiModuli < 8 || ozakiModuli > 16)) return SPLAB_ERR_INVALID;
   const int rp = resolve_path(p, path, ozakiModuli);
-  if (rp == SPLAB_PATH_TF32X3) {
-    const size_t need = tf32x3_workspace_bytes(p);
+  if (rp == SPLAB_PATH_TF32X3 || rp == SPLAB_PATH_OZAKI) {
+    const size_t need = path_workspace(p, rp, ozakiModuli);
     if (need > workspaceBytes || (need && !workspace)) return SPLAB_ERR_WORKSPACE;
-    err = tf32x3_gemm(p, workspace, workspaceBytes, st);
-  } else if (rp == SPLAB_PATH_OZAKI) {
-    const size_t need = ozaki_workspace_bytes(p, ozakiModuli);
-    if (need > workspaceBytes || (need && !workspace)) return SPLAB_ERR_WORKSPACE;
-    err = ozaki_gemm(p, ozakiModuli, workspace, workspaceBytes, st);
+    Normalized N = normalize(p, rp);
+    char* ws = static_cast<char*>(workspace);
+    err = run_normalization(N, p, ws, st);
+    if (err == cudaSuccess)
+      err = rp == SPLAB_PATH_TF32X3
+                ? tf32x3_gemm(N.p, ws + N.prefix, workspaceBytes - N.prefix, st)
+                : ozaki_gemm(N.p, ozakiModuli, ws + N.prefix, workspaceBytes - N.prefix, st);
   } else {
     const DmmaPlan plan = dmma_plan(p, num_sms());
     if (plan.workspace_bytes > workspaceBytes || (plan.workspace_bytes && !workspace))

@@ -350,3 +350,41 @@ print('DEVICE_OK')
                          timeout=300)
     assert "TIMEOUT_REPORTED" in out.stdout, out.stdout + out.stderr
     assert "DEVICE_OK" in out.stdout, out.stdout + out.stderr
+
+
+@pytest.mark.parametrize("m,n,k,opA,pad", [(300, 150, 150000, 2, 0), (257, 129, 1000, 1, 3),
+                                           (40, 24, 3000, 2, 1), (513, 70, 769, 0, 0),
+                                           (128, 1024, 250000, 2, 0)])
+def test_tensor_core_slicer_matches_fp32_slicer(m, n, k, opA, pad):
+    """Complex double rows are sliced with the digit sums on the INT8 tensor
+    cores (oz_slice_tc); SPLAB_OZAKI_SLICE_TC=0 selects the FP32 digit-sum
+    slicer. Both produce the same symmetric residues, so C is bit-identical:
+    unit tails (k not a multiple of 768), residue rows padded to 128, partial
+    groups, op(A) = N (the k-major copy), both signs of the sum plane, and
+    several k-chunks."""
+    import torch
+    dt = np.complex128
+    lda = (m if opA == 0 else k) + pad
+    A = buffer(dt, lda, k if opA == 0 else m, 31, "gauss_k", k)
+    B = buffer(dt, k + pad, n, 32, "gauss_k", k)
+    C = buffer(dt, m + pad, n, 33, "uniform11")
+    out = []
+    for tc in ("1", "0"):
+        os.environ["SPLAB_OZAKI_SLICE_TC"] = tc
+        try:
+            ctx = spla.Context(spla.PU_GPU)
+            ctx.set_fp64_path(spla.PATH_OZAKI)
+            dC = _dev(C)
+            spla.gemm(opA, 0, m, n, k, 0.5 - 0.25j, _dev(A), lda, _dev(B), k + pad, 1.5, dC,
+                      m + pad, ctx)
+            torch.cuda.synchronize()
+            out.append(dC.cpu().numpy())
+        finally:
+            os.environ.pop("SPLAB_OZAKI_SLICE_TC", None)
+    assert np.array_equal(out[0], out[1])
+    # accuracy against the device double-double product (k up to 250000)
+    R = torch.zeros(n * (m + pad), dtype=torch.complex128, device="cuda")
+    assert spla.gemm_dd(3, opA, 0, m, n, k, _dev(A), lda, _dev(B), k + pad, R, m + pad) == 0
+    torch.cuda.synchronize()
+    ref = ((0.5 - 0.25j) * R.cpu().numpy() + 1.5 * C).reshape(n, m + pad)[:, :m]
+    assert oracle.rel_fro(out[0].reshape(n, m + pad)[:, :m], ref) <= 1e-14
