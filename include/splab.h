@@ -197,6 +197,37 @@ SPLAB_API int splab_block_cyclic_info(int64_t rowsInBlock, int64_t colsInBlock, 
                             int64_t count, int64_t *out, void *stream);
 
 /*
+ * Multi-rank exchange support (pgemm_ssb / pgemm_sbs over several ranks).
+ *
+ * splab_block_cyclic_blocks: HOST. The block-cyclic map of the
+ * globalRows x globalCols submatrix at (rowOffset, colOffset) of a matrix in
+ * rowsInBlock x colsInBlock blocks on a gridRows x gridCols process grid, as
+ * BlockCyclicGenerator::get_block_info does it
+ * (src/block_generation/block_cyclic_generator.cpp:59-100): returns the
+ * number of blocks (-1 on bad arguments) and, when out is non-null, writes 9
+ * values per block (global row, global col, sub-row, sub-col, local row,
+ * local col, rows, cols, grid index of the owner) in column-major block
+ * order. The exchange plans of the distributed layer are built from it.
+ *
+ * splab_copy_blocks: DEVICE, asynchronous on `stream`. For each of `count`
+ * block descriptors (6 int64 in device memory: srcOff, srcLd, dstOff, dstLd,
+ * rows, cols, in elements) dst[dstOff + i + j*dstLd] =
+ * alpha * src[srcOff + i + j*srcLd] + beta * dst[...] (dst not read when beta
+ * is 0); maxBlockElems bounds rows*cols. alpha/beta are host scalars of the
+ * dtype. It performs the block moves of the reference's ring engines: sending
+ * each finished block of C to its owner and adding it there
+ * (src/pgemm_ssb/ring_ssb_gpu.cpp:413-500, src/pgemm_ssb/add_kernel.cpp:40-62)
+ * and redistributing the blocks of B (src/pgemm_sbs/ring_sbs_gpu.cpp:114-351).
+ */
+SPLAB_API int64_t splab_block_cyclic_blocks(int64_t rowsInBlock, int64_t colsInBlock,
+                                            int64_t gridRows, int64_t gridCols,
+                                            int64_t globalRows, int64_t globalCols,
+                                            int64_t rowOffset, int64_t colOffset, int64_t *out);
+SPLAB_API int splab_copy_blocks(int dtype, const void *src, void *dst, const int64_t *desc,
+                                int64_t count, int64_t maxBlockElems, const void *alpha,
+                                const void *beta, void *stream);
+
+/*
  * Double-double reference product for verification (no reference counterpart;
  * it is the device form of the compensated CPU oracle and sits on no
  * contraction path): R = op(A) * op(B) with every product split exactly

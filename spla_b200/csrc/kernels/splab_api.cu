@@ -350,6 +350,65 @@ __global__ void block_cyclic_info_kernel(int64_t rb, int64_t cb, int64_t gr, int
   o[8] = (gbRow % gr) + (gbCol % gc) * gr;
 }
 
+// Block copies of the distributed exchange: for every block descriptor
+// (srcOff, srcLd, dstOff, dstLd, rows, cols) in elements,
+// dst[dstOff + i + j dstLd] = alpha src[srcOff + i + j srcLd] + beta dst[...]
+// (dst not read when beta = 0). blockIdx.y walks the blocks, blockIdx.x and
+// the threads their elements.
+template <typename T, bool CPLX>
+__global__ void copy_blocks_kernel(const T* __restrict__ src, T* __restrict__ dst,
+                                   const int64_t* __restrict__ desc, int64_t count, double ar,
+                                   double ai, double br, double bi) {
+  for (int64_t b = blockIdx.y; b < count; b += gridDim.y) {
+    const int64_t* d = desc + 6 * b;
+    const int64_t so = d[0], sld = d[1], dof = d[2], dld = d[3], rows = d[4], cols = d[5];
+    const int64_t total = rows * cols;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+         e += int64_t(gridDim.x) * blockDim.x) {
+      const int64_t i = e % rows, j = e / rows;
+      const int64_t s = so + i + j * sld, t = dof + i + j * dld;
+      if (CPLX) {
+        const double xr = double(src[2 * s]), xi = double(src[2 * s + 1]);
+        double yr = ar * xr - ai * xi, yi = ar * xi + ai * xr;
+        if (br != 0.0 || bi != 0.0) {
+          const double cr = double(dst[2 * t]), ci = double(dst[2 * t + 1]);
+          yr += br * cr - bi * ci;
+          yi += br * ci + bi * cr;
+        }
+        dst[2 * t] = T(yr);
+        dst[2 * t + 1] = T(yi);
+      } else {
+        double y = ar * double(src[s]);
+        if (br != 0.0) y += br * double(dst[t]);
+        dst[t] = T(y);
+      }
+    }
+  }
+}
+
+// Host form of the block-cyclic map (the device kernel above, one block at a
+// time): BlockCyclicGenerator::get_block_info
+// (src/block_generation/block_cyclic_generator.cpp:59-100).
+void block_cyclic_info_host(int64_t rb, int64_t cb, int64_t gr, int64_t gc, int64_t nr,
+                            int64_t nc, int64_t ro, int64_t co, int64_t b, int64_t* o) {
+  const int64_t firstRow = (ro / rb) * rb, firstCol = (co / cb) * cb;
+  const int64_t numBlockRows = (ro - firstRow + nr + rb - 1) / rb;
+  const int64_t bRow = b % numBlockRows, bCol = b / numBlockRows;
+  const int64_t gbRow = bRow + ro / rb, gbCol = bCol + co / cb;
+  const int64_t gRow = std::max(ro, firstRow + bRow * rb), gCol = std::max(co, firstCol + bCol * cb);
+  const int64_t endRow = std::min((gbRow + 1) * rb, ro + nr);
+  const int64_t endCol = std::min((gbCol + 1) * cb, co + nc);
+  o[0] = gRow;
+  o[1] = gCol;
+  o[2] = gRow - ro;
+  o[3] = gCol - co;
+  o[4] = (gbRow / gr) * rb + gRow % rb;
+  o[5] = (gbCol / gc) * cb + gCol % cb;
+  o[6] = endRow - gRow;
+  o[7] = endCol - gCol;
+  o[8] = (gbRow % gr) + (gbCol % gc) * gr;
+}
+
 // A batch plan: the grouped FP64 launch or a tensor-core sequence.
 struct BatchHandle {
   BatchPlanImpl* grouped = nullptr;
@@ -629,6 +688,55 @@ int splab_block_cyclic_info(int64_t rowsInBlock, int64_t colsInBlock, int64_t gr
   block_cyclic_info_kernel<<<unsigned(blocks), threads, 0, static_cast<cudaStream_t>(stream)>>>(
       rowsInBlock, colsInBlock, gridRows, gridCols, globalRows, globalCols, rowOffset, colOffset,
       blockIdx, count, out);
+  return cudaGetLastError() == cudaSuccess ? SPLAB_OK : SPLAB_ERR_LAUNCH;
+}
+
+int64_t splab_block_cyclic_blocks(int64_t rowsInBlock, int64_t colsInBlock, int64_t gridRows,
+                                  int64_t gridCols, int64_t globalRows, int64_t globalCols,
+                                  int64_t rowOffset, int64_t colOffset, int64_t* out) {
+  if (rowsInBlock < 1 || colsInBlock < 1 || gridRows < 1 || gridCols < 1 || globalRows < 0 ||
+      globalCols < 0 || rowOffset < 0 || colOffset < 0)
+    return -1;
+  if (globalRows == 0 || globalCols == 0) return 0;
+  const int64_t firstRow = (rowOffset / rowsInBlock) * rowsInBlock;
+  const int64_t firstCol = (colOffset / colsInBlock) * colsInBlock;
+  const int64_t nbr = (rowOffset - firstRow + globalRows + rowsInBlock - 1) / rowsInBlock;
+  const int64_t nbc = (colOffset - firstCol + globalCols + colsInBlock - 1) / colsInBlock;
+  const int64_t count = nbr * nbc;
+  if (out)
+    for (int64_t b = 0; b < count; ++b)
+      block_cyclic_info_host(rowsInBlock, colsInBlock, gridRows, gridCols, globalRows, globalCols,
+                             rowOffset, colOffset, b, out + 9 * b);
+  return count;
+}
+
+int splab_copy_blocks(int dtype, const void* src, void* dst, const int64_t* desc, int64_t count,
+                      int64_t maxBlockElems, const void* alpha, const void* beta, void* stream) {
+  if (dtype < 0 || dtype > 3 || count < 0 || maxBlockElems < 0 || !alpha || !beta)
+    return SPLAB_ERR_INVALID;
+  if (count == 0 || maxBlockElems == 0) return SPLAB_OK;
+  if (!src || !dst || !desc) return SPLAB_ERR_INVALID;
+  const bool dbl = dtype_is_double(dtype), cplx = dtype_is_complex(dtype);
+  double a[2] = {0, 0}, b[2] = {0, 0};
+  for (int i = 0; i < (cplx ? 2 : 1); ++i) {
+    a[i] = dbl ? static_cast<const double*>(alpha)[i] : static_cast<const float*>(alpha)[i];
+    b[i] = dbl ? static_cast<const double*>(beta)[i] : static_cast<const float*>(beta)[i];
+  }
+  const int threads = 256;
+  const dim3 grid(unsigned(std::min<int64_t>((maxBlockElems + threads - 1) / threads, 1024)),
+                  unsigned(std::min<int64_t>(count, 65535)));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  auto go = [&](auto tag, auto cflag) {
+    using T = decltype(tag);
+    copy_blocks_kernel<T, decltype(cflag)::value><<<grid, threads, 0, st>>>(
+        static_cast<const T*>(src), static_cast<T*>(dst), desc, count, a[0], a[1], b[0], b[1]);
+  };
+  switch (dtype) {
+    case kR32: go(float{}, std::false_type{}); break;
+    case kR64: go(double{}, std::false_type{}); break;
+    case kC32: go(float{}, std::true_type{}); break;
+    default: go(double{}, std::true_type{}); break;
+  }
   return cudaGetLastError() == cudaSuccess ? SPLAB_OK : SPLAB_ERR_LAUNCH;
 }
 
