@@ -12,8 +12,9 @@ headline metric). One step = one contraction of the whole problem.
   e2e   : the same metric through the public C ABI (spla_pzgemm_ssb) with A, B,
           C in pinned HOST memory: every step streams A and B to the GPU and
           reads C back inside the timed region.
-  paths : TFLOP/s and relative Frobenius error (vs the double-double oracle on
-          sampled columns) of each contraction path.
+  paths : TFLOP/s and relative Frobenius error of each contraction path on the
+          whole C, against the device double-double product (splab_gemm_dd),
+          which is itself checked against the CPU Dot2 oracle on three columns.
 
 Multi-GPU (torchrun, one rank per GPU): every rank runs its own replica of the
 single-rank problem (the single-rank path has no exchange step); value is the
@@ -21,7 +22,8 @@ sum of all ranks' flops over the max-over-ranks time.
 
 --impl reference times the reference's own CPU path (oracle/_ref, the
 reference library compiled from its sources, else the oracle's C
-restatement) on the host cores, rank 0 only.
+restatement) on the host cores, rank 0 only: the same metric and workload,
+one full call per step.
 """
 from __future__ import annotations
 
@@ -609,6 +611,54 @@ def workload_cgemm_ssb(torch, spla, steps, warmup, path=None):
                                 3: "3xTF32"}[path]}}
 
 
+def workload_gemm_ops(torch, spla, steps, warmup, opA, opB, path=None):
+    """Local spla_zgemm, C = op(A) op(B), complex double, m = n = 1024,
+    k = 250000 (the headline's size), Gaussian/sqrt(k) operands stored as each
+    op requires (op N: A is m x k, B is k x n; op T/C: A is k x m, B is n x k),
+    beta = 0, on the context's path (AUTO by default); error on the whole C
+    against the device double-double product."""
+    m = n = 1024
+    k = 250000
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20250010 + 3 * opA + opB)
+    s = (1.0 / (2.0 * k)) ** 0.5
+    A = torch.randn(m * k, dtype=torch.complex128, device="cuda", generator=g) * s
+    B = torch.randn(n * k, dtype=torch.complex128, device="cuda", generator=g) * s
+    lda = m if opA == 0 else k
+    ldb = k if opB == 0 else n
+    C = torch.zeros(m * n, dtype=torch.complex128, device="cuda")
+    ctx = spla.Context(spla.PU_GPU)
+    if path is not None:
+        ctx.set_fp64_path(path)
+    resolved = spla.lib().splab_gemm_path(3, spla.PATH_AUTO if path is None else path, opA, opB,
+                                          m, n, k)
+
+    def step():
+        spla.gemm(opA, opB, m, n, k, 1.0, A, lda, B, ldb, 0.0, C, m, ctx)
+
+    for _ in range(warmup):
+        step()
+    e0, e1 = _events(torch)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    R = torch.zeros(m * n, dtype=torch.complex128, device="cuda")
+    assert spla.gemm_dd(3, opA, opB, m, n, k, A, lda, B, ldb, R, m) == 0
+    torch.cuda.synchronize()
+    err = float(torch.linalg.vector_norm(C - R) / torch.linalg.vector_norm(R))
+    ops = "NTC"
+    name = {1: "FP64 DMMA", 2: "Ozaki INT8", 3: "3xTF32"}[resolved]
+    return {"metric": f"ZGEMM TFLOP/s (spla_zgemm op(A)={ops[opA]} op(B)={ops[opB]}, {name})",
+            "value": 8.0 * m * n * k / (ms / 1e3) / 1e12, "unit": "TFLOP/s", "ms_per_step": ms,
+            "rel_err_whole_c_vs_double_double": err,
+            "config": {"workload": f"spla_zgemm {ops[opA]}{ops[opB]} m=n=1024 k=250000",
+                       "path": ("auto: " if path is None else "") + name}}
+
+
 def workload_batch(torch, spla, steps, warmup, dtype="complex128", count=64, sub=32, path=None):
     """64 ssb instances, k ~ U{120000..180000}, m = n ~ U{512, 768, 1024}
     (seeded draw order: k then m per instance), Gaussian/sqrt(k); run as
@@ -688,6 +738,10 @@ def run_workload(name, steps, warmup):
           "cgemm_ssb_dmma": lambda t, s, st, w: workload_cgemm_ssb(t, s, st, w, 1),
           "cgemm_ssb_ozaki": lambda t, s, st, w: workload_cgemm_ssb(t, s, st, w, 2),
           "cgemm_ssb_tf32x3": lambda t, s, st, w: workload_cgemm_ssb(t, s, st, w, 3),
+          "zgemm_nn": lambda t, s, st, w: workload_gemm_ops(t, s, st, w, 0, 0),
+          "zgemm_nt": lambda t, s, st, w: workload_gemm_ops(t, s, st, w, 0, 1),
+          "zgemm_cn": lambda t, s, st, w: workload_gemm_ops(t, s, st, w, 2, 0),
+          "zgemm_cc": lambda t, s, st, w: workload_gemm_ops(t, s, st, w, 2, 2),
           "batch": workload_batch,
           "batch_c64": lambda t, s, st, w: workload_batch(t, s, st, w, "complex64", 64, 64),
           "batch_ozaki": lambda t, s, st, w: workload_batch(t, s, st, w, "complex128", 64, 32, 2),
@@ -717,7 +771,8 @@ def main():
                     choices=["zgemm_ssb", "sbs", "sbs_dmma", "sbs_ozaki", "ssbtr_float",
                              "ssbtr_float_dmma",
                              "ssbtr_float_ozaki", "ssbtr_float_tf32x3", "cgemm_ssb_dmma",
-                             "cgemm_ssb_ozaki", "cgemm_ssb_tf32x3", "batch", "batch_c64",
+                             "cgemm_ssb_ozaki", "cgemm_ssb_tf32x3", "zgemm_nn", "zgemm_nt",
+                             "zgemm_cn", "zgemm_cc", "batch", "batch_c64",
                              "batch_ozaki", "batch_c64_ozaki", "batch_c64_tf32x3"])
     args = ap.parse_args()
     if args.workload != "zgemm_ssb" and args.impl == "ours":

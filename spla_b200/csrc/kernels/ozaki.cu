@@ -315,7 +315,7 @@ __device__ __forceinline__ uint32_t pack4(float a, float b, float c, float d) {
 // NMU > 0: moduli 0 .. NMU-1 in one fully unrolled pass (the per-modulus
 // constants become fixed parameter operands); 0: t_begin .. t_end-1 in a loop.
 template <typename TIn, bool VEC, int NDIG, int EL, int NMU>
-__global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
+__global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
     oz_slice(const TIn* __restrict__ X, int64_t ld_doubles, int64_t len, int rows, int64_t kp,
              const int* __restrict__ sigma, int mode, int s_sum, int8_t* __restrict__ res,
              int64_t res_mod_stride, SliceConsts sc, int t_begin, int t_end) {
@@ -479,11 +479,16 @@ __global__ void __launch_bounds__(256, EL == 8 ? 3 : 2)
 // stages the bytes of its 256-element row segment in shared memory and writes
 // it with one bulk copy.
 //
-// Warps 0-3: epilogue (warp w reads TMEM lanes 32 w .. 32 w + 31, one
-// (group, modulus, plane) row each); warps 4-7: producers (row scaling,
-// digits into the 128-byte-swizzled B tile, modulus-256 bytes); warp 8: TMEM
-// allocation and the MMA issue. Digits and accumulators are double-buffered;
-// every wait is bounded and a give-up sets *status.
+// Warps 0-7: epilogue (warp w reads TMEM lanes 32 (w % 4) .. + 31, one
+// (group, modulus, plane) row each, and columns 128 (w / 4) .. + 127, two
+// warps per lane quarter so that the TMEM loads and the reduction of one
+// overlap the other's); warps 8-11: producers (row scaling, digits into the
+// 128-byte-swizzled B tile, modulus-256 bytes); warp 12: TMEM allocation and
+// the MMA issue. Digits and accumulators are double-buffered; every wait is
+// bounded and a give-up sets *status. Each epilogue warp stages its 32 row
+// segments of 128 bytes in shared memory and writes them with coalesced
+// 16-byte stores (4 rows of 128 bytes per instruction; one bulk copy per row
+// segment measured 30 % slower: the copy engine's cost per small copy).
 struct SliceTcParams {
   const double* X;        // rows of interleaved complex doubles
   int64_t ld;             // row stride in doubles
@@ -505,7 +510,7 @@ struct SliceTcParams {
   unsigned long long wait_limit_ns;
 };
 
-constexpr int TC_THREADS = 288;
+constexpr int TC_THREADS = 416;  // warps 0-7 epilogue, 8-11 producers, 12 MMA
 constexpr int TC_W_BYTES = 128 * 128;            // weights: 128 rows x 128 B (SW128)
 constexpr int TC_D_BYTES = 256 * 128;            // digits: 256 rows x 128 B (SW128)
 constexpr int TC_ROW_STAGE = 256 + 16;           // one staged row segment (padded)
@@ -534,12 +539,6 @@ __device__ __forceinline__ long long round_to_int64(double y) {
 __device__ __forceinline__ unsigned long long balanced_digits(long long x) {
   constexpr unsigned long long kOff = 0x0080808080808080ull;
   return (static_cast<unsigned long long>(x) + kOff) ^ kOff;
-}
-
-__device__ __forceinline__ void bulk_store(void* gdst, uint32_t ssrc, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst),
-               "r"(ssrc), "r"(bytes)
-               : "memory");
 }
 
 __global__ void __launch_bounds__(TC_THREADS, 1) oz_slice_tc(const __grid_constant__ SliceTcParams P) {
@@ -595,13 +594,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) oz_slice_tc(const __grid_consta
       mbar_init(dfull(b), 128);
       mbar_init(dempty(b), 1);
       mbar_init(accf(b), 1);
-      mbar_init(acce(b), 128);
+      mbar_init(acce(b), 256);
     }
     mbar_init(drain_bar, 1);
     *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 8) {
+  if (warp == 12) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
                      smem_u32(tmem_slot))
                  : "memory");
@@ -613,10 +612,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) oz_slice_tc(const __grid_consta
   const uint32_t tmem_base = *tmem_slot;
   const int unit_elems = 256 * P.groups;
 
-  if (warp >= 4 && warp < 8) {
+  if (warp >= 8 && warp < 12) {
     // ---- producers: 2 G elements per thread and unit, consecutive threads
     // on consecutive elements (coalesced 16-byte loads)
-    const int pt = threadIdx.x - 128;
+    const int pt = threadIdx.x - 256;
     const int per = 2 * P.groups;
     // the elements of unit u, loaded one unit ahead of their use
     auto load = [&](long long u, double2 (&v)[8]) {
@@ -668,7 +667,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) oz_slice_tc(const __grid_consta
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(dfull(b));
     }
-  } else if (warp == 8) {
+  } else if (warp == 12) {
     if (lane == 0) {
       // ---- MMA issuer
       bool ok = true;
@@ -695,9 +694,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) oz_slice_tc(const __grid_consta
         }
       }
     }
-  } else if (warp < 4) {
-    // ---- epilogue: TMEM lane L = (group, modulus, plane) row
-    const int L = warp * 32 + lane;
+  } else if (warp < 8) {
+    // ---- epilogue: TMEM lane L = (group, modulus, plane) row, half of the columns
+    const int quarter = warp & 3, half = warp >> 2;
+    const int L = quarter * 32 + lane;
     const bool active = L < wrows;
     int g = 0, t = 1, q = 0;
     if (active) {
@@ -710,62 +710,84 @@ __global__ void __launch_bounds__(TC_THREADS, 1) oz_slice_tc(const __grid_consta
     const unsigned long long NP2 = f2_pack(-pf, -pf);
     const unsigned long long IP2 = f2_pack(1.0f / pf, 1.0f / pf);
     const unsigned long long M2 = f2_pack(kMagic, kMagic), NM2 = f2_pack(-kMagic, -kMagic);
-    const uint32_t row_stage = uint32_t(L) * TC_ROW_STAGE;
+    const uint32_t seg_stage = uint32_t(L) * TC_ROW_STAGE + uint32_t(half * 128);
+    const uint32_t lane_taddr = tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(half * 128);
+    // 32 sums -> 32 residue bytes at st
+    auto reduce32 = [&](const uint32_t (&v)[32], unsigned char* st) {
+      uint32_t wv[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        float r[4];
+#pragma unroll
+        for (int e2 = 0; e2 < 2; ++e2) {
+          const int c = 4 * h + 2 * e2;
+          // MAGIC + s exactly (|s| < 2^22), s, its nearest quotient by p,
+          // MAGIC + s - q p = MAGIC + (s mod p)
+          const unsigned long long tM = f2_pack(__int_as_float(0x4B400000 + int(v[c])),
+                                                __int_as_float(0x4B400000 + int(v[c + 1])));
+          const unsigned long long t2 = f2_add(tM, NM2);
+          const unsigned long long q2 = f2_add(f2_fma(t2, IP2, M2), NM2);
+          f2_unpack(f2_fma(q2, NP2, tM), r[2 * e2], r[2 * e2 + 1]);
+        }
+        wv[h] = pack4(r[0], r[1], r[2], r[3]);
+      }
+      *reinterpret_cast<uint4*>(st) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+      *reinterpret_cast<uint4*>(st + 16) = make_uint4(wv[4], wv[5], wv[6], wv[7]);
+    };
     for (long long u = blockIdx.x, it = 0; u < P.total_units; u += gridDim.x, ++it) {
       const int b = int(it & 1);
       const uint32_t par = uint32_t((it >> 1) & 1);
       if (!mbar_wait(accf(b), par, abort, P.wait_limit_ns)) break;
       tc_fence_after();
-      // the staging slot of this unit was last read by the bulk copy of unit it - 2
-      if (active) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-      unsigned char* st = St + b * TC_S_BYTES + row_stage;
-#pragma unroll 1
-      for (int c0 = 0; c0 < 256; c0 += 32) {
-        uint32_t v[32];
-        tmem_ld32(tmem_base + (uint32_t(warp * 32) << 16) + uint32_t(b * 256 + c0), v);
-        if (active) {
-          uint32_t wv[8];
-#pragma unroll
-          for (int h = 0; h < 8; ++h) {
-            float r[4];
-#pragma unroll
-            for (int e2 = 0; e2 < 2; ++e2) {
-              const int c = 4 * h + 2 * e2;
-              // MAGIC + s exactly (|s| < 2^22), s, its nearest quotient by p,
-              // MAGIC + s - q p = MAGIC + (s mod p)
-              const unsigned long long tM = f2_pack(__int_as_float(0x4B400000 + int(v[c])),
-                                                    __int_as_float(0x4B400000 + int(v[c + 1])));
-              const unsigned long long t2 = f2_add(tM, NM2);
-              const unsigned long long q2 = f2_add(f2_fma(t2, IP2, M2), NM2);
-              f2_unpack(f2_fma(q2, NP2, tM), r[2 * e2], r[2 * e2 + 1]);
-            }
-            wv[h] = pack4(r[0], r[1], r[2], r[3]);
-          }
-          *reinterpret_cast<uint4*>(st + c0) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
-          *reinterpret_cast<uint4*>(st + c0 + 16) = make_uint4(wv[4], wv[5], wv[6], wv[7]);
-        }
-      }
+      unsigned char* st = St + b * TC_S_BYTES + seg_stage;
+      const uint32_t taddr = lane_taddr + uint32_t(b * 256);
+      // four chunks of 32 columns; the load of chunk c + 1 is in flight while
+      // chunk c is reduced
+      uint32_t va[32], vb[32];
+      tmem_ld32_nowait(taddr, va);
+      tmem_wait_ld();
+      tmem_ld32_nowait(taddr + 32, vb);
+      if (active) reduce32(va, st);
+      tmem_wait_ld();
+      tmem_ld32_nowait(taddr + 64, va);
+      if (active) reduce32(vb, st + 32);
+      tmem_wait_ld();
+      tmem_ld32_nowait(taddr + 96, vb);
+      if (active) reduce32(va, st + 64);
+      tmem_wait_ld();
       tc_fence_before();
-      mbar_arrive(acce(b));
-      if (active) {
-        const int row = int(u / P.units_per_row);
-        const int64_t e = (u - int64_t(row) * P.units_per_row) * unit_elems + 256 * g;
-        const int64_t n = P.kp - e < 256 ? P.kp - e : 256;  // a multiple of 128, or <= 0
-        if (n > 0) {
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          bulk_store(P.res + t * P.mod_stride + q * P.plane + int64_t(row) * P.kp + e,
-                     s_addr + uint32_t(b * TC_S_BYTES) + row_stage, uint32_t(n));
+      mbar_arrive(acce(b));  // TMEM buffer b is free for the MMA of unit it + 2
+      if (active) reduce32(vb, st + 96);
+      const int row = int(u / P.units_per_row);
+      const int64_t e_unit = (u - int64_t(row) * P.units_per_row) * unit_elems;
+      // this lane's row segment: destination and valid bytes (a multiple of 16)
+      const int64_t e = e_unit + 256 * g + 128 * half;
+      const int64_t nb = active ? (P.kp - e < 128 ? P.kp - e : 128) : 0;
+      int8_t* dst = P.res + t * P.mod_stride + q * P.plane + int64_t(row) * P.kp + e;
+      {
+        // coalesced: per instruction 4 rows x 8 lanes x 16 bytes
+        __syncwarp();
+        const unsigned long long dst_u = reinterpret_cast<unsigned long long>(dst);
+        const unsigned char* wst = St + b * TC_S_BYTES + uint32_t(quarter * 32) * TC_ROW_STAGE +
+                                   uint32_t(half * 128);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int r = 4 * i + (lane >> 3), c = lane & 7;
+          const unsigned long long rd = __shfl_sync(0xffffffffu, dst_u, r);
+          const int64_t rn = __shfl_sync(0xffffffffu, nb, r);
+          if (16 * c < rn)
+            *reinterpret_cast<uint4*>(reinterpret_cast<int8_t*>(rd) + 16 * c) =
+                *reinterpret_cast<const uint4*>(wst + r * TC_ROW_STAGE + 16 * c);
         }
-        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        __syncwarp();
       }
     }
-    if (active) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
 
   tc_fence_before();
   __syncthreads();
   if (*abort && threadIdx.x == 0) atomicExch(P.status, 1);
-  if (warp == 8) {
+  if (warp == 12) {
     __syncwarp();
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base)
@@ -1689,12 +1711,17 @@ void scale_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
 }
 
 // Residue slicing of complex double rows with the digit sums on the tensor
-// cores (oz_slice_tc): used for all moduli at once when the modulus 256 comes
-// first and the rows are 16-byte aligned; SPLAB_OZAKI_SLICE_TC=0 selects the
-// FP32 digit-sum slicer instead.
-bool slice_tc_enabled() {  // read per call: tests compare both slicers in one process
+// cores (oz_slice_tc), selected by SPLAB_OZAKI_SLICE_TC=1 (read per call, so
+// that tests compare both slicers in one process); used for all moduli at once
+// when the modulus 256 comes first and the rows are 16-byte aligned. The FP32
+// digit-sum slicer (oz_slice) is the default: on B200 it measured faster
+// (headline problem: 5.25 + 4.75 ms against 5.77 + 5.10 ms for the residues
+// of A and B), the tensor-core form being bound by instruction issue and
+// latency (TMEM round trip, staging, synchronisation) rather than by the FP32
+// pipe it relieves.
+bool slice_tc_enabled() {
   const char* v = std::getenv("SPLAB_OZAKI_SLICE_TC");
-  return !(v && v[0] == '0');
+  return v && v[0] == '1';
 }
 
 cudaError_t launch_slice_tc(const double* X, int64_t ld, int64_t len, int rows, int64_t kp,

@@ -28,8 +28,10 @@ def test_explicit_paths():
     L = spla.lib()
     assert L.splab_gemm_path(C64, OZAKI, 2, 0, 64, 64, 100) == OZAKI
     assert L.splab_gemm_path(C64, TF3, 2, 0, 4096, 4096, 100000) == DMMA  # double: no 3xTF32
-    assert L.splab_gemm_path(C32, TF3, 0, 0, 512, 512, 4096) == DMMA      # op(A) = N
-    assert L.splab_gemm_path(C64, OZAKI, 0, 1, 64, 64, 100) == DMMA       # op(B) = T
+    # any op pair on the tensor-core paths (k-major copies of op(A) = N / op(B) != N)
+    assert L.splab_gemm_path(C32, TF3, 0, 0, 512, 512, 4096) == TF3       # op(A) = N
+    assert L.splab_gemm_path(C64, OZAKI, 0, 1, 64, 64, 100) == OZAKI      # op(B) = T
+    assert L.splab_gemm_path(C32, TF3, 2, 2, 64, 64, 100) == TF3          # op(B) = C
     # op(A) = N on Ozaki (A copied k-major first): the subspace rotation shape
     assert L.splab_gemm_path(C64, spla.PATH_AUTO, 0, 0, 200000, 2048, 2048) == OZAKI
     assert L.splab_gemm_path(C64, spla.PATH_AUTO, 0, 0, 4096, 4096, 100000) == OZAKI

@@ -51,9 +51,9 @@ def block(x, ldc, m, n, ro, co):
 def test_path_resolution():
     assert spla.lib().splab_gemm_path(2, spla.PATH_TF32X3, 2, 0, 512, 512, 4096) == spla.PATH_TF32X3
     assert spla.lib().splab_gemm_path(0, spla.PATH_TF32X3, 1, 0, 512, 512, 4096) == spla.PATH_TF32X3
-    # double dtypes and op(A) = N are not handled by the path
+    # double dtypes are not handled by the path; op(A) = N is, through a k-major copy of A
     assert spla.lib().splab_gemm_path(3, spla.PATH_TF32X3, 2, 0, 512, 512, 4096) == spla.PATH_DMMA
-    assert spla.lib().splab_gemm_path(2, spla.PATH_TF32X3, 0, 0, 512, 512, 4096) == spla.PATH_DMMA
+    assert spla.lib().splab_gemm_path(2, spla.PATH_TF32X3, 0, 0, 512, 512, 4096) == spla.PATH_TF32X3
 
 
 @pytest.mark.parametrize("dt,opA", [(np.complex64, 2), (np.complex64, 1), (np.float32, 1)])
