@@ -895,14 +895,17 @@ def main():
         int8_ops = 2.0 * nmod * 3 * M * N * K
         achieved = int8_ops / (k_ms / 1e3) / 1e12
         peak = peaks.get("int8_tops")
-        # DRAM bytes of one GEMM launch of this workload (m=n=1024, k=250000), from a one-pass
-        # ncu capture of oz_gemm_pair on it: 28.32 GB read + 0.229 GB written
-        traffic = 28.32e9 + 0.229e9 if (M, N, K) == (1024, 1024, 250000) else None
+        # DRAM bytes of one GEMM launch: 1.286 x the algorithmic residue bytes, the ratio of
+        # an ncu capture of oz_gemm_pair on the same tiling with a shorter k (m = n = 1024,
+        # k = 40000: 4.745 GB for 3.692 GB of residues), scaled by the k-blocks processed
+        alg_bytes = float(OZAKI_MODULI) * 3 * (M + N) * ((K + 127) // 128 * 128)
+        traffic = 1.286 * alg_bytes if (M, N) == (1024, 1024) else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
                 "frac": (achieved / peak) if peak else None, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_{read,write}.sum of oz_gemm_pair, one-pass "
-                                  "capture of this launch (profiles/oz_gemm_pair_int8_traffic_"
-                                  "zgemm_m1024_k250000.md)",
+                "traffic_source": "ncu dram__bytes_{read,write}.sum of oz_gemm_pair on "
+                                  "m=n=1024 k=40000 (same tiles, one k-chunk), 1.286 x the "
+                                  "residue bytes, scaled to this launch by its k-blocks "
+                                  "(profiles/oz_gemm_pair_int8_traffic_zgemm_m1024_k40000.md)",
                 "algorithmic_residue_bytes": float(OZAKI_MODULI) * 3 * (M + N) * K,
                 "kernel": "oz_gemm_pair (tcgen05.mma.cta_group::2.kind::i8, TMA, TMEM)",
                 "peak_source": "measured here: cuBLASLt int8 GEMM 8192^3 via torch._int_mm",
