@@ -324,18 +324,21 @@ __global__ void __launch_bounds__(THREADS, 1)
           break;
         }
         tc_fence_after();
-#pragma unroll
-        for (int q = 0; q < TN / 64; ++q) {
-          uint32_t a[32];
-          tmem_ld32_nowait(lane_addr + uint32_t(accb * TN + col_lo + 32 * q), a);
+        static_assert(TN / 64 == 2, "two 32-column loads per warp and window");
+        {
+          uint32_t a0[32], a1[32];  // both loads in flight, one wait
+          tmem_ld32_nowait(lane_addr + uint32_t(accb * TN + col_lo), a0);
+          tmem_ld32_nowait(lane_addr + uint32_t(accb * TN + col_lo + 32), a1);
           tmem_wait_ld();
 #pragma unroll
-          for (int cc = 0; cc < 32; ++cc)
-            mid[32 * q + cc] = __fadd_rn(mid[32 * q + cc], __uint_as_float(a[cc]));
+          for (int cc = 0; cc < 32; ++cc) {
+            mid[cc] = __fadd_rn(mid[cc], __uint_as_float(a0[cc]));
+            mid[32 + cc] = __fadd_rn(mid[32 + cc], __uint_as_float(a1[cc]));
+          }
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive_cluster(map_to_rank(acce_bar(accb), 0));
+        if (lane == 0) mbar_arrive_remote(map_to_rank(acce_bar(accb), 0));
         acc_phase[accb] ^= 1u;
         accb ^= 1;
 
