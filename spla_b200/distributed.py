@@ -373,8 +373,11 @@ def pgemm_ssb(m, n, kLocal, opA, alpha, A, lda, B, ldb, beta, C, ldc, cRowOffset
     else:
         lr, lc = distC.local_size(m, n, cRowOffset, cColOffset, distC.grid_index(me))
     _check_param(opA, OP_NONE, lr, lc, kLocal, A, lda, B, ldb, C, ldc)
-    # the local partial product, m x n, dense
-    P = backend.empty(C if C is not None else A, m * n)
+    # the local partial product, m x n, dense (dtype and device of the first buffer given)
+    like = next((x for x in (C, A, B) if x is not None), None)
+    if like is None:
+        raise InvalidPointerError("no buffer given")
+    P = backend.empty(like, m * n)
     backend.product(opA, OP_NONE, m, n, kLocal, 1.0, A, lda, B, ldb, 0.0, P, m)
     if distC.type == DIST_MIRROR:
         dist.all_reduce(_real(P), group=group)
@@ -414,7 +417,9 @@ def pgemm_sbs(mLocal, n, k, alpha, A, lda, B, ldb, bRowOffset, bColOffset, descB
     lr, lc = descB.local_size(k, n, bRowOffset, bColOffset, descB.grid_index(me))
     _check_param(OP_NONE, OP_NONE, mLocal, lc, lr, A, lda, B, ldb, C, ldc)
     plan = sbs_plan(descB, k, n, bRowOffset, bColOffset)
-    like = C if C is not None else A
+    like = next((x for x in (C, A, B) if x is not None), None)
+    if like is None:
+        raise InvalidPointerError("no buffer given")
     send = backend.empty(like, plan.seg)
     if B is not None:
         backend.copy_blocks(B, send, sbs_pack_desc(plan, me, ldb), 1.0, 0.0)
