@@ -445,8 +445,6 @@ def workload_sbs(torch, spla, steps, warmup, path=None):
     Haar-random unitary 2048 x 2048 (QR of a complex Gaussian, phases of
     diag(R) folded in), C 200000 x 2048 U[-1,1], alpha = beta = 1. The path
     is AUTO (None), FP64 DMMA (1) or Ozaki INT8 (2)."""
-    import numpy as np
-    import oracle
     mloc, n, k = 200000, 2048, 2048
     g = torch.Generator(device="cuda")
     g.manual_seed(20250003)
@@ -511,8 +509,6 @@ def workload_sbs(torch, spla, steps, warmup, path=None):
 def workload_ssbtr_float(torch, spla, steps, warmup, path=None):
     """psgemm_ssbtr lower fill, real float, k = 400000, m = n = 1536,
     Gaussian/sqrt(k)."""
-    import numpy as np
-    import oracle
     m = n = 1536
     k = 400000
     g = torch.Generator(device="cuda")
@@ -562,8 +558,6 @@ def workload_cgemm_ssb(torch, spla, steps, warmup, path=None):
     """pcgemm_ssb complex float, A^H B, k = 250000, m = n = 1024, complex
     Gaussian/sqrt(k) (the complex-double ssb configuration in single
     precision), full C, beta = 0."""
-    import numpy as np
-    import oracle
     m = n = 1024
     k = 250000
     g = torch.Generator(device="cuda")

@@ -213,7 +213,9 @@ SPLAB_API int splab_block_cyclic_info(int64_t rowsInBlock, int64_t colsInBlock, 
  * block descriptors (6 int64 in device memory: srcOff, srcLd, dstOff, dstLd,
  * rows, cols, in elements) dst[dstOff + i + j*dstLd] =
  * alpha * src[srcOff + i + j*srcLd] + beta * dst[...] (dst not read when beta
- * is 0); maxBlockElems bounds rows*cols. alpha/beta are host scalars of the
+ * is 0); maxBlockElems bounds rows*cols. src, dst and desc must be memory the
+ * device can reach (SPLAB_ERR_INVALID otherwise); the descriptors must stay
+ * inside the buffers. alpha/beta are host scalars of the
  * dtype. It performs the block moves of the reference's ring engines: sending
  * each finished block of C to its owner and adding it there
  * (src/pgemm_ssb/ring_ssb_gpu.cpp:413-500, src/pgemm_ssb/add_kernel.cpp:40-62)

@@ -716,6 +716,17 @@ int splab_copy_blocks(int dtype, const void* src, void* dst, const int64_t* desc
     return SPLAB_ERR_INVALID;
   if (count == 0 || maxBlockElems == 0) return SPLAB_OK;
   if (!src || !dst || !desc) return SPLAB_ERR_INVALID;
+  // all three are dereferenced by the kernel: memory the device cannot reach
+  // (pageable host memory) is refused here instead of faulting there
+  for (const void* ptr : {src, static_cast<const void*>(dst), static_cast<const void*>(desc)}) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+      cudaGetLastError();
+      return SPLAB_ERR_INVALID;
+    }
+    if (at.type == cudaMemoryTypeUnregistered || at.devicePointer == nullptr)
+      return SPLAB_ERR_INVALID;
+  }
   const bool dbl = dtype_is_double(dtype), cplx = dtype_is_complex(dtype);
   double a[2] = {0, 0}, b[2] = {0, 0};
   for (int i = 0; i < (cplx ? 2 : 1); ++i) {

@@ -281,6 +281,13 @@ class DeviceBackend:
         import torch
         if len(desc) == 0:
             return
+        # the kernel dereferences both buffers on the device: refuse host memory
+        # here rather than hand a host address to the GPU
+        for name, t in (("source", src), ("destination", dst)):
+            if not (isinstance(t, torch.Tensor) and t.is_cuda):
+                raise InvalidPointerError(f"block {name} must be a CUDA tensor")
+        if src.dtype != dst.dtype:
+            raise InvalidParameterError("block source and destination dtypes differ")
         dt = _CODE[str(dst.dtype).replace("torch.", "")]
         d = torch.from_numpy(np.ascontiguousarray(desc, np.int64)).to(dst.device)
         cplx = dt >= 2
