@@ -314,14 +314,17 @@ __device__ __forceinline__ uint32_t pack4(float a, float b, float c, float d) {
 // TIn: double (|x| < 2^62, five digits) or float (|x| < 2^38, three digits).
 // NMU > 0: moduli 0 .. NMU-1 in one fully unrolled pass (the per-modulus
 // constants become fixed parameter operands); 0: t_begin .. t_end-1 in a loop.
-template <typename TIn, bool VEC, int NDIG, int EL, int NMU>
+// MODE (0 or 2, the mode above) is a template parameter so that the unrolled
+// modulus loop carries no branch on it.
+template <typename TIn, bool VEC, int NDIG, int EL, int NMU, int MODE>
 __global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
     oz_slice(const TIn* __restrict__ X, int64_t ld_doubles, int64_t len, int rows, int64_t kp,
-             const int* __restrict__ sigma, int mode, int s_sum, int8_t* __restrict__ res,
+             const int* __restrict__ sigma, int s_sum, int8_t* __restrict__ res,
              int64_t res_mod_stride, SliceConsts sc, int t_begin, int t_end) {
   static_assert(EL == 8 || EL == 16, "8 or 16 reals per thread");
+  static_assert(MODE == 0 || MODE == 2, "real rows or complex rows");
   constexpr int W = EL / 4;  // packed words per modulus
-  const int64_t groups = (mode == 2 ? 2 * kp : kp) / EL;
+  const int64_t groups = (MODE == 2 ? 2 * kp : kp) / EL;
   const int64_t gid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   const int row = int(gid / groups);
   if (row >= rows) return;
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
     }
     // pairs (2i, 2i + 1) in mode 0; in mode 2 the real parts pair up first,
     // then the imaginary parts: (re0, re1), (re2, re3), ..., (im0, im1), ...
-    if (mode == 2) {
+    if constexpr (MODE == 2) {
       double u[EL];
 #pragma unroll
       for (int i = 0; i < EL / 2; ++i) {
@@ -382,10 +385,16 @@ __global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
   int8_t* const out0 = res + int64_t(row) * kp + l0;
   auto modulus = [&](const int t) {
     int8_t* out = out0 + t * res_mod_stride;
+    constexpr int H = EL / 4;        // mode 2: pairs of complex elements
     unsigned long long rp2[EL / 2];  // MAGIC + residue of elements 2i, 2i + 1
+    unsigned long long ri2[H];       // mode 2: residues of the imaginary pairs, unbiased
     if (t == 0 && sc.p0 == 256.0f) {
 #pragma unroll
       for (int i = 0; i < EL / 2; ++i) rp2[i] = f2_add(dp[i][0], M2);
+      if constexpr (MODE == 2) {
+#pragma unroll
+        for (int h = 0; h < H; ++h) ri2[h] = dp[H + h][0];
+      }
     } else {
       const unsigned long long np = sc.neg_p[t], ip = sc.inv_p[t];
       const unsigned long long c1 = sc.c[t][0], c2 = sc.c[t][1], c3 = sc.c[t][2],
@@ -397,17 +406,22 @@ __global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
         if (NDIG > 3) s2 = f2_fma(c3, dp[i][3], s2);
         if (NDIG > 4) s2 = f2_fma(c4, dp[i][4], s2);
         const unsigned long long q2 = f2_add(f2_fma(s2, ip, M2), NM2);
-        if (NDIG == 4)  // |s| may exceed 2^22: s + MAGIC is not exact, add it to r
-          rp2[i] = f2_add(f2_fma(q2, np, s2), M2);
-        else
+        // |s| may exceed 2^22 with four digits (s + MAGIC is not exact): r
+        // first, then MAGIC + r; both exact. Otherwise one operation fewer.
+        if (NDIG == 4 || (MODE == 2 && i >= H)) {
+          const unsigned long long r2 = f2_fma(q2, np, s2);
+          rp2[i] = f2_add(r2, M2);
+          if (MODE == 2 && i >= H) ri2[i - H] = r2;
+        } else {
           rp2[i] = f2_fma(q2, np, f2_add(s2, M2));
+        }
       }
     }
     float r[EL];
 #pragma unroll
     for (int i = 0; i < EL / 2; ++i) f2_unpack(rp2[i], r[2 * i], r[2 * i + 1]);
     uint32_t wu[W];
-    if (mode == 0) {
+    if constexpr (MODE == 0) {
 #pragma unroll
       for (int q = 0; q < W; ++q)
         wu[q] = pack4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
@@ -417,17 +431,17 @@ __global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
         *reinterpret_cast<uint2*>(out) = make_uint2(wu[0], wu[1]);
     } else {
       // rp2[h] = MAGIC + residues of (re_2h, re_2h+1), rp2[H + h] those of the
-      // imaginary parts. Third plane: t = r(re) + s_sum r(im) (|t| < 2^16):
-      // MAGIC + t exactly in one FMA, t, its nearest quotient by p and
-      // MAGIC + (t - q p) = (MAGIC + t) - q p (for p = 256 the residues are
-      // unreduced low bytes and the reduction gives the low byte of the sum)
-      constexpr int H = EL / 4;  // pairs of complex elements
+      // imaginary parts (ri2[h] without MAGIC). Third plane: t = r(re) +
+      // s_sum r(im) (|t| < 2^16): MAGIC + t exactly in one FMA, t, its nearest
+      // quotient by p and MAGIC + (t - q p) = (MAGIC + t) - q p (for p = 256
+      // the residues are unreduced low bytes and the reduction gives the low
+      // byte of the sum)
       const unsigned long long np = sc.neg_p[t], ip = sc.inv_p[t];
       const unsigned long long S2 = f2_pack(float(s_sum), float(s_sum));
       unsigned long long sm2[H];
 #pragma unroll
       for (int h = 0; h < H; ++h) {
-        const unsigned long long tM = f2_fma(S2, f2_add(rp2[H + h], NM2), rp2[h]);
+        const unsigned long long tM = f2_fma(S2, ri2[h], rp2[h]);
         const unsigned long long t2 = f2_add(tM, NM2);
         const unsigned long long q2 = f2_add(f2_fma(t2, ip, M2), NM2);
         sm2[h] = f2_fma(q2, np, tM);
@@ -1657,27 +1671,27 @@ bool slice_unroll() {
   return on;
 }
 
-template <typename TIn, bool VEC, int EL>
+template <typename TIn, bool VEC, int EL, int MODE>
 void launch_slice_el(int ndig, unsigned grid, cudaStream_t st, const TIn* X, int64_t ld,
-                     int64_t len, int rows, int64_t kp, const int* sig, int mode, int s_sign,
-                     int8_t* res, int64_t stride, const oz::SliceConsts& sc, int t0, int t1) {
+                     int64_t len, int rows, int64_t kp, const int* sig, int s_sign, int8_t* res,
+                     int64_t stride, const oz::SliceConsts& sc, int t0, int t1) {
   using namespace oz;
   constexpr int kNU = sizeof(TIn) == 8 ? kDefaultModuli : kDefaultModuliFloat;
   constexpr int kDigU = sizeof(TIn) == 8 ? 4 : 3;  // digits of the default scaling
   if (t0 == 0 && t1 == kNU && sc.n == kNU && ndig == kDigU && slice_unroll()) {
-    oz_slice<TIn, VEC, kDigU, EL, kNU><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode,
-                                                              s_sign, res, stride, sc, t0, t1);
+    oz_slice<TIn, VEC, kDigU, EL, kNU, MODE>
+        <<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1);
     return;
   }
   if (ndig <= 3)
-    oz_slice<TIn, VEC, 3, EL, 0><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign,
-                                                        res, stride, sc, t0, t1);
+    oz_slice<TIn, VEC, 3, EL, 0, MODE>
+        <<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1);
   else if (ndig == 4)
-    oz_slice<TIn, VEC, 4, EL, 0><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign,
-                                                        res, stride, sc, t0, t1);
+    oz_slice<TIn, VEC, 4, EL, 0, MODE>
+        <<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1);
   else
-    oz_slice<TIn, VEC, 5, EL, 0><<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, mode, s_sign,
-                                                        res, stride, sc, t0, t1);
+    oz_slice<TIn, VEC, 5, EL, 0, MODE>
+        <<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1);
 }
 
 template <typename TIn, bool VEC>
@@ -1687,12 +1701,21 @@ void launch_slice(int ndig, cudaStream_t st, const TIn* X, int64_t ld, int64_t l
   const int el = slice_elems();
   const int64_t kreal = mode == 2 ? 2 * kp : kp;  // reals per row a thread group covers
   const unsigned grid = unsigned((int64_t(rows) * (kreal / el) + 255) / 256);
-  if (el == 16)
-    launch_slice_el<TIn, VEC, 16>(ndig, grid, st, X, ld, len, rows, kp, sig, mode, s_sign, res,
-                                  stride, sc, t0, t1);
-  else
-    launch_slice_el<TIn, VEC, 8>(ndig, grid, st, X, ld, len, rows, kp, sig, mode, s_sign, res,
-                                 stride, sc, t0, t1);
+  auto run = [&](auto el_tag, auto mode_tag) {
+    launch_slice_el<TIn, VEC, decltype(el_tag)::value, decltype(mode_tag)::value>(
+        ndig, grid, st, X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1);
+  };
+  using E8 = std::integral_constant<int, 8>;
+  using E16 = std::integral_constant<int, 16>;
+  using M0 = std::integral_constant<int, 0>;
+  using M2 = std::integral_constant<int, 2>;
+  if (el == 16) {
+    if (mode == 2) run(E16{}, M2{});
+    else run(E16{}, M0{});
+  } else {
+    if (mode == 2) run(E8{}, M2{});
+    else run(E8{}, M0{});
+  }
 }
 
 // Row scale exponents of A (which & 1) and B (which & 2).
