@@ -79,14 +79,19 @@ constexpr uint32_t kIdescI8 = (2u << 4)              // D format S32
                               | (uint32_t(BN >> 3) << 17)  // N / 8
                               | (uint32_t(BM >> 4) << 24); // M / 16
 
-__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                        uint32_t accumulate) {
+// the same with an explicit instruction descriptor
+__device__ __forceinline__ void umma_i8_desc(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                             uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(kIdescI8), "r"(accumulate)
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
+}
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t accumulate) {
+  umma_i8_desc(tmem_d, adesc, bdesc, kIdescI8, accumulate);
 }
 
 
@@ -840,6 +845,7 @@ struct Unit {
   int t, c, tm, tn;
 };
 
+
 // Tile raster within one (product, k-chunk): bands of kBandTiles row tiles,
 // row tiles fastest within a band. The units in flight at one time cover a
 // few row tiles of A and a few column tiles of B, so that each A tile is
@@ -1555,6 +1561,270 @@ inline int staged_smem_bytes(bool cplx, int nmod) {
 }
 
 // --------------------------------------------------------------------------
+// 4b. CRT reconstruction on the tensor cores (byte residues, m % 16 == 0)
+//
+// By linearity the CRT sum needs no reduction of the product combination:
+// with V_k the weight of product plane k, W_t for the plane's modulus t where
+// the product enters Re or Im with a plus sign and P - W_t where it enters
+// with a minus (Re = P0 -+ P1, Im = P2 - P0 -+ P1, see combine3; p_t W_t = 0
+// mod P), S = sum_k r_k V_k is congruent mod P to the sum the CUDA-core
+// kernels form. Written in the bytes of V_k, S = sum_j 256^j S_j with
+// S_j = sum_k r_k byte_j(V_k), and for 128 consecutive rows of one column of
+// C one tcgen05.mma kind::i8 (unsigned bytes, exact INT32 sums below 2^22)
+//   D[128 x NO] = R[128 x KP] . V[KP x NO]
+// forms all of them: R is the tile's residue bytes as TMA loads them (one
+// 128-byte row per product plane: the MN-major operand layout), V the
+// weight bytes (K-major, columns 0-15 for Re, 16-31 for Im). The epilogue
+// (one TMEM lane per row of C) combines its 16 sums per part into the four
+// 32-bit limb sums of S and finishes with crt_from_limbs, as the CUDA-core
+// kernels do: the results are the same doubles.
+//
+// Warp 0: TMA producer (4-stage ring), warp 1: TMEM allocation and MMA issue
+// (accumulators double-buffered), warps 2-5: epilogue. Every wait is bounded;
+// a give-up sets *status.
+constexpr int RT_THREADS = 192;
+constexpr int RT_STAGES = 4;
+constexpr int RT_KP = 64;                     // planes per tile (K), padded
+constexpr int RT_STAGE = 128 * RT_KP;         // bytes per stage
+constexpr int RT_W_BYTES = 32 * 128;          // weights: 32 rows x 128 B (SW128)
+constexpr int RT_SMEM = RT_STAGES * RT_STAGE + RT_W_BYTES + 256 + 1024;
+
+struct ReconTcParams {
+  int m, n;
+  int row_blocks;         // ceil(m / 128)
+  long long total_units;  // row_blocks * n
+  int planes;             // product planes of the residue array (loaded per tile)
+  int kp;                 // K of the MMA: 32 or 64 (planes past `planes` are zero rows)
+  const int* sigA;
+  const int* sigB;
+  void* C;
+  int64_t ldc;
+  double alr, ali, ber, bei;
+  int fill;
+  int64_t ro, co;
+  int tile_m, tile_n;
+  ReconParams rp;
+  unsigned char v[32][RT_KP];  // weight bytes: v[o][k] = byte (o % 16) of V_k for part o / 16
+  int* status;
+  unsigned long long wait_limit_ns;
+};
+
+// UMMA shared-memory descriptor of an MN-major operand in the 128-byte
+// swizzle layout: 8-row atoms of 128 bytes along M (one atom covers the 128
+// rows of the tile), atoms 1024 B apart along K.
+__device__ __forceinline__ uint64_t umma_desc_sw128_mn(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= uint64_t((saddr >> 4) & 0x3FFFu);  // start address
+  d |= uint64_t(1) << 16;                  // leading byte offset (one atom along M: unused)
+  d |= uint64_t(1024 >> 4) << 32;          // stride byte offset: 8 K-rows x 128 B
+  d |= uint64_t(1) << 46;                  // descriptor version (sm_100)
+  d |= uint64_t(2) << 61;                  // layout: 128-byte swizzle
+  return d;
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            int z, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
+template <int DT>
+__global__ void __launch_bounds__(RT_THREADS, 5)
+    oz_reconstruct_tc(const __grid_constant__ CUtensorMap tmR,
+                      const __grid_constant__ ReconTcParams P) {
+  constexpr bool CPLX = dtype_is_complex(DT);
+  constexpr int NO = CPLX ? 32 : 16;  // output columns of the MMA
+  // D S32, A and B unsigned int8, A MN-major, B K-major, N = NO, M = 128
+  constexpr uint32_t kIdesc = (2u << 4) | (1u << 15) | (uint32_t(NO >> 3) << 17) |
+                              (uint32_t(128 >> 4) << 24);
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw_addr = smem_u32(smem_raw);
+  const uint32_t base = (raw_addr + 1023u) & ~1023u;
+  unsigned char* base_ptr = smem_raw + (base - raw_addr);
+  const uint32_t w_addr = base + RT_STAGES * RT_STAGE;
+  const uint32_t bar_base = w_addr + RT_W_BYTES;
+  auto full_bar = [&](int s) { return bar_base + 8u * s; };
+  auto empty_bar = [&](int s) { return bar_base + 8u * (RT_STAGES + s); };
+  auto accf_bar = [&](int b) { return bar_base + 8u * (2 * RT_STAGES + b); };
+  auto acce_bar = [&](int b) { return bar_base + 8u * (2 * RT_STAGES + 2 + b); };
+  const uint32_t drain_bar = bar_base + 8u * (2 * RT_STAGES + 4);
+  unsigned char* ctl = base_ptr + RT_STAGES * RT_STAGE + RT_W_BYTES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ctl + 8 * (2 * RT_STAGES + 5));
+  volatile int* abort = reinterpret_cast<volatile int*>(ctl + 8 * (2 * RT_STAGES + 5) + 8);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  // weight bytes into the K-major 128-byte-swizzled B tile (row o, K byte k),
+  // and zeros into the plane rows planes .. kp-1 of every stage (TMA writes
+  // rows 0 .. planes-1 only)
+  {
+    unsigned char* wp = base_ptr + RT_STAGES * RT_STAGE;
+    for (int idx = threadIdx.x; idx < RT_W_BYTES; idx += RT_THREADS) {
+      const int o = idx >> 7, k = idx & 127;
+      const unsigned char b = (o < NO && k < P.kp) ? P.v[o][k] : 0;
+      wp[(o >> 3) * 1024 + (o & 7) * 128 + (((k >> 4) ^ (o & 7)) << 4) + (k & 15)] = b;
+    }
+    const int pad = (P.kp - P.planes) * 128;  // bytes per stage, 16-byte words below
+    for (int idx = threadIdx.x; idx < RT_STAGES * (pad / 16); idx += RT_THREADS) {
+      const int st = idx / (pad / 16), w16 = idx - st * (pad / 16);
+      *reinterpret_cast<uint4*>(base_ptr + st * RT_STAGE + P.planes * 128 + 16 * w16) =
+          make_uint4(0u, 0u, 0u, 0u);
+    }
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < RT_STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf_bar(b), 1);
+      mbar_init(acce_bar(b), 4);
+    }
+    mbar_init(drain_bar, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // the tensor cores read the weights through the async proxy
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(
+                     smem_u32(tmem_slot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const uint32_t tile_bytes = uint32_t(128 * P.planes);
+  bool copies_pending = false;  // the producer gave up with copies possibly in flight
+
+  // unit u = (row block rb, column j), u = rb + j row_blocks: every role walks
+  // u = blockIdx.x, + gridDim.x, ... with (rb, j) advanced without division
+  const int drb = int(gridDim.x % unsigned(P.row_blocks));
+  const int dj = int(gridDim.x / unsigned(P.row_blocks));
+  auto next_unit = [&](int& rb, int& j) {
+    rb += drb;
+    j += dj;
+    if (rb >= P.row_blocks) {
+      rb -= P.row_blocks;
+      ++j;
+    }
+  };
+  const int rb0 = int(blockIdx.x % unsigned(P.row_blocks));
+  const int j0 = int(blockIdx.x / unsigned(P.row_blocks));
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer: the tile's planes, 128 residue bytes each
+    int rb = rb0, j = j0;
+    for (long long u = blockIdx.x, it = 0; u < P.total_units;
+         u += gridDim.x, ++it, next_unit(rb, j)) {
+      const int stage = int(it % RT_STAGES);
+      const uint32_t phase = uint32_t((it / RT_STAGES) & 1);
+      if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort, P.wait_limit_ns)) {
+        copies_pending = true;
+        break;
+      }
+      mbar_arrive_expect_tx(full_bar(stage), tile_bytes);
+      tma_load_3d(base + stage * RT_STAGE, &tmR, rb * 128, j, 0, full_bar(stage));
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer
+    bool ok = true;
+    for (long long u = blockIdx.x, it = 0; u < P.total_units; u += gridDim.x, ++it) {
+      const int stage = int(it % RT_STAGES);
+      const uint32_t phase = uint32_t((it / RT_STAGES) & 1);
+      const int b = int(it & 1);
+      const uint32_t bpar = uint32_t((it >> 1) & 1);
+      if (!mbar_wait(acce_bar(b), bpar ^ 1u, abort, P.wait_limit_ns) ||
+          !mbar_wait(full_bar(stage), phase, abort, P.wait_limit_ns)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t sa = base + stage * RT_STAGE;
+      for (int kb = 0; kb < P.kp / 32; ++kb)
+        umma_i8_desc(tmem_base + uint32_t(b * 32), umma_desc_sw128_mn(sa + kb * 4096),
+                     umma_desc_sw128(w_addr + kb * 32), kIdesc, kb > 0 ? 1u : 0u);
+      umma_commit(empty_bar(stage));
+      umma_commit(accf_bar(b));
+    }
+    if (!ok) {
+      umma_commit(drain_bar);  // MMAs may be in flight: wait (bounded) until they retire
+      const unsigned long long t0 = globaltimer();
+      while (!mbar_try_wait(drain_bar, 0) && globaltimer() - t0 < 1000000ull) {
+      }
+    }
+  } else if (warp >= 2) {
+    // ---- epilogue: lane quarter (warp % 4), one row of C per lane
+    const int quarter = warp & 3;
+    const bool read_c = (P.ber != 0.0 || P.bei != 0.0);
+    const uint32_t lane_taddr = tmem_base + (uint32_t(quarter * 32) << 16);
+    int rb = rb0, j = j0;
+    for (long long u = blockIdx.x, it = 0; u < P.total_units;
+         u += gridDim.x, ++it, next_unit(rb, j)) {
+      const int b = int(it & 1);
+      const uint32_t bpar = uint32_t((it >> 1) & 1);
+      const int i = rb * 128 + quarter * 32 + lane;
+      // the scale exponents load while the accumulator is awaited
+      const int si = i < P.m ? P.sigA[i] : 0;
+      const int tauj = P.sigB[j];
+      if (!mbar_wait(accf_bar(b), bpar, abort, P.wait_limit_ns)) break;
+      tc_fence_after();
+      __syncwarp();
+      uint32_t v[32];
+      tmem_ld32(lane_taddr + uint32_t(b * 32), v);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce_bar(b));  // the accumulator may be overwritten
+      bool active = i < P.m;
+      if (active && P.fill != 0) {
+        const int64_t ti = (i / P.tile_m) * int64_t(P.tile_m);
+        const int64_t tj = (j / P.tile_n) * int64_t(P.tile_n);
+        active = tile_is_active(P.fill, ti, tj, ::min((int64_t)P.tile_m, (int64_t)P.m - ti),
+                                ::min((int64_t)P.tile_n, (int64_t)P.n - tj), P.ro, P.co);
+      }
+      if (active) {
+        // limb L of S = sum of S_j 2^(8 (j - 4L)) over j = 4L .. 4L + 3 (below
+        // 2^47): two 32-bit shift-adds (each below 2^31) and one wide multiply-add
+        auto limb = [&](int j0) {
+          const uint32_t a = v[j0] + (v[j0 + 1] << 8);
+          const uint32_t b = v[j0 + 2] + (v[j0 + 3] << 8);
+          return (unsigned long long)b * 65536ull + a;
+        };
+        const int e = -(si + tauj);
+        double xr =
+            scale_pow2(crt_from_limbs<true>(limb(0), limb(4), limb(8), limb(12), P.rp), e);
+        double xi = 0.0;
+        if (CPLX)
+          xi = scale_pow2(crt_from_limbs<true>(limb(16), limb(20), limb(24), limb(28), P.rp), e);
+        if (si == kSigmaNonFinite || tauj == kSigmaNonFinite)
+          xr = xi = __longlong_as_double(kNaNBits);
+        store_c<DT>(P.C, i + int64_t(j) * P.ldc, xr, xi, P.alr, P.ali, P.ber, P.bei, read_c);
+      }
+    }
+  }
+
+  if (copies_pending) {
+    // copies issued by this CTA may still be landing in shared memory
+    const unsigned long long t0 = globaltimer();
+    while (globaltimer() - t0 < 2000000ull) {
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (*abort && threadIdx.x == 0) atomicExch(P.status, 1);
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem_base)
+                 : "memory");
+  }
+}
+
+// --------------------------------------------------------------------------
 // host orchestration
 
 struct Layout {
@@ -1627,6 +1897,23 @@ bool make_map(CUtensorMap* map, void* base, int64_t kp, int64_t rows, int box_ro
   cuuint32_t box[2] = {cuuint32_t(BKB), cuuint32_t(box_rows)};
   cuuint32_t estr[2] = {1, 1};
   const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// Residue bytes of C for the tensor-core reconstruction: dims (m, nb, planes)
+// with strides (m, nb m) bytes (m % 16 == 0, m >= 128), boxes of 128 rows x 1
+// column x all planes (rows past m read as zeros), 128-byte swizzle: one
+// 128-byte row per plane, the MN-major operand layout.
+bool make_map_recon(CUtensorMap* map, void* base, int m, int nb, int planes) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {cuuint64_t(m), cuuint64_t(nb), cuuint64_t(planes)};
+  cuuint64_t strides[2] = {cuuint64_t(m), cuuint64_t(int64_t(nb) * m)};
+  cuuint32_t box[3] = {128u, 1u, cuuint32_t(planes)};
+  cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
@@ -1912,6 +2199,94 @@ int modulus_groups(const oz::Layout& L) {
 }  // namespace
 
 namespace {
+// Tensor-core CRT reconstruction (oz_reconstruct_tc), the default for byte
+// residues (one k-chunk) with m % 16 == 0, m >= 128 and at most 64 product
+// planes; SPLAB_OZAKI_RECON_TC=0 (read per call) selects the CUDA-core
+// kernels. True when it applies and its tensor map was made.
+bool recon_tc_plan(const oz::Layout& L, unsigned char* R8, CUtensorMap* map) {
+  using namespace oz;
+  const char* v = std::getenv("SPLAB_OZAKI_RECON_TC");
+  if ((v && v[0] == '0') || !R8 || L.nmod * L.nsub > RT_KP || L.rowsA % 16 != 0 ||
+      L.rowsA < 128)
+    return false;
+  return make_map_recon(map, R8, L.rowsA, L.nb, L.nmod * L.nsub);
+}
+
+cudaError_t launch_recon_tc(const GemmProblem& p, const oz::Layout& L, const oz::Crt& crt,
+                            const oz::ReconParams& rp, const CUtensorMap& map, const int* sigA,
+                            const int* sigB, int* status, cudaStream_t st) {
+  using namespace oz;
+  const bool cplx = dtype_is_complex(p.dtype);
+  const int planes = L.nmod * L.nsub;
+  static thread_local ReconTcParams P;  // 2.7 KB: kept off the stack
+  P = ReconTcParams{};
+  P.m = L.rowsA;
+  P.n = int(p.n);
+  P.row_blocks = (P.m + 127) / 128;
+  P.total_units = (long long)P.row_blocks * P.n;
+  P.planes = planes;
+  P.kp = planes <= 32 ? 32 : 64;
+  P.sigA = sigA;
+  P.sigB = sigB;
+  P.C = p.C;
+  P.ldc = p.ldc;
+  P.alr = p.alpha[0];
+  P.ali = p.alpha[1];
+  P.ber = p.beta[0];
+  P.bei = p.beta[1];
+  P.fill = p.fill_mode;
+  P.ro = p.fill_ro;
+  P.co = p.fill_co;
+  P.tile_m = BM;
+  P.tile_n = cplx ? BN / 2 : BN;
+  P.rp = rp;
+  // weight bytes: plane k = t * nsub + s takes W_t or P - W_t (the combination
+  // of combine3 with its signs carried by the weights)
+  const unsigned __int128 Pm = (unsigned __int128)crt.P_hi << 64 | crt.P_lo;
+  for (int t = 0; t < L.nmod; ++t) {
+    const unsigned __int128 W = (unsigned __int128)crt.w_hi[t] << 64 | crt.w_lo[t];
+    const unsigned __int128 Wn = Pm - W;
+    for (int s = 0; s < L.nsub; ++s) {
+      unsigned __int128 vre = W, vim = 0;
+      if (cplx) {
+        if (s == 0) {
+          vre = W;
+          vim = Wn;
+        } else if (s == 1) {
+          vre = rp.conj ? W : Wn;
+          vim = rp.conj ? W : Wn;
+        } else {
+          vre = 0;
+          vim = W;
+        }
+      }
+      const int k = t * L.nsub + s;
+      for (int o = 0; o < 16; ++o) {
+        P.v[o][k] = static_cast<unsigned char>(vre >> (8 * o));
+        P.v[16 + o][k] = static_cast<unsigned char>(vim >> (8 * o));
+      }
+    }
+  }
+  P.status = status;
+  P.wait_limit_ns = kWaitLimitNs;
+  auto run = [&](auto kern) -> cudaError_t {
+    const cudaError_t ea = set_dynamic_smem(reinterpret_cast<const void*>(kern), RT_SMEM);
+    if (ea != cudaSuccess) return ea;
+    // five CTAs per SM (their shared memory and TMEM fit; measured against
+    // three and four on the complex sbs problem m = 200000, n = k = 2048:
+    // 9.0 against 10.1 and 9.3 ms)
+    const long long grid = std::min<long long>(P.total_units, 5LL * sm_count());
+    kern<<<unsigned(grid), RT_THREADS, RT_SMEM, st>>>(map, P);
+    return cudaGetLastError();
+  };
+  switch (p.dtype) {
+    case kC64: return run(oz_reconstruct_tc<kC64>);
+    case kC32: return run(oz_reconstruct_tc<kC32>);
+    case kR64: return run(oz_reconstruct_tc<kR64>);
+    default: return run(oz_reconstruct_tc<kR32>);
+  }
+}
+
 // At <- A k-major (op(A) = N operands); see oz_transpose
 cudaError_t transpose_a(const GemmProblem& p, const oz::Layout& L, void* At, cudaStream_t st) {
   const dim3 block(32, 8);
@@ -1949,6 +2324,9 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
   int* R = reinterpret_cast<int*>(w + L.off_R);
   unsigned char* R8 = L.r8 ? reinterpret_cast<unsigned char*>(w + L.off_R) : nullptr;
   int* status = reinterpret_cast<int*>(w + L.off_status);
+  // byte residues of C, where they apply, go to the tensor-core reconstruction
+  CUtensorMap rmap;
+  const bool tc_recon = p_in.k > 0 && recon_tc_plan(L, R8, &rmap);
 
   cudaError_t e;
   // op(A) = N: everything below reads the k-major copy At as op(A) = T
@@ -2213,6 +2591,12 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
   const unsigned gy = unsigned(std::min<int64_t>(p.n, 65535));
   const unsigned gx = unsigned(std::max<int64_t>(1, (p.m + threads - 1) / threads));
   const bool fixed = L.nmod == (dtype_is_double(p.dtype) ? kDefaultModuli : kDefaultModuliFloat);
+  if (tc_recon) {
+    if ((e = launch_recon_tc(p, L, crt, rp, rmap, sigA, sigB, status, st)) != cudaSuccess)
+      return e;
+    phase_mark(2, true, st);
+    return cudaGetLastError();
+  }
   if (staged) {
     const int smem = staged_smem_bytes(cplx, L.nmod);
     const int64_t items = (p.m + kStageRows - 1) / kStageRows * p.n;

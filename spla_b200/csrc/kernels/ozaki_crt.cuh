@@ -149,6 +149,14 @@ __host__ __device__ __forceinline__ double u32_to_double(unsigned x) {
   return double(x);
 #endif
 }
+// The same for a signed integer of magnitude below 2^31 (offset by 2^31).
+__host__ __device__ __forceinline__ double i32_to_double(int x) {
+#ifdef __CUDA_ARCH__
+  return __hiloint2double(0x43300000, x ^ int(0x80000000u)) - 4503601774854144.0;
+#else
+  return double(x);
+#endif
+}
 __host__ __device__ __forceinline__ double u52_to_double(unsigned long long x) {
 #ifdef __CUDA_ARCH__
   return __longlong_as_double((long long)(x | 0x4330000000000000ull)) - 4503599627370496.0;
@@ -175,18 +183,16 @@ __host__ __device__ __forceinline__ double u52_to_double(unsigned long long x) {
 //
 // N: number of moduli (0: rp.n at run time). BYTES: residues below 2^10 (the
 // limb sums are then below 2^46 and convert exactly by the mantissa method).
-template <int N, bool BYTES>
-__host__ __device__ __forceinline__ double crt_value(const int* r, const ReconParams& rp) {
-  unsigned long long l0 = 0, l1 = 0, l2 = 0, l3 = 0;
-#pragma unroll
-  for (int t = 0; t < (N > 0 ? N : kMaxUsableModuli); ++t) {
-    if (N == 0 && t >= rp.n) break;
-    const unsigned rt = unsigned(r[t]);
-    l0 += (unsigned long long)rt * rp.w[t][0];
-    l1 += (unsigned long long)rt * rp.w[t][1];
-    l2 += (unsigned long long)rt * rp.w[t][2];
-    l3 += (unsigned long long)rt * rp.w[t][3];
-  }
+//
+// crt_from_limbs: the same from S given as limb sums, S = l0 + l1 2^32 +
+// l2 2^64 + l3 2^96 with every l below 2^62 (below 2^52 with BYTES), and
+// S / P below 2^14.
+template <bool BYTES>
+__host__ __device__ __forceinline__ double crt_from_limbs(unsigned long long l0,
+                                                          unsigned long long l1,
+                                                          unsigned long long l2,
+                                                          unsigned long long l3,
+                                                          const ReconParams& rp) {
   // q = round(S / P) from (l1 + l2 2^32 + l3 2^64) * 2^32 / P
   double s1, s2, s3;
   if (BYTES) {
@@ -214,9 +220,24 @@ __host__ __device__ __forceinline__ double crt_value(const int* r, const ReconPa
   c = (c >> 32) + (long long)(l2 - qq * rp.P[2]);
   const unsigned x2 = unsigned(c);
   c = (c >> 32) + (long long)(l3 - qq * rp.P[3]);  // |c| < 2^22
-  double v = fma(double(int(c)), 4294967296.0, u32_to_double(x2));
+  double v = fma(i32_to_double(int(c)), 4294967296.0, u32_to_double(x2));
   v = fma(v, 4294967296.0, u32_to_double(x1));
   return fma(v, 4294967296.0, u32_to_double(x0));
+}
+
+template <int N, bool BYTES>
+__host__ __device__ __forceinline__ double crt_value(const int* r, const ReconParams& rp) {
+  unsigned long long l0 = 0, l1 = 0, l2 = 0, l3 = 0;
+#pragma unroll
+  for (int t = 0; t < (N > 0 ? N : kMaxUsableModuli); ++t) {
+    if (N == 0 && t >= rp.n) break;
+    const unsigned rt = unsigned(r[t]);
+    l0 += (unsigned long long)rt * rp.w[t][0];
+    l1 += (unsigned long long)rt * rp.w[t][1];
+    l2 += (unsigned long long)rt * rp.w[t][2];
+    l3 += (unsigned long long)rt * rp.w[t][3];
+  }
+  return crt_from_limbs<BYTES>(l0, l1, l2, l3, rp);
 }
 
 }  // namespace oz

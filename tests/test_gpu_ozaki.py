@@ -388,3 +388,60 @@ def test_tensor_core_slicer_matches_fp32_slicer(m, n, k, opA, pad):
     torch.cuda.synchronize()
     ref = ((0.5 - 0.25j) * R.cpu().numpy() + 1.5 * C).reshape(n, m + pad)[:, :m]
     assert oracle.rel_fro(out[0].reshape(n, m + pad)[:, :m], ref) <= 1e-14
+
+
+@pytest.mark.parametrize("dt,m,n,k,opA,fill,moduli,nan", [
+    (np.complex128, 3088, 70, 500, 2, 0, 0, False),     # partial last block of 128 rows
+    (np.complex128, 400, 130, 3000, 1, 0, 0, False),    # A^T B: the other signs of Im
+    (np.complex128, 520, 520, 16500, 2, spla.FILL_MODE_LOWER, 0, False),
+    (np.complex128, 2064, 70, 500, 2, 0, 12, False),    # non-default modulus count
+    (np.complex128, 256, 200, 1000, 2, 0, 0, True),     # a NaN row of A and of B
+    (np.float64, 1040, 70, 500, 1, 0, 0, False),
+    (np.complex64, 2064, 70, 500, 2, 0, 0, False),
+    (np.float32, 1056, 70, 500, 1, 0, 0, False),
+    (np.complex128, 300, 150, 1000, 2, 0, 0, False),    # m % 16 != 0: plain kernel
+    (np.float32, 77, 50, 500, 1, 0, 0, False),          # m below one block of 128 rows
+])
+def test_tensor_core_reconstruction_matches_staged(dt, m, n, k, opA, fill, moduli, nan):
+    """Byte residues (one k-chunk) with m % 16 == 0 and m >= 128 are
+    reconstructed with the CRT sums on the INT8 tensor cores
+    (oz_reconstruct_tc); SPLAB_OZAKI_RECON_TC=0 selects the staged CUDA-core
+    kernel (the last two cases take the plain kernel either way). Both reduce
+    the same congruence class to the same limbs, so C is bit-identical (bytes
+    compared, NaN included); both are also checked against the oracle."""
+    import torch
+    cplx = np.dtype(dt).kind == "c"
+    alpha, beta = ((0.5 + 0.25j), (-1.0 + 0.5j)) if cplx else (0.5, -1.0)
+    A = buffer(dt, k, m, 41, "gauss_k", k)
+    B = buffer(dt, k, n, 42, "gauss_k", k)
+    if nan:
+        A[k * 7 + 3] = np.nan
+        B[k * 5 + 1] = np.nan
+    C = buffer(dt, m, n, 43, "uniform11")
+    d = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128, 128)
+    out = []
+    for tc in ("1", "0"):
+        os.environ["SPLAB_OZAKI_RECON_TC"] = tc
+        try:
+            ctx = spla.Context(spla.PU_GPU)
+            ctx.set_fp64_path(spla.PATH_OZAKI, moduli)
+            dC = _dev(C)
+            spla.pgemm_ssbtr(m, n, k, opA, alpha, _dev(A), k, _dev(B), k, beta, dC, m, 0, 0,
+                             fill, d, ctx)
+            torch.cuda.synchronize()
+            out.append(dC.cpu().numpy())
+        finally:
+            os.environ.pop("SPLAB_OZAKI_RECON_TC", None)
+    assert np.array_equal(out[0].view(np.uint8), out[1].view(np.uint8))
+    ref = C.copy()
+    assert oracle.pgemm_ssb(m, n, k, opA, alpha, A, k, B, k, beta, ref, m, 0, 0) == 0
+    g, r = out[0].reshape(n, m).T, ref.reshape(n, m).T
+    sel = np.tril(np.ones((m, n), bool)) if fill else np.ones((m, n), bool)
+    if nan:
+        bad = np.zeros((m, n), bool)
+        bad[7, :] = True
+        bad[:, 5] = True
+        assert np.isnan(g[bad]).all()
+        sel &= ~bad
+    tol = 1e-9 if moduli else (1e-14 if np.dtype(dt).itemsize >= 16 or dt == np.float64 else 1e-6)
+    assert oracle.rel_fro(g[sel], r[sel]) <= tol
