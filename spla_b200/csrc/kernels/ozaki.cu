@@ -307,63 +307,23 @@ __device__ __forceinline__ uint32_t pack4(float a, float b, float c, float d) {
 }
 
 
-// Residues of one operand, written K-major (row stride kp bytes).
-// Each thread handles EL (8 or 16) consecutive reals of one row.
-// mode 0: real rows: res[t][row][l], l < kp.
-// mode 2: complex rows for the three-product (Karatsuba) form: complex element
-//         e = (re, im) of row `row` goes to three planes of `rows` x kp bytes,
-//         res[t][0][row][e] = r(re), res[t][1][row][e] = r(im) and
-//         res[t][2][row][e] = r(re + s_sum im) (residues are linear in the
-//         scaled integers, so the third is r(re) + s_sum r(im) reduced mod p).
-//         The input row then holds 2 kp reals (kp complex elements).
-// TIn: double (|x| < 2^62, five digits) or float (|x| < 2^38, three digits).
-// NMU > 0: moduli 0 .. NMU-1 in one fully unrolled pass (the per-modulus
-// constants become fixed parameter operands); 0: t_begin .. t_end-1 in a loop.
-// MODE (0 or 2, the mode above) is a template parameter so that the unrolled
-// modulus loop carries no branch on it.
-template <typename TIn, bool VEC, int NDIG, int EL, int NMU, int MODE>
-__global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
-    oz_slice(const TIn* __restrict__ X, int64_t ld_doubles, int64_t len, int rows, int64_t kp,
-             const int* __restrict__ sigma, int s_sum, int8_t* __restrict__ res,
-             int64_t res_mod_stride, SliceConsts sc, int t_begin, int t_end) {
+// The work of one slicing thread once its EL reals (of one row, starting at
+// real l0) are loaded: scaling by 2^sg, digits, and for every modulus the
+// residues written to res_row + l0 (mode 0) or, in mode 2, to the three
+// planes `plane` bytes apart at complex offset l0 / 2.
+template <typename TIn, int NDIG, int EL, int NMU, int MODE>
+__device__ __forceinline__ void slice_thread(double (&v)[EL], int sg, int8_t* res_row,
+                                             int64_t l0, int64_t plane, int s_sum,
+                                             int64_t res_mod_stride, const SliceConsts& sc,
+                                             int t_begin, int t_end) {
   static_assert(EL == 8 || EL == 16, "8 or 16 reals per thread");
   static_assert(MODE == 0 || MODE == 2, "real rows or complex rows");
   constexpr int W = EL / 4;  // packed words per modulus
-  const int64_t groups = (MODE == 2 ? 2 * kp : kp) / EL;
-  const int64_t gid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  const int row = int(gid / groups);
-  if (row >= rows) return;
-  const int64_t l0 = (gid % groups) * EL;
-  const TIn* x = X + int64_t(row) * ld_doubles + l0;
-  const int sg = sigma[row];
   // 2^sg as a double when representable, else ldexp per element
   const bool direct = sg > -1000 && sg < 1000;
   const double scale = direct ? __longlong_as_double((long long)(sg + 1023) << 52) : 1.0;
   unsigned long long dp[EL / 2][5];  // digits of the element pairs (see below)
   {
-    double v[EL];
-    if (VEC && l0 + EL <= len) {
-      if constexpr (sizeof(TIn) == 8) {
-#pragma unroll
-        for (int i = 0; i < EL / 2; ++i) {
-          const double2 t = __ldg(reinterpret_cast<const double2*>(x) + i);
-          v[2 * i] = t.x;
-          v[2 * i + 1] = t.y;
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < EL / 4; ++i) {
-          const float4 t = __ldg(reinterpret_cast<const float4*>(x) + i);
-          v[4 * i] = t.x;
-          v[4 * i + 1] = t.y;
-          v[4 * i + 2] = t.z;
-          v[4 * i + 3] = t.w;
-        }
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < EL; ++i) v[i] = (l0 + i < len) ? double(x[i]) : 0.0;
-    }
     // pairs (2i, 2i + 1) in mode 0; in mode 2 the real parts pair up first,
     // then the imaginary parts: (re0, re1), (re2, re3), ..., (im0, im1), ...
     if constexpr (MODE == 2) {
@@ -386,8 +346,7 @@ __global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
     }
   }
   const unsigned long long M2 = f2_pack(kMagic, kMagic), NM2 = f2_pack(-kMagic, -kMagic);
-  const unsigned long long NEG1 = f2_pack(-1.0f, -1.0f), TWO_M2 = f2_pack(2 * kMagic, 2 * kMagic);
-  int8_t* const out0 = res + int64_t(row) * kp + l0;
+  int8_t* const out0 = res_row + l0;
   auto modulus = [&](const int t) {
     int8_t* out = out0 + t * res_mod_stride;
     constexpr int H = EL / 4;        // mode 2: pairs of complex elements
@@ -451,7 +410,6 @@ __global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
         const unsigned long long q2 = f2_add(f2_fma(t2, ip, M2), NM2);
         sm2[h] = f2_fma(q2, np, tM);
       }
-      const int64_t plane = int64_t(rows) * kp;
       int8_t* o = out0 - l0 + l0 / 2 + t * res_mod_stride;  // complex offset l0 / 2
 #pragma unroll
       for (int w = 0; w < H / 2; ++w) {
@@ -474,6 +432,211 @@ __global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
   } else {
     for (int t = t_begin; t < t_end; ++t) modulus(t);
   }
+}
+
+// Residues of one operand, written K-major (row stride kp bytes).
+// Each thread handles EL (8 or 16) consecutive reals of one row.
+// mode 0: real rows: res[t][row][l], l < kp.
+// mode 2: complex rows for the three-product (Karatsuba) form: complex element
+//         e = (re, im) of row `row` goes to three planes of `rows` x kp bytes,
+//         res[t][0][row][e] = r(re), res[t][1][row][e] = r(im) and
+//         res[t][2][row][e] = r(re + s_sum im) (residues are linear in the
+//         scaled integers, so the third is r(re) + s_sum r(im) reduced mod p).
+//         The input row then holds 2 kp reals (kp complex elements).
+// TIn: double (|x| < 2^62, five digits) or float (|x| < 2^38, three digits).
+// NMU > 0: moduli 0 .. NMU-1 in one fully unrolled pass (the per-modulus
+// constants become fixed parameter operands); 0: t_begin .. t_end-1 in a loop.
+// MODE (0 or 2, the mode above) is a template parameter so that the unrolled
+// modulus loop carries no branch on it.
+template <typename TIn, bool VEC, int NDIG, int EL, int NMU, int MODE>
+__global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
+    oz_slice(const TIn* __restrict__ X, int64_t ld_doubles, int64_t len, int rows, int64_t kp,
+             const int* __restrict__ sigma, int s_sum, int8_t* __restrict__ res,
+             int64_t res_mod_stride, SliceConsts sc, int t_begin, int t_end) {
+  const int64_t groups = (MODE == 2 ? 2 * kp : kp) / EL;
+  const int64_t gid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int row = int(gid / groups);
+  if (row >= rows) return;
+  const int64_t l0 = (gid % groups) * EL;
+  const TIn* x = X + int64_t(row) * ld_doubles + l0;
+  double v[EL];
+  if (VEC && l0 + EL <= len) {
+    if constexpr (sizeof(TIn) == 8) {
+#pragma unroll
+      for (int i = 0; i < EL / 2; ++i) {
+        const double2 t = __ldg(reinterpret_cast<const double2*>(x) + i);
+        v[2 * i] = t.x;
+        v[2 * i + 1] = t.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < EL / 4; ++i) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(x) + i);
+        v[4 * i] = t.x;
+        v[4 * i + 1] = t.y;
+        v[4 * i + 2] = t.z;
+        v[4 * i + 3] = t.w;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < EL; ++i) v[i] = (l0 + i < len) ? double(x[i]) : 0.0;
+  }
+  slice_thread<TIn, NDIG, EL, NMU, MODE>(v, sigma[row], res + int64_t(row) * kp, l0,
+                                         int64_t(rows) * kp, s_sum, res_mod_stride, sc, t_begin,
+                                         t_end);
+}
+
+// --------------------------------------------------------------------------
+// 2a. op(A) = N operands with many rows, read in place: A is m-major (element
+// (i, kk) at X[i + kk ld], the rows of op(A) are the columns of X), and
+// instead of a k-major copy the norms read it along i and the slicer
+// transposes tiles through shared memory.
+constexpr int kMnRows = 65536;  // rows from which op(A) = N is read in place
+
+// Row scale exponents of m-major rows, as oz_row_scale computes them: one
+// thread per row (a warp reads 32 consecutive rows of one kk: coalesced),
+// batches of 8 loads in flight.
+template <typename TIn, bool CPLX>
+__global__ void __launch_bounds__(256) oz_row_scale_mn(const TIn* __restrict__ X, int64_t ld,
+                                                       int m, int64_t k, int q_bits,
+                                                       int* __restrict__ sigma) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  constexpr int R = CPLX ? 2 : 1;  // reals per element
+  const TIn* x = X + int64_t(i) * R;
+  const int64_t step = ld * R;  // reals between consecutive kk
+  double S = 0.0, inv = 0.0;
+  int E = -2100;
+  int64_t kk = 0;
+  for (; kk + 8 <= k; kk += 8) {
+    double v[8 * R];
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+#pragma unroll
+      for (int c = 0; c < R; ++c) v[b * R + c] = double(x[(kk + b) * step + c]);
+    int em = exponent_of(v[0]);
+#pragma unroll
+    for (int b = 1; b < 8 * R; ++b) em = max(em, exponent_of(v[b]));
+    if (em > E) {
+      S = ldexp(S, 2 * (E - em));
+      E = em;
+      inv = ldexp(1.0, -E);
+    }
+#pragma unroll
+    for (int b = 0; b < 8 * R; ++b) {
+      const double w = v[b] * inv;
+      S = fma(w, w, S);
+    }
+  }
+  for (; kk < k; ++kk) {
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      const double v = double(x[kk * step + c]);
+      const int ev = exponent_of(v);
+      if (ev > E) {
+        S = ldexp(S, 2 * (E - ev));
+        E = ev;
+        inv = ldexp(1.0, -E);
+      }
+      const double w = v * inv;
+      S = fma(w, w, S);
+    }
+  }
+  if (!(S < 1e300)) {  // NaN or infinite input
+    sigma[i] = kSigmaNonFinite;
+  } else if (S > 0.0) {
+    int e0 = 0;
+    frexp(sqrt(S), &e0);
+    sigma[i] = q_bits - (e0 + E);
+  } else {
+    sigma[i] = 0;
+  }
+}
+
+// Raw element of ESZ bytes (a complex or real value of TIn) in shared memory
+template <int ESZ> struct RawElem;
+template <> struct RawElem<16> { using T = double2; };
+template <> struct RawElem<8> { using T = unsigned long long; };
+template <> struct RawElem<4> { using T = unsigned int; };
+
+// Residues of m-major rows: a block covers 8 rows (one warp each) and, per row,
+// the KT = 32 G elements of one warp row (G = EL / reals per element: 4
+// complex or 8 real). The tile is read along i (8 consecutive rows per kk) into
+// shared memory and read back along kk; the element index is XOR-swizzled
+// within groups of 128 bytes and the row stride is odd, so that the reads are
+// free of bank conflicts (the writes at most 2-way, 4-way for real float).
+// Each thread then does oz_slice's work (slice_thread) on its EL = 8 reals.
+// VEC: 16-byte loads of complex double elements (the base is 16-byte aligned).
+template <typename TIn, bool VEC, int NDIG, int NMU, int MODE>
+__global__ void __launch_bounds__(256, 4)
+    oz_slice_mn(const TIn* __restrict__ X, int64_t ld, int m, int64_t k, int64_t kp,
+                const int* __restrict__ sigma, int s_sum, int8_t* __restrict__ res,
+                int64_t res_mod_stride, SliceConsts sc, int t_begin, int t_end) {
+  constexpr int EL = 8;
+  constexpr int R = MODE == 2 ? 2 : 1;  // reals per element
+  constexpr int G = EL / R;             // elements per thread
+  constexpr int KT = 32 * G;            // elements per row per tile
+  constexpr int ESZ = R * int(sizeof(TIn));
+  constexpr int GROUPS = 128 / ESZ;     // elements per 128 bytes of shared memory
+  constexpr int RSTR = KT + 1;          // row stride in elements (odd)
+  using T = typename RawElem<ESZ>::T;
+  __shared__ T tile[8 * RSTR];
+  auto swz = [](int kk) { return kk ^ ((kk / G) & (GROUPS - 1)); };
+  const int i0 = blockIdx.x * 8;
+  const int64_t kk0 = int64_t(blockIdx.y) * KT;
+#pragma unroll
+  for (int it = 0; it < KT / 32; ++it) {
+    const int r = threadIdx.x & 7, kk = (threadIdx.x >> 3) + 32 * it;
+    T val;
+    if (i0 + r < m && kk0 + kk < k) {
+      const int64_t e = int64_t(i0 + r) + (kk0 + kk) * ld;  // element index
+      if constexpr (ESZ == 16) {
+        if (VEC) {
+          val = __ldg(reinterpret_cast<const double2*>(X) + e);
+        } else {
+          val.x = double(X[2 * e]);
+          val.y = double(X[2 * e + 1]);
+        }
+      } else if constexpr (ESZ == 8 && sizeof(TIn) == 8) {
+        val = __double_as_longlong(double(X[e]));
+      } else if constexpr (ESZ == 8) {  // complex float
+        val = (static_cast<unsigned long long>(__float_as_uint(float(X[2 * e + 1]))) << 32) |
+              __float_as_uint(float(X[2 * e]));
+      } else {
+        val = __float_as_uint(float(X[e]));
+      }
+    } else {
+      if constexpr (ESZ == 16)
+        val = make_double2(0.0, 0.0);
+      else
+        val = 0;
+    }
+    tile[r * RSTR + swz(kk)] = val;
+  }
+  __syncthreads();
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int row = i0 + w;
+  if (row >= m || kk0 + G * l >= kp) return;
+  double v[EL];
+#pragma unroll
+  for (int q = 0; q < G; ++q) {
+    const T e = tile[w * RSTR + swz(G * l + q)];
+    if constexpr (ESZ == 16) {
+      v[2 * q] = e.x;
+      v[2 * q + 1] = e.y;
+    } else if constexpr (ESZ == 8 && sizeof(TIn) == 8) {
+      v[q] = __longlong_as_double(static_cast<long long>(e));
+    } else if constexpr (ESZ == 8) {
+      v[2 * q] = double(__uint_as_float(unsigned(e)));
+      v[2 * q + 1] = double(__uint_as_float(unsigned(e >> 32)));
+    } else {
+      v[q] = double(__uint_as_float(e));
+    }
+  }
+  slice_thread<TIn, NDIG, EL, NMU, MODE>(v, sigma[row], res + int64_t(row) * kp,
+                                         (kk0 + G * l) * R, int64_t(m) * kp, s_sum,
+                                         res_mod_stride, sc, t_begin, t_end);
 }
 
 // --------------------------------------------------------------------------
@@ -1833,6 +1996,7 @@ struct Layout {
   int64_t K2, kp;          // reals per operand row; residue row length (k padded to 128)
   int rowsA, rowsB, nb;    // A rows, B rows, B residue rows per product
   bool at;                 // op(A) = N: A is first copied k-major into At
+  bool mn;                 // op(A) = N with many rows: A read in place (m-major)
   bool r8;                 // one k-chunk: the residues of C are stored as bytes
   int64_t ldAt;            // leading dimension of At (elements of A's type)
   size_t off_sigA, off_sigB, off_resA, off_resB, off_R, off_At, off_status, off_tiles, total;
@@ -1851,7 +2015,11 @@ Layout layout_of(const GemmProblem& p, int moduli) {
   L.rowsA = int(p.m);
   L.rowsB = int(p.n);
   L.nb = int(p.n);
-  L.at = p.opA == 0;
+  // op(A) = N: read in place when there are enough rows for one norm thread
+  // each (and the tiles of the transposing slicer fit the grid), else copied
+  const int64_t kt = cplx ? 128 : 256;
+  L.mn = p.opA == 0 && p.m >= kMnRows && (L.kp + kt - 1) / kt <= 65535;
+  L.at = p.opA == 0 && !L.mn;
   L.r8 = (L.kp / BKB + kChunkBlocks - 1) / kChunkBlocks == 1;
   L.ldAt = L.at ? (p.k + 7) / 8 * 8 : 0;
   size_t off = 0;
@@ -2005,6 +2173,50 @@ void launch_slice(int ndig, cudaStream_t st, const TIn* X, int64_t ld, int64_t l
   }
 }
 
+// Residues of m-major rows (op(A) = N read in place): oz_slice_mn
+template <typename TIn, bool VEC, int MODE>
+void launch_slice_mn_v(int ndig, dim3 grid, cudaStream_t st, const TIn* X, int64_t ld, int m,
+                       int64_t k, int64_t kp, const int* sig, int s_sign, int8_t* res,
+                       int64_t stride, const oz::SliceConsts& sc, int t0, int t1) {
+  using namespace oz;
+  constexpr int kNU = sizeof(TIn) == 8 ? kDefaultModuli : kDefaultModuliFloat;
+  constexpr int kDigU = sizeof(TIn) == 8 ? 4 : 3;
+  if (t0 == 0 && t1 == kNU && sc.n == kNU && ndig == kDigU && slice_unroll()) {
+    oz_slice_mn<TIn, VEC, kDigU, kNU, MODE>
+        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, res, stride, sc, t0, t1);
+    return;
+  }
+  if (ndig <= 3)
+    oz_slice_mn<TIn, VEC, 3, 0, MODE>
+        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, res, stride, sc, t0, t1);
+  else if (ndig == 4)
+    oz_slice_mn<TIn, VEC, 4, 0, MODE>
+        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, res, stride, sc, t0, t1);
+  else
+    oz_slice_mn<TIn, VEC, 5, 0, MODE>
+        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, res, stride, sc, t0, t1);
+}
+
+template <typename TIn>
+void launch_slice_mn(int ndig, cudaStream_t st, const TIn* X, int64_t ld, int m, int64_t k,
+                     int64_t kp, const int* sig, int mode, int s_sign, int8_t* res,
+                     int64_t stride, const oz::SliceConsts& sc, int t0, int t1) {
+  const int64_t kt = mode == 2 ? 128 : 256;  // elements per row per tile
+  const dim3 grid(unsigned((m + 7) / 8), unsigned((kp + kt - 1) / kt));
+  if (mode == 2) {
+    // 16-byte element loads for complex double with a 16-byte aligned base
+    if (sizeof(TIn) == 8 && reinterpret_cast<uintptr_t>(X) % 16 == 0)
+      launch_slice_mn_v<TIn, true, 2>(ndig, grid, st, X, ld, m, k, kp, sig, s_sign, res, stride,
+                                      sc, t0, t1);
+    else
+      launch_slice_mn_v<TIn, false, 2>(ndig, grid, st, X, ld, m, k, kp, sig, s_sign, res, stride,
+                                       sc, t0, t1);
+  } else {
+    launch_slice_mn_v<TIn, false, 0>(ndig, grid, st, X, ld, m, k, kp, sig, s_sign, res, stride,
+                                     sc, t0, t1);
+  }
+}
+
 // Row scale exponents of A (which & 1) and B (which & 2).
 template <typename TIn>
 void scale_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
@@ -2012,9 +2224,18 @@ void scale_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
   using namespace oz;
   const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in real elements
   const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
-  if (which & 1)
+  if ((which & 1) && L.mn) {
+    const unsigned grid = unsigned((L.rowsA + 255) / 256);
+    if (cplx)
+      oz_row_scale_mn<TIn, true><<<grid, 256, 0, st>>>(static_cast<const TIn*>(p.A), p.lda,
+                                                       L.rowsA, p.k, crt.q_bits, sigA);
+    else
+      oz_row_scale_mn<TIn, false><<<grid, 256, 0, st>>>(static_cast<const TIn*>(p.A), p.lda,
+                                                        L.rowsA, p.k, crt.q_bits, sigA);
+  } else if (which & 1) {
     oz_row_scale<TIn><<<L.rowsA, 256, 0, st>>>(static_cast<const TIn*>(p.A), ldA, L.K2,
                                                L.rowsA, crt.q_bits, sigA);
+  }
   if (which & 2)
     oz_row_scale<TIn><<<L.rowsB, 256, 0, st>>>(static_cast<const TIn*>(p.B), ldB, L.K2,
                                                L.rowsB, crt.q_bits, sigB);
@@ -2078,7 +2299,7 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
   const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in real elements
   const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
   if (std::is_same<TIn, double>::value && cplx && t0 == 0 && t1 == L.nmod && crt.p[0] == 256 &&
-      L.nmod >= 2 && slice_tc_enabled()) {
+      L.nmod >= 2 && !((which & 1) && L.mn) && slice_tc_enabled()) {
     const double* Ad = reinterpret_cast<const double*>(A);
     const double* Bd = reinterpret_cast<const double*>(B);
     const bool okA = reinterpret_cast<uintptr_t>(Ad) % 16 == 0;
@@ -2123,7 +2344,10 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
   const int sumA = p.opA == 2 ? -1 : 1;
   const int64_t strideA = int64_t(L.nsub) * L.rowsA * L.kp;
   const int64_t strideB = int64_t(L.nsub) * L.nb * L.kp;
-  if ((which & 1) && vecA)
+  if ((which & 1) && L.mn)
+    launch_slice_mn<TIn>(ndig, st, A, p.lda, L.rowsA, p.k, L.kp, sigA, mode, sumA, resA, strideA,
+                         sc, t0, t1);
+  else if ((which & 1) && vecA)
     launch_slice<TIn, true>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, mode, sumA, resA,
                             strideA, sc, t0, t1);
   else if (which & 1)
