@@ -39,13 +39,14 @@ extern "C" {
 #define SPLAB_PATH_AUTO 0  /* the supported path with the least modelled time */
 #define SPLAB_PATH_DMMA 1  /* FP64 tensor cores (mma.sync f64); float inputs accumulate in FP64 */
 #define SPLAB_PATH_OZAKI 2 /* Ozaki scheme II on INT8 tcgen05 (all four dtypes), any
-                              op pair: op(A) = N and op(B) in {T, C} are first copied
-                              k-major into the workspace (conjugated for C) */
+                              op pair: op(A) = N and op(B) in {T, C} are read in place
+                              (conjugated on load for C) */
 #define SPLAB_PATH_TF32X3 3 /* float / complex float: each input split into two TF32
                                parts, three TF32 tcgen05 products, FP32 accumulation
                                in 64-real windows folded into double-float sums; any
-                               op pair (k-major copies as for Ozaki); double dtypes
-                               use DMMA */
+                               op pair: op(A) = N and op(B) in {T, C} are first copied
+                               k-major into the workspace (conjugated for C); double
+                               dtypes use DMMA */
 
 #define SPLAB_OK 0
 #define SPLAB_ERR_INVALID 1     /* bad argument (sizes, leading dimensions, dtype, path) */
@@ -157,7 +158,8 @@ SPLAB_API int splab_batch_create(int dtype, int count, const splab_problem *prob
  * stream with one shared workspace (the largest instance's), the sequence
  * captured in a CUDA graph on the second run and replayed afterwards.
  * SPLAB_ERR_UNSUPPORTED when an instance's dtype or op pair is not handled by
- * the path (the tensor-core paths take op(A) in {T, C}, op(B) = N). */
+ * the path (Ozaki: every op pair; 3x TF32 batches: op(A) in {T, C}, op(B) = N,
+ * the k-major copies of splab_gemm being made per call). */
 SPLAB_API int splab_batch_create_path(int dtype, int path, int count,
                                       const splab_problem *problems, void **plan,
                                       size_t *workspaceBytes);
@@ -251,7 +253,8 @@ SPLAB_API int splab_gemm_dd(int dtype, int opA, int opB, int64_t m, int64_t n, i
  *   DMMA path : 0 = contraction kernel, 1 = split-K reduction
  *   Ozaki path: 0 = slicing, 1 = INT8 residue GEMMs, 2 = reconstruction,
  *               3 + g = GEMM launch of modulus group g; inside phase 0:
- *               15 = k-major copy of A (op(A) = N), 16 = row norms (of A, and
+ *               15 = k-major copy of A (op(A) = N with k too long to be read in
+ *               place), 16 = row norms (of A, and
  *               of B unless they run on a side stream), 17 = residues of A,
  *               18 = residues of B (one modulus group)
  * Pass events = NULL to stop. Returns SPLAB_OK.

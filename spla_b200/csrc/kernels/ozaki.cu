@@ -1,9 +1,9 @@
 // Ozaki scheme II contraction on INT8 tensor cores (tcgen05, sm_100a).
 //
-// C <- alpha * op(A) * B + beta * C for float / double / complex with
-// op(A) in {N, T, C} (the layouts of pgemm_ssb, K-major operands, reference
-// src/pgemm_ssb/pgemm_ssb_host.cpp:168-171, and of pgemm_sbs / gemm N N:
-// op(A) = N is first copied K-major).
+// C <- alpha * op(A) * op(B) + beta * C for float / double / complex with
+// op(A), op(B) in {N, T, C} (the layouts of pgemm_ssb, K-major operands,
+// reference src/pgemm_ssb/pgemm_ssb_host.cpp:168-171, of pgemm_sbs and of
+// gemm; op(A) = N and op(B) = T, C are read in place, see 2a).
 //
 // Method (Ozaki, Uchino & Imamura, "Ozaki Scheme II: A GEMM-oriented emulation
 // of floating-point matrix multiplication using an integer modular
@@ -488,19 +488,34 @@ __global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
 }
 
 // --------------------------------------------------------------------------
-// 2a. op(A) = N operands with many rows, read in place: A is m-major (element
-// (i, kk) at X[i + kk ld], the rows of op(A) are the columns of X), and
-// instead of a k-major copy the norms read it along i and the slicer
-// transposes tiles through shared memory.
-constexpr int kMnRows = 65536;  // rows from which op(A) = N is read in place
+// 2a. operands read in place: op(A) = N (A m-major: element (i, kk) at
+// X[i + kk ld], the rows of op(A) are the columns of X) and op(B) = T or C
+// (B n-major the same way). Instead of a k-major copy the norms read them
+// along the rows and the slicer transposes tiles through shared memory.
+constexpr int kMnRows = 65536;  // rows from which the norms need no k-slicing
+
+// sigma from the exponent-tracked sum of squares S 2^(2E) of a row
+__device__ __forceinline__ int sigma_of(double S, int E, int q_bits) {
+  if (!(S < 1e300)) return kSigmaNonFinite;  // NaN or infinite input
+  if (S > 0.0) {
+    int e0 = 0;
+    frexp(sqrt(S), &e0);
+    return q_bits - (e0 + E);
+  }
+  return 0;
+}
 
 // Row scale exponents of m-major rows, as oz_row_scale computes them: one
-// thread per row (a warp reads 32 consecutive rows of one kk: coalesced),
-// batches of 8 loads in flight.
+// thread per row and k-slice (a warp reads 32 consecutive rows of one kk:
+// coalesced), batches of 8 loads in flight. With one k-slice (gridDim.y == 1)
+// the thread writes sigma; with several it writes its partial sum (S, E) to
+// partS / partE [slice][row] for oz_row_scale_combine.
 template <typename TIn, bool CPLX>
 __global__ void __launch_bounds__(256) oz_row_scale_mn(const TIn* __restrict__ X, int64_t ld,
-                                                       int m, int64_t k, int q_bits,
-                                                       int* __restrict__ sigma) {
+                                                       int m, int64_t k, int64_t kspan, int q_bits,
+                                                       int* __restrict__ sigma,
+                                                       double* __restrict__ partS,
+                                                       int* __restrict__ partE) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   constexpr int R = CPLX ? 2 : 1;  // reals per element
@@ -508,8 +523,9 @@ __global__ void __launch_bounds__(256) oz_row_scale_mn(const TIn* __restrict__ X
   const int64_t step = ld * R;  // reals between consecutive kk
   double S = 0.0, inv = 0.0;
   int E = -2100;
-  int64_t kk = 0;
-  for (; kk + 8 <= k; kk += 8) {
+  int64_t kk = int64_t(blockIdx.y) * kspan;
+  const int64_t kend = min(k, kk + kspan);
+  for (; kk + 8 <= kend; kk += 8) {
     double v[8 * R];
 #pragma unroll
     for (int b = 0; b < 8; ++b)
@@ -529,7 +545,7 @@ __global__ void __launch_bounds__(256) oz_row_scale_mn(const TIn* __restrict__ X
       S = fma(w, w, S);
     }
   }
-  for (; kk < k; ++kk) {
+  for (; kk < kend; ++kk) {
 #pragma unroll
     for (int c = 0; c < R; ++c) {
       const double v = double(x[kk * step + c]);
@@ -543,15 +559,26 @@ __global__ void __launch_bounds__(256) oz_row_scale_mn(const TIn* __restrict__ X
       S = fma(w, w, S);
     }
   }
-  if (!(S < 1e300)) {  // NaN or infinite input
-    sigma[i] = kSigmaNonFinite;
-  } else if (S > 0.0) {
-    int e0 = 0;
-    frexp(sqrt(S), &e0);
-    sigma[i] = q_bits - (e0 + E);
+  if (gridDim.y == 1) {
+    sigma[i] = sigma_of(S, E, q_bits);
   } else {
-    sigma[i] = 0;
+    partS[int64_t(blockIdx.y) * m + i] = S;
+    partE[int64_t(blockIdx.y) * m + i] = E;
   }
+}
+
+// sigma of each row from its k-slice partial sums
+__global__ void __launch_bounds__(256) oz_row_scale_combine(const double* __restrict__ partS,
+                                                            const int* __restrict__ partE, int m,
+                                                            int slices, int q_bits,
+                                                            int* __restrict__ sigma) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double S = 0.0;
+  int E = -2100;
+  for (int sl = 0; sl < slices; ++sl)
+    scaled_add(S, E, partS[int64_t(sl) * m + i], partE[int64_t(sl) * m + i]);
+  sigma[i] = sigma_of(S, E, q_bits);
 }
 
 // Raw element of ESZ bytes (a complex or real value of TIn) in shared memory
@@ -568,10 +595,11 @@ template <> struct RawElem<4> { using T = unsigned int; };
 // free of bank conflicts (the writes at most 2-way, 4-way for real float).
 // Each thread then does oz_slice's work (slice_thread) on its EL = 8 reals.
 // VEC: 16-byte loads of complex double elements (the base is 16-byte aligned).
+// conj: complex elements are conjugated as they are loaded (op(B) = C).
 template <typename TIn, bool VEC, int NDIG, int NMU, int MODE>
 __global__ void __launch_bounds__(256, 4)
     oz_slice_mn(const TIn* __restrict__ X, int64_t ld, int m, int64_t k, int64_t kp,
-                const int* __restrict__ sigma, int s_sum, int8_t* __restrict__ res,
+                const int* __restrict__ sigma, int s_sum, int conj, int8_t* __restrict__ res,
                 int64_t res_mod_stride, SliceConsts sc, int t_begin, int t_end) {
   constexpr int EL = 8;
   constexpr int R = MODE == 2 ? 2 : 1;  // reals per element
@@ -624,12 +652,13 @@ __global__ void __launch_bounds__(256, 4)
     const T e = tile[w * RSTR + swz(G * l + q)];
     if constexpr (ESZ == 16) {
       v[2 * q] = e.x;
-      v[2 * q + 1] = e.y;
+      v[2 * q + 1] = conj ? -e.y : e.y;
     } else if constexpr (ESZ == 8 && sizeof(TIn) == 8) {
       v[q] = __longlong_as_double(static_cast<long long>(e));
     } else if constexpr (ESZ == 8) {
       v[2 * q] = double(__uint_as_float(unsigned(e)));
-      v[2 * q + 1] = double(__uint_as_float(unsigned(e >> 32)));
+      const double im = double(__uint_as_float(unsigned(e >> 32)));
+      v[2 * q + 1] = conj ? -im : im;
     } else {
       v[q] = double(__uint_as_float(e));
     }
@@ -1995,14 +2024,34 @@ struct Layout {
   int nsub;                // products per modulus: 3 (complex, Karatsuba) or 1 (real)
   int64_t K2, kp;          // reals per operand row; residue row length (k padded to 128)
   int rowsA, rowsB, nb;    // A rows, B rows, B residue rows per product
-  bool at;                 // op(A) = N: A is first copied k-major into At
-  bool mn;                 // op(A) = N with many rows: A read in place (m-major)
+  bool at;                 // op(A) = N too long for in-place tiles: A copied k-major
+  bool mn;                 // op(A) = N: A read in place (m-major)
+  bool mnB;                // op(B) = T or C: B read in place (n-major)
+  int ksA, ksB;            // k-slices of the in-place row norms of A and B (1: none)
   bool r8;                 // one k-chunk: the residues of C are stored as bytes
   int64_t ldAt;            // leading dimension of At (elements of A's type)
-  size_t off_sigA, off_sigB, off_resA, off_resB, off_R, off_At, off_status, off_tiles, total;
+  size_t off_sigA, off_sigB, off_resA, off_resB, off_R, off_At, off_status, off_tiles;
+  size_t off_partA, off_partB;  // k-slice partial sums of the in-place row norms
+  size_t total;
 };
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// In-place reading of an m-major operand: the transposing slicer's tiles of
+// 128 (complex) or 256 (real) elements along k must fit the grid's y extent.
+bool mn_fits(const GemmProblem& p) {
+  const int64_t kp = (p.k + BKB - 1) / BKB * BKB;
+  const int64_t kt = dtype_is_complex(p.dtype) ? 128 : 256;
+  return (kp + kt - 1) / kt <= 65535;
+}
+
+// k-slices of the in-place row norms: about 2^18 threads in all (one per row
+// and slice), slices of at least 512 elements
+int norm_slices(int64_t rows, int64_t k) {
+  if (rows >= kMnRows || k <= 512) return 1;
+  const int64_t want = ((int64_t(1) << 18) + rows - 1) / rows;
+  return int(std::max<int64_t>(1, std::min<int64_t>(want, (k + 511) / 512)));
+}
 
 Layout layout_of(const GemmProblem& p, int moduli) {
   Layout L{};
@@ -2015,11 +2064,13 @@ Layout layout_of(const GemmProblem& p, int moduli) {
   L.rowsA = int(p.m);
   L.rowsB = int(p.n);
   L.nb = int(p.n);
-  // op(A) = N: read in place when there are enough rows for one norm thread
-  // each (and the tiles of the transposing slicer fit the grid), else copied
-  const int64_t kt = cplx ? 128 : 256;
-  L.mn = p.opA == 0 && p.m >= kMnRows && (L.kp + kt - 1) / kt <= 65535;
+  // op(A) = N and op(B) = T, C: read in place (the tiles of the transposing
+  // slicer fit the grid), else A is copied k-major (B is then unsupported)
+  L.mn = p.opA == 0 && mn_fits(p);
   L.at = p.opA == 0 && !L.mn;
+  L.mnB = p.opB != 0;
+  L.ksA = L.mn ? norm_slices(p.m, p.k) : 1;
+  L.ksB = L.mnB ? norm_slices(p.n, p.k) : 1;
   L.r8 = (L.kp / BKB + kChunkBlocks - 1) / kChunkBlocks == 1;
   L.ldAt = L.at ? (p.k + 7) / 8 * 8 : 0;
   size_t off = 0;
@@ -2039,6 +2090,10 @@ Layout layout_of(const GemmProblem& p, int moduli) {
   off = align256(off + 256);
   L.off_tiles = off;
   off = align256(off + sizeof(int) * size_t((L.rowsA + 255) / 256) * ((L.nb + 255) / 256));
+  L.off_partA = off;
+  off = align256(off + (L.ksA > 1 ? size_t(L.ksA) * L.rowsA * (sizeof(double) + sizeof(int)) : 0));
+  L.off_partB = off;
+  off = align256(off + (L.ksB > 1 ? size_t(L.ksB) * L.rowsB * (sizeof(double) + sizeof(int)) : 0));
   L.total = off;
   return L;
 }
@@ -2102,7 +2157,9 @@ size_t ozaki_workspace_bytes(const GemmProblem& p, int moduli) {
 }
 
 bool ozaki_supported(const GemmProblem& p) {
-  return p.opB == 0 && p.m <= (1 << 24) && p.n <= (1 << 23);
+  // op(B) = T or C: B is read in place, which needs the slicer's tiles to fit
+  return (p.opB == 0 || ((p.opB == 1 || p.opB == 2) && oz::mn_fits(p))) &&
+         p.m <= (1 << 24) && p.n <= (1 << 23);
 }
 
 namespace {
@@ -2176,67 +2233,78 @@ void launch_slice(int ndig, cudaStream_t st, const TIn* X, int64_t ld, int64_t l
 // Residues of m-major rows (op(A) = N read in place): oz_slice_mn
 template <typename TIn, bool VEC, int MODE>
 void launch_slice_mn_v(int ndig, dim3 grid, cudaStream_t st, const TIn* X, int64_t ld, int m,
-                       int64_t k, int64_t kp, const int* sig, int s_sign, int8_t* res,
+                       int64_t k, int64_t kp, const int* sig, int s_sign, int conj, int8_t* res,
                        int64_t stride, const oz::SliceConsts& sc, int t0, int t1) {
   using namespace oz;
   constexpr int kNU = sizeof(TIn) == 8 ? kDefaultModuli : kDefaultModuliFloat;
   constexpr int kDigU = sizeof(TIn) == 8 ? 4 : 3;
   if (t0 == 0 && t1 == kNU && sc.n == kNU && ndig == kDigU && slice_unroll()) {
     oz_slice_mn<TIn, VEC, kDigU, kNU, MODE>
-        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, res, stride, sc, t0, t1);
+        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, conj, res, stride, sc, t0, t1);
     return;
   }
   if (ndig <= 3)
     oz_slice_mn<TIn, VEC, 3, 0, MODE>
-        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, res, stride, sc, t0, t1);
+        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, conj, res, stride, sc, t0, t1);
   else if (ndig == 4)
     oz_slice_mn<TIn, VEC, 4, 0, MODE>
-        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, res, stride, sc, t0, t1);
+        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, conj, res, stride, sc, t0, t1);
   else
     oz_slice_mn<TIn, VEC, 5, 0, MODE>
-        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, res, stride, sc, t0, t1);
+        <<<grid, 256, 0, st>>>(X, ld, m, k, kp, sig, s_sign, conj, res, stride, sc, t0, t1);
 }
 
 template <typename TIn>
 void launch_slice_mn(int ndig, cudaStream_t st, const TIn* X, int64_t ld, int m, int64_t k,
-                     int64_t kp, const int* sig, int mode, int s_sign, int8_t* res,
+                     int64_t kp, const int* sig, int mode, int s_sign, int conj, int8_t* res,
                      int64_t stride, const oz::SliceConsts& sc, int t0, int t1) {
   const int64_t kt = mode == 2 ? 128 : 256;  // elements per row per tile
   const dim3 grid(unsigned((m + 7) / 8), unsigned((kp + kt - 1) / kt));
   if (mode == 2) {
     // 16-byte element loads for complex double with a 16-byte aligned base
     if (sizeof(TIn) == 8 && reinterpret_cast<uintptr_t>(X) % 16 == 0)
-      launch_slice_mn_v<TIn, true, 2>(ndig, grid, st, X, ld, m, k, kp, sig, s_sign, res, stride,
-                                      sc, t0, t1);
+      launch_slice_mn_v<TIn, true, 2>(ndig, grid, st, X, ld, m, k, kp, sig, s_sign, conj, res,
+                                      stride, sc, t0, t1);
     else
-      launch_slice_mn_v<TIn, false, 2>(ndig, grid, st, X, ld, m, k, kp, sig, s_sign, res, stride,
-                                       sc, t0, t1);
+      launch_slice_mn_v<TIn, false, 2>(ndig, grid, st, X, ld, m, k, kp, sig, s_sign, conj, res,
+                                       stride, sc, t0, t1);
   } else {
-    launch_slice_mn_v<TIn, false, 0>(ndig, grid, st, X, ld, m, k, kp, sig, s_sign, res, stride,
-                                     sc, t0, t1);
+    launch_slice_mn_v<TIn, false, 0>(ndig, grid, st, X, ld, m, k, kp, sig, s_sign, conj, res,
+                                     stride, sc, t0, t1);
   }
 }
 
 // Row scale exponents of A (which & 1) and B (which & 2).
 template <typename TIn>
 void scale_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
-                    int* sigA, int* sigB, int which, cudaStream_t st) {
+                    int* sigA, int* sigB, char* w, int which, cudaStream_t st) {
   using namespace oz;
   const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in real elements
   const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
-  if ((which & 1) && L.mn) {
-    const unsigned grid = unsigned((L.rowsA + 255) / 256);
+  // m-major rows read in place: k-sliced norms, combined when sliced
+  auto in_place = [&](const void* X, int64_t ld, int rows, int ks, size_t off_part, int* sig) {
+    const int64_t kspan = (p.k + ks - 1) / ks;
+    double* partS = reinterpret_cast<double*>(w + off_part);
+    int* partE = reinterpret_cast<int*>(w + off_part + sizeof(double) * size_t(ks) * rows);
+    const dim3 grid(unsigned((rows + 255) / 256), unsigned(ks));
     if (cplx)
-      oz_row_scale_mn<TIn, true><<<grid, 256, 0, st>>>(static_cast<const TIn*>(p.A), p.lda,
-                                                       L.rowsA, p.k, crt.q_bits, sigA);
+      oz_row_scale_mn<TIn, true><<<grid, 256, 0, st>>>(static_cast<const TIn*>(X), ld, rows, p.k,
+                                                       kspan, crt.q_bits, sig, partS, partE);
     else
-      oz_row_scale_mn<TIn, false><<<grid, 256, 0, st>>>(static_cast<const TIn*>(p.A), p.lda,
-                                                        L.rowsA, p.k, crt.q_bits, sigA);
-  } else if (which & 1) {
+      oz_row_scale_mn<TIn, false><<<grid, 256, 0, st>>>(static_cast<const TIn*>(X), ld, rows, p.k,
+                                                        kspan, crt.q_bits, sig, partS, partE);
+    if (ks > 1)
+      oz_row_scale_combine<<<unsigned((rows + 255) / 256), 256, 0, st>>>(partS, partE, rows, ks,
+                                                                         crt.q_bits, sig);
+  };
+  if ((which & 1) && L.mn)
+    in_place(p.A, p.lda, L.rowsA, L.ksA, L.off_partA, sigA);
+  else if (which & 1)
     oz_row_scale<TIn><<<L.rowsA, 256, 0, st>>>(static_cast<const TIn*>(p.A), ldA, L.K2,
                                                L.rowsA, crt.q_bits, sigA);
-  }
-  if (which & 2)
+  if ((which & 2) && L.mnB)
+    in_place(p.B, p.ldb, L.rowsB, L.ksB, L.off_partB, sigB);
+  else if (which & 2)
     oz_row_scale<TIn><<<L.rowsB, 256, 0, st>>>(static_cast<const TIn*>(p.B), ldB, L.K2,
                                                L.rowsB, crt.q_bits, sigB);
 }
@@ -2299,7 +2367,7 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
   const int64_t ldA = cplx ? 2 * p.lda : p.lda;  // in real elements
   const int64_t ldB = cplx ? 2 * p.ldb : p.ldb;
   if (std::is_same<TIn, double>::value && cplx && t0 == 0 && t1 == L.nmod && crt.p[0] == 256 &&
-      L.nmod >= 2 && !((which & 1) && L.mn) && slice_tc_enabled()) {
+      L.nmod >= 2 && !((which & 1) && L.mn) && !((which & 2) && L.mnB) && slice_tc_enabled()) {
     const double* Ad = reinterpret_cast<const double*>(A);
     const double* Bd = reinterpret_cast<const double*>(B);
     const bool okA = reinterpret_cast<uintptr_t>(Ad) % 16 == 0;
@@ -2345,15 +2413,18 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
   const int64_t strideA = int64_t(L.nsub) * L.rowsA * L.kp;
   const int64_t strideB = int64_t(L.nsub) * L.nb * L.kp;
   if ((which & 1) && L.mn)
-    launch_slice_mn<TIn>(ndig, st, A, p.lda, L.rowsA, p.k, L.kp, sigA, mode, sumA, resA, strideA,
-                         sc, t0, t1);
+    launch_slice_mn<TIn>(ndig, st, A, p.lda, L.rowsA, p.k, L.kp, sigA, mode, sumA, 0, resA,
+                         strideA, sc, t0, t1);
   else if ((which & 1) && vecA)
     launch_slice<TIn, true>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, mode, sumA, resA,
                             strideA, sc, t0, t1);
   else if (which & 1)
     launch_slice<TIn, false>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, mode, sumA, resA,
                              strideA, sc, t0, t1);
-  if ((which & 2) && vecB)
+  if ((which & 2) && L.mnB)  // op(B) = T or C: n-major rows, conjugated for C
+    launch_slice_mn<TIn>(ndig, st, B, p.ldb, L.rowsB, p.k, L.kp, sigB, mode, 1,
+                         p.opB == 2 ? 1 : 0, resB, strideB, sc, t0, t1);
+  else if ((which & 2) && vecB)
     launch_slice<TIn, true>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, mode, 1, resB, strideB,
                             sc, t0, t1);
   else if (which & 2)
@@ -2578,9 +2649,9 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
   if (ps) lk = std::unique_lock<std::mutex>(ps->mu);
   auto scale = [&](int which, cudaStream_t s) {
     if (dbl)
-      scale_operands<double>(L, crt, p, cplx, sigA, sigB, which, s);
+      scale_operands<double>(L, crt, p, cplx, sigA, sigB, w, which, s);
     else
-      scale_operands<float>(L, crt, p, cplx, sigA, sigB, which, s);
+      scale_operands<float>(L, crt, p, cplx, sigA, sigB, w, which, s);
   };
   phase_mark(0, false, st);
   if (L.at && p.k > 0) {

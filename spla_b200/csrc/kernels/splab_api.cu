@@ -195,7 +195,7 @@ Normalized normalize(const GemmProblem& p, int rp) {
   const size_t esz = size_t(dtype_bytes(p.dtype));
   const int64_t kn = (std::max<int64_t>(p.k, 1) + 7) / 8 * 8;  // 16-byte aligned rows
   size_t off = 0;
-  if (p.opB != 0) {
+  if (p.opB != 0 && rp == SPLAB_PATH_TF32X3) {  // the Ozaki path reads op(B) = T, C in place
     N.copyB = true;
     N.ldBn = kn;
     N.offB = off;
@@ -299,7 +299,7 @@ size_t path_workspace(const GemmProblem& p, int rp, int moduli) {
 }
 
 int resolve_path(const GemmProblem& p, int path, int moduli) {
-  const bool oz = ozaki_supported(k_major_view(p, false));
+  const bool oz = ozaki_supported(p);  // op(B) = T, C read in place by the path itself
   const bool tf = tf32x3_supported(k_major_view(p, true));
   if (path == SPLAB_PATH_TF32X3) return tf ? SPLAB_PATH_TF32X3 : SPLAB_PATH_DMMA;
   if (path == SPLAB_PATH_OZAKI) return oz ? SPLAB_PATH_OZAKI : SPLAB_PATH_DMMA;
@@ -312,7 +312,7 @@ int resolve_path(const GemmProblem& p, int path, int moduli) {
   int best = SPLAB_PATH_DMMA;
   double best_ms = model::dmma_ms(p);
   if (oz && path_workspace(p, SPLAB_PATH_OZAKI, moduli) <= cap) {
-    const double t = model::ozaki_ms(k_major_view(p, false)) + copyB;
+    const double t = model::ozaki_ms(k_major_view(p, false));
     if (t < 0.9 * best_ms) {
       best = SPLAB_PATH_OZAKI;
       best_ms = t;

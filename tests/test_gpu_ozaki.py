@@ -447,45 +447,58 @@ def test_tensor_core_reconstruction_matches_staged(dt, m, n, k, opA, fill, modul
     assert oracle.rel_fro(g[sel], r[sel]) <= tol
 
 
-@pytest.mark.parametrize("dt,m,n,k,pad,offset", [
-    ("complex128", 65536 + 37, 48, 999, 0, False),   # ragged rows and k (k-tile tail)
-    ("complex128", 70000, 40, 1000, 5, True),        # padded lda, base 8 bytes off 16
-    ("float64", 65536 + 9, 40, 1500, 3, False),
-    ("complex64", 66000, 40, 700, 0, False),
-    ("float32", 65600, 36, 900, 1, False),
+@pytest.mark.parametrize("dt,opA,opB,m,n,k,pad,offset", [
+    ("complex128", 0, 0, 65536 + 37, 48, 999, 0, False),  # many rows, ragged m and k
+    ("complex128", 0, 0, 70000, 40, 1000, 5, True),       # padded lda, base 8 bytes off 16
+    ("float64", 0, 0, 65536 + 9, 40, 1500, 3, False),
+    ("complex64", 0, 0, 66000, 40, 700, 0, False),
+    ("float32", 0, 0, 65600, 36, 900, 1, False),
+    ("complex128", 0, 0, 300, 200, 40000, 2, False),      # few rows: k-sliced norms
+    ("complex128", 2, 1, 257, 300, 20000, 1, False),      # op(B) = T in place
+    ("complex128", 1, 2, 128, 260, 3000, 0, True),        # op(B) = C: conjugated on load
+    ("complex128", 0, 2, 200, 70001, 600, 0, False),      # both in place, many B rows
+    ("float64", 1, 1, 190, 210, 30000, 2, False),
+    ("complex64", 0, 2, 150, 170, 20000, 0, False),
+    ("float32", 0, 1, 100, 90, 50000, 0, False),
 ])
-def test_op_a_n_in_place(dt, m, n, k, pad, offset):
-    """op(A) = N with m >= 65536 rows is read in place (m-major): row norms
-    along i and residues through a transposing shared-memory tile, no k-major
-    copy of A. Checked against the device double-double product, with alpha
-    and beta, ragged m and k, a padded lda and (complex double) a base address
-    that is only 8-byte aligned (the scalar-load variant)."""
+def test_in_place_operands(dt, opA, opB, m, n, k, pad, offset):
+    """op(A) = N and op(B) = T or C are read in place (m- and n-major rows):
+    row norms along the rows (k-sliced and combined when the rows are few)
+    and residues through a transposing shared-memory tile, conjugated on load
+    for op(B) = C; no k-major copy of either operand. Checked against the
+    device double-double product, with alpha and beta, ragged sizes, padded
+    leading dimensions and (complex double) a base address only 8-byte
+    aligned (the scalar-load variant)."""
     import torch
     cplx = dt.startswith("complex")
     rt = torch.float64 if dt in ("complex128", "float64") else torch.float32
     r = 2 if cplx else 1
-    lda = m + pad
     g = torch.Generator(device="cuda")
     g.manual_seed(7)
     s = (1.0 / (r * k)) ** 0.5
-    # A: lda x k (m-major), B: k x n (k-major), as real buffers of the element type
-    Abuf = torch.randn(r * lda * k + 2, dtype=rt, device="cuda", generator=g) * s
-    A = Abuf[1:] if offset else Abuf  # complex128 at offset 1 real: 8 bytes off 16
-    B = torch.randn(r * k * n, dtype=rt, device="cuda", generator=g) * s
+    lda = (m if opA == 0 else k) + pad
+    ldb = (k if opB == 0 else n) + pad
+    acols = k if opA == 0 else m
+    bcols = n if opB == 0 else k
+    Abuf = torch.randn(r * lda * acols + 2, dtype=rt, device="cuda", generator=g) * s
+    A = Abuf[1:] if offset else Abuf  # complex double at one real off: 8 bytes off 16
+    B = torch.randn(r * ldb * bcols, dtype=rt, device="cuda", generator=g) * s
     C0 = torch.rand(r * m * n, dtype=rt, device="cuda", generator=g) * 2 - 1
     alpha, beta = ((0.5 - 0.25j), (1.0 + 0.5j)) if cplx else (0.5, -1.0)
     C = C0.clone()
-    ws_bytes = spla.splab_gemm_workspace_size(dt, spla.PATH_OZAKI, 0, 0, m, n, k)
+    ws_bytes = spla.splab_gemm_workspace_size(dt, spla.PATH_OZAKI, opA, opB, m, n, k)
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
-    rc = spla.splab_gemm(dt, spla.PATH_OZAKI, 0, 0, m, n, k, alpha, A, lda, B, k, beta, C, m,
-                         workspace=ws, workspace_bytes=ws_bytes)
+    assert spla.lib().splab_gemm_path(spla._dtype_of(dtype=dt), spla.PATH_OZAKI, opA, opB, m, n,
+                                      k) == spla.PATH_OZAKI
+    rc = spla.splab_gemm(dt, spla.PATH_OZAKI, opA, opB, m, n, k, alpha, A, lda, B, ldb, beta, C,
+                         m, workspace=ws, workspace_bytes=ws_bytes)
     assert rc == 0
     Rdt = torch.complex128 if cplx else torch.float64
     R = torch.zeros(m * n, dtype=Rdt, device="cuda")
     Ad = A.double() if rt == torch.float32 else A
     Bd = B.double() if rt == torch.float32 else B
-    assert spla.gemm_dd("complex128" if cplx else "float64", 0, 0, m, n, k, Ad, lda, Bd, k, R,
-                        m) == 0
+    assert spla.gemm_dd("complex128" if cplx else "float64", opA, opB, m, n, k, Ad, lda, Bd, ldb,
+                        R, m) == 0
     torch.cuda.synchronize()
     if cplx:
         got = torch.view_as_complex(C.double().reshape(-1, 2))
