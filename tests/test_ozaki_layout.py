@@ -2,16 +2,17 @@
 ABI's sizing call (no device needed): complex products keep three residue
 planes per modulus and operand (re, im and their sum), real ones a single
 plane; the residues of C are bytes when the contraction is one k-chunk (at
-most 124928 residue bytes per row) and int32 sums beyond; op(A) = N adds a
-k-major copy of A; the modulus count follows the dtype default or the knob."""
+most 124928 residue bytes per row) and int32 sums beyond; op(A) = N and
+op(B) = T, C are read in place (no k-major copy: only the partial sums of the
+k-sliced row norms); the modulus count follows the dtype default or the knob."""
 import spla_b200 as spla
 
 OZ = spla.PATH_OZAKI
 SLACK = 1 << 20  # row exponents, status word, tile list and 256-byte alignment
 
 
-def ws(dtype, opA, m, n, k, moduli=0):
-    return spla.splab_gemm_workspace_size(dtype, OZ, opA, 0, m, n, k, moduli)
+def ws(dtype, opA, m, n, k, moduli=0, opB=0):
+    return spla.splab_gemm_workspace_size(dtype, OZ, opA, opB, m, n, k, moduli)
 
 
 def kp(k):
@@ -41,11 +42,27 @@ def test_int32_sums_beyond_one_chunk():
     assert abs((two - one) - (plane_growth + r_growth)) <= 4096
 
 
-def test_op_n_adds_k_major_copy_of_a():
+def norm_slices(rows, k):
+    """k-slices of the in-place row norms (about 2^18 threads, >= 512 elements each)"""
+    if rows >= 65536 or k <= 512:
+        return 1
+    return max(1, min(-(-(1 << 18) // rows), -(-k // 512)))
+
+
+def partials(rows, k):
+    s = norm_slices(rows, k)
+    return s * rows * 12 if s > 1 else 0  # a double and an int per row and slice
+
+
+def test_in_place_operands_need_no_copy():
     m, n, k = 2000, 256, 3000
-    ldat = (k + 7) // 8 * 8
     diff = ws("complex128", 0, m, n, k) - ws("complex128", 1, m, n, k)
-    assert abs(diff - 16 * m * ldat) <= 4096
+    assert abs(diff - partials(m, k)) <= 512  # op(A) = N: no copy of A (96 MB)
+    for opB in (1, 2):
+        diff = ws("complex128", 1, m, n, k, opB=opB) - ws("complex128", 1, m, n, k)
+        assert abs(diff - partials(n, k)) <= 512
+    # many rows: the norms are not sliced
+    assert ws("complex128", 0, 70000, 64, 2048) - ws("complex128", 1, 70000, 64, 2048) == 0
 
 
 def test_modulus_count():
