@@ -1199,7 +1199,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     int accb = 0;
     for (int u = blockIdx.x; u < g.total_units; u += gridDim.x) {
       const Unit w = decode_unit(u, g);
-      if (!mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)) break;
+      // warp-uniform: the TMEM loads below are collective
+      if (!__all_sync(0xffffffffu,
+                      mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)))
+        break;
       tc_fence_after();
       const int mt = w.t / g.nsub;  // modulus of this product
       const int p = g.p[mt], c16 = g.c16[mt], off = g.off[mt];
@@ -1319,7 +1322,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(accf_bar(b), 1);
-      mbar_init(acce_bar(b), 2 * 128 * g.epi_split);
+      mbar_init(acce_bar(b), 2 * 4 * g.epi_split);  // one arrival per epilogue warp of the pair
     }
     mbar_init(drain_bar, 1);
     *abort = 0;
@@ -1445,7 +1448,10 @@ __global__ void __launch_bounds__(PAIR_THREADS, 1)
     for (int u = pair; u < g.total_units; u += npairs) {
       int t, c, tm, tn;
       unit_of(u, t, c, tm, tn);
-      if (!mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)) break;
+      // warp-uniform: the TMEM loads and the warp's arrival below are collective
+      if (!__all_sync(0xffffffffu,
+                      mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)))
+        break;
       tc_fence_after();
       const int mt = t / g.nsub;  // modulus of this product
       const int p = g.p[mt], c16 = g.c16[mt], off = g.off[mt];
@@ -1487,8 +1493,13 @@ __global__ void __launch_bounds__(PAIR_THREADS, 1)
           }
         }
       }
+      // the accumulator is drained: one arrival per warp with the default
+      // (CTA-scope) semantics on the MMA issuer's barrier; the ordering of the
+      // TMEM loads before the next MMAs comes from the tcgen05 fences around
+      // the barrier (a cluster-scope release per thread cost membar stalls)
       tc_fence_before();
-      mbar_arrive_cluster(map_to_rank(acce_bar(accb), 0));
+      __syncwarp();
+      if (lane == 0) mbar_arrive_remote(map_to_rank(acce_bar(accb), 0));
       acc_phase[accb] ^= 1u;
       accb = (accb + 1) % P::NBUF;
     }
@@ -1963,7 +1974,8 @@ __global__ void __launch_bounds__(RT_THREADS, 5)
       // the scale exponents load while the accumulator is awaited
       const int si = i < P.m ? P.sigA[i] : 0;
       const int tauj = P.sigB[j];
-      if (!mbar_wait(accf_bar(b), bpar, abort, P.wait_limit_ns)) break;
+      // warp-uniform: the TMEM load and the warp's arrival below are collective
+      if (!__all_sync(0xffffffffu, mbar_wait(accf_bar(b), bpar, abort, P.wait_limit_ns))) break;
       tc_fence_after();
       __syncwarp();
       uint32_t v[32];

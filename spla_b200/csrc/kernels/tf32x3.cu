@@ -319,7 +319,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       bool first_fold = true;
       int wi = 0;
       for (int w0 = kb0; w0 < kb1; w0 += kWin, ++wi) {
-        if (!mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns)) {
+        // warp-uniform: the TMEM loads and the warp's arrival below are collective
+        if (!__all_sync(0xffffffffu,
+                        mbar_wait(accf_bar(accb), acc_phase[accb], abort, g.wait_limit_ns))) {
           ok = false;
           break;
         }
