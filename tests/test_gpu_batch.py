@@ -151,3 +151,43 @@ def test_batch_new_workspace_after_tuning():
         assert oracle.pgemm_ssb(p["m"], p["n"], p["k"], p["opA"], alpha, A, p["k"], B, p["k"],
                                 0.0, ref, p["m"], 0, 0) == 0
         assert oracle.rel_fro(p["C"].cpu().numpy(), ref) <= 1e-14
+
+
+@pytest.mark.parametrize("opA,opB", [(0, 1), (2, 2)])
+def test_ozaki_batch_in_place_operands(opA, opB):
+    """Ozaki batches whose instances read op(A) = N or op(B) = T, C in place
+    (m- and n-major rows through the transposing slicer): direct run, graph
+    capture and replay, each instance checked against the device
+    double-double product."""
+    import torch
+    import spla_b200 as spla
+    g = torch.Generator(device="cuda")
+    g.manual_seed(901)
+    shapes = [(130, 70, 9000), (257, 300, 20000), (17, 300, 2048)]
+    probs, refs = [], []
+    for m, n, k in shapes:
+        lda = m if opA == 0 else k
+        ldb = k if opB == 0 else n
+        s = (1.0 / (2 * k)) ** 0.5
+        A = torch.randn(lda * (k if opA == 0 else m), dtype=torch.complex128, device="cuda",
+                        generator=g) * s
+        B = torch.randn(ldb * (n if opB == 0 else k), dtype=torch.complex128, device="cuda",
+                        generator=g) * s
+        C = torch.zeros(m * n, dtype=torch.complex128, device="cuda")
+        R = torch.zeros(m * n, dtype=torch.complex128, device="cuda")
+        assert spla.gemm_dd("complex128", opA, opB, m, n, k, A, lda, B, ldb, R, m) == 0
+        probs.append(dict(opA=opA, opB=opB, m=m, n=n, k=k, A=A, lda=lda, B=B, ldb=ldb, C=C,
+                          ldc=m, alpha=0.5 - 0.25j, beta=0.0))
+        refs.append(R)
+    batch = spla.Batch("complex128", probs, path=spla.PATH_OZAKI)
+    ws = torch.empty(batch.workspace_bytes, dtype=torch.uint8, device="cuda")
+    for _ in range(3):  # direct, capture + replay, replay
+        for p in probs:
+            p["C"].zero_()
+        batch.run(ws)
+        torch.cuda.synchronize()
+        batch.check(ws)
+        for p, R in zip(probs, refs):
+            ref = (0.5 - 0.25j) * R
+            err = float(torch.linalg.vector_norm(p["C"] - ref) / torch.linalg.vector_norm(ref))
+            assert err <= 1e-14, (p["m"], p["n"], p["k"], err)
