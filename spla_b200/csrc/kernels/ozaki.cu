@@ -28,12 +28,15 @@
 // The only rounding is the integer rounding of step 2 (relative to each row's
 // 2-norm, 2^-Q) and the final conversion of X to double.
 //
-// Kernels: oz_transpose (op(A) = N), oz_row_scale (row norms -> sigma),
-// oz_slice (scaled residues, int8, K-major, one plane per modulus and
-// product), oz_gemm_pair / oz_gemm (tcgen05.mma kind::i8, TMA-fed, TMEM
-// accumulators, warp-specialised persistent kernels), oz_reconstruct /
-// oz_reconstruct_staged (CRT + scaling + alpha/beta + fill-mode tile skipping
-// into C).
+// Kernels: oz_row_scale (row norms -> sigma), oz_slice (scaled residues,
+// int8, K-major, one plane per modulus and product), oz_row_scale_mn /
+// oz_slice_mn (the same for op(A) = N and op(B) = T, C read in place),
+// oz_transpose (op(A) = N copied K-major when k is too long for that),
+// oz_slice_tc (opt-in: digit sums on the tensor cores), oz_gemm_pair / oz_gemm
+// (tcgen05.mma kind::i8, TMA-fed, TMEM accumulators, warp-specialised
+// persistent kernels), oz_reconstruct_tc (CRT sums on the tensor cores) and
+// oz_reconstruct / oz_reconstruct_staged (CRT on the CUDA cores), each with
+// scaling, alpha/beta and fill-mode tile skipping into C.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 

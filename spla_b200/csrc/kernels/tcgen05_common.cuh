@@ -157,15 +157,11 @@ __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
                    : "memory");
 }
-__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
-               : "memory");
-}
 // Arrival on a barrier of another CTA of the cluster with the default
 // semantics (release at CTA scope): enough to hand a drained TMEM
 // accumulator back to the MMA issuer, whose ordering comes from the
 // tcgen05.fence::before_thread_sync / after_thread_sync pair around the
-// barrier, without the cluster-scope fence of mbar_arrive_cluster.
+// barrier (a cluster-scope release per arrival measured as membar stalls).
 __device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
   asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
 }
