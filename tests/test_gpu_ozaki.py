@@ -509,3 +509,54 @@ def test_in_place_operands(dt, opA, opB, m, n, k, pad, offset):
     err = float(torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref))
     tol = 1e-14 if rt == torch.float64 else 1e-6
     assert err <= tol, err
+
+
+def test_in_place_non_finite_and_extreme_rows():
+    """The k-sliced in-place row norms (op(A) = N, op(B) = T; few rows, so the
+    k range is sliced and the partial sums combined) keep the k-major path's
+    semantics: a NaN or an infinity anywhere in a row makes that row's results
+    NaN, and rows of magnitude 1e300 or 1e-300 scale without overflow or
+    underflow (checked against the device double-double product)."""
+    import torch
+    m, n, k = 96, 80, 30000
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    s = (1.0 / (2 * k)) ** 0.5
+    A = torch.randn(m * k, dtype=torch.complex128, device="cuda", generator=g) * s  # m x k
+    B = torch.randn(n * k, dtype=torch.complex128, device="cuda", generator=g) * s  # n x k
+    Av = A.view(k, m)  # element (i, kk) at kk * m + i
+    Bv = B.view(k, n)
+    Av[:, 3] *= 1e300
+    Av[:, 4] *= 1e-300
+    Bv[:, 6] *= 1e-300  # (3, 6) meets a 1e300 row: about 1
+    Av[20000, 9] = complex(float("nan"), 0.0)   # late in the row: another k-slice
+    Bv[25000, 11] = complex(0.0, float("inf"))
+    C = torch.zeros(m * n, dtype=torch.complex128, device="cuda")
+    ws_bytes = spla.splab_gemm_workspace_size("complex128", spla.PATH_OZAKI, 0, 1, m, n, k)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    assert spla.splab_gemm("complex128", spla.PATH_OZAKI, 0, 1, m, n, k, 1.0, A, m, B, n, 0.0,
+                           C, m, workspace=ws, workspace_bytes=ws_bytes) == 0
+    R = torch.zeros(m * n, dtype=torch.complex128, device="cuda")
+    assert spla.gemm_dd("complex128", 0, 1, m, n, k, A, m, B, n, R, m) == 0
+    torch.cuda.synchronize()
+    got = C.view(n, m).T.cpu().numpy()
+    ref = R.view(n, m).T.cpu().numpy()
+    bad = np.zeros((m, n), bool)
+    bad[9, :] = True
+    bad[:, 11] = True
+    assert np.isnan(got[bad]).all()
+    ok = ~bad
+
+    def rel(x, r):  # relative Frobenius error, scaled first (rows near 1e300)
+        sc = np.abs(r).max()
+        return oracle.rel_fro(x / sc, r / sc)
+
+    # the extreme rows and column on their own scale, then the ordinary block
+    for sel in (np.s_[3, :], np.s_[4, :], np.s_[:, 6]):
+        keep = ok[sel]
+        assert rel(got[sel][keep], ref[sel][keep]) <= 1e-14
+    rows = np.r_[0:3, 5:m]
+    block_ok = ok[rows][:, [c for c in range(n) if c != 6]]
+    gb = got[rows][:, [c for c in range(n) if c != 6]]
+    rb = ref[rows][:, [c for c in range(n) if c != 6]]
+    assert rel(gb[block_ok], rb[block_ok]) <= 1e-14
