@@ -1785,19 +1785,26 @@ inline int staged_smem_bytes(bool cplx, int nmod) {
 // 32-bit limb sums of S and finishes with crt_from_limbs, as the CUDA-core
 // kernels do: the results are the same doubles.
 //
-// Warp 0: TMA producer (4-stage ring), warp 1: TMEM allocation and MMA issue
-// (accumulators double-buffered), warps 2-5: epilogue. Every wait is bounded;
-// a give-up sets *status.
+// A work unit is RT_G blocks of 128 rows of one column (the fixed cost of the
+// hand-offs below is paid once per unit). Warp 0: TMA producer (4-stage
+// ring), warp 1: TMEM allocation and MMA issue (accumulators double-buffered),
+// warps 2-5: epilogue (RT_G rows per lane). Every wait is bounded; a give-up
+// sets *status.
 constexpr int RT_THREADS = 192;
 constexpr int RT_STAGES = 4;
-constexpr int RT_KP = 64;                     // planes per tile (K), padded
-constexpr int RT_STAGE = 128 * RT_KP;         // bytes per stage
+constexpr int RT_G = 2;                       // blocks of 128 rows per work unit
+constexpr int RT_KP = 64;                     // planes per block (K), padded
+constexpr int RT_BLOCK = 128 * RT_KP;         // bytes per block of 128 rows
+constexpr int RT_STAGE = RT_G * RT_BLOCK;     // bytes per stage
 constexpr int RT_W_BYTES = 32 * 128;          // weights: 32 rows x 128 B (SW128)
 constexpr int RT_SMEM = RT_STAGES * RT_STAGE + RT_W_BYTES + 256 + 1024;
+// three CTAs fit an SM's shared memory, so their 2 x RT_G x 32 TMEM columns fit
+static_assert(4 * (RT_SMEM + 1024) > 228 * 1024 && 3 * 2 * RT_G * 32 <= 512,
+              "at most three CTAs per SM, within the TMEM");
 
 struct ReconTcParams {
   int m, n;
-  int row_blocks;         // ceil(m / 128)
+  int row_blocks;         // groups of RT_G blocks of 128 rows: ceil(m / (128 RT_G))
   long long total_units;  // row_blocks * n
   int planes;             // product planes of the residue array (loaded per tile)
   int kp;                 // K of the MMA: 32 or 64 (planes past `planes` are zero rows)
@@ -1838,7 +1845,7 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
 }
 
 template <int DT>
-__global__ void __launch_bounds__(RT_THREADS, 5)
+__global__ void __launch_bounds__(RT_THREADS, 3)
     oz_reconstruct_tc(const __grid_constant__ CUtensorMap tmR,
                       const __grid_constant__ ReconTcParams P) {
   constexpr bool CPLX = dtype_is_complex(DT);
@@ -1872,10 +1879,10 @@ __global__ void __launch_bounds__(RT_THREADS, 5)
       const unsigned char b = (o < NO && k < P.kp) ? P.v[o][k] : 0;
       wp[(o >> 3) * 1024 + (o & 7) * 128 + (((k >> 4) ^ (o & 7)) << 4) + (k & 15)] = b;
     }
-    const int pad = (P.kp - P.planes) * 128;  // bytes per stage, 16-byte words below
-    for (int idx = threadIdx.x; idx < RT_STAGES * (pad / 16); idx += RT_THREADS) {
-      const int st = idx / (pad / 16), w16 = idx - st * (pad / 16);
-      *reinterpret_cast<uint4*>(base_ptr + st * RT_STAGE + P.planes * 128 + 16 * w16) =
+    const int pad = (P.kp - P.planes) * 128;  // bytes per block, 16-byte words below
+    for (int idx = threadIdx.x; idx < RT_STAGES * RT_G * (pad / 16); idx += RT_THREADS) {
+      const int blk = idx / (pad / 16), w16 = idx - blk * (pad / 16);  // blk: stage, block
+      *reinterpret_cast<uint4*>(base_ptr + blk * RT_BLOCK + P.planes * 128 + 16 * w16) =
           make_uint4(0u, 0u, 0u, 0u);
     }
   }
@@ -1895,8 +1902,8 @@ __global__ void __launch_bounds__(RT_THREADS, 5)
   // the tensor cores read the weights through the async proxy
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(
-                     smem_u32(tmem_slot))
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)), "n"(2 * RT_G * 32)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -1904,7 +1911,7 @@ __global__ void __launch_bounds__(RT_THREADS, 5)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
-  const uint32_t tile_bytes = uint32_t(128 * P.planes);
+  const uint32_t tile_bytes = uint32_t(RT_G * 128 * P.planes);
   bool copies_pending = false;  // the producer gave up with copies possibly in flight
 
   // unit u = (row block rb, column j), u = rb + j row_blocks: every role walks
@@ -1934,7 +1941,11 @@ __global__ void __launch_bounds__(RT_THREADS, 5)
         break;
       }
       mbar_arrive_expect_tx(full_bar(stage), tile_bytes);
-      tma_load_3d(base + stage * RT_STAGE, &tmR, rb * 128, j, 0, full_bar(stage));
+      // the last group's blocks past m read as zeros (their rows are not stored)
+#pragma unroll
+      for (int g = 0; g < RT_G; ++g)
+        tma_load_3d(base + stage * RT_STAGE + g * RT_BLOCK, &tmR, (rb * RT_G + g) * 128, j, 0,
+                    full_bar(stage));
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer
@@ -1951,9 +1962,12 @@ __global__ void __launch_bounds__(RT_THREADS, 5)
       }
       tc_fence_after();
       const uint32_t sa = base + stage * RT_STAGE;
-      for (int kb = 0; kb < P.kp / 32; ++kb)
-        umma_i8_desc(tmem_base + uint32_t(b * 32), umma_desc_sw128_mn(sa + kb * 4096),
-                     umma_desc_sw128(w_addr + kb * 32), kIdesc, kb > 0 ? 1u : 0u);
+#pragma unroll
+      for (int g = 0; g < RT_G; ++g)
+        for (int kb = 0; kb < P.kp / 32; ++kb)
+          umma_i8_desc(tmem_base + uint32_t((b * RT_G + g) * 32),
+                       umma_desc_sw128_mn(sa + g * RT_BLOCK + kb * 4096),
+                       umma_desc_sw128(w_addr + kb * 32), kIdesc, kb > 0 ? 1u : 0u);
       umma_commit(empty_bar(stage));
       umma_commit(accf_bar(b));
     }
@@ -1973,43 +1987,55 @@ __global__ void __launch_bounds__(RT_THREADS, 5)
          u += gridDim.x, ++it, next_unit(rb, j)) {
       const int b = int(it & 1);
       const uint32_t bpar = uint32_t((it >> 1) & 1);
-      const int i = rb * 128 + quarter * 32 + lane;
       // the scale exponents load while the accumulator is awaited
-      const int si = i < P.m ? P.sigA[i] : 0;
+      int si[RT_G];
+#pragma unroll
+      for (int g = 0; g < RT_G; ++g) {
+        const int i = (rb * RT_G + g) * 128 + quarter * 32 + lane;
+        si[g] = i < P.m ? P.sigA[i] : 0;
+      }
       const int tauj = P.sigB[j];
-      // warp-uniform: the TMEM load and the warp's arrival below are collective
+      // warp-uniform: the TMEM loads and the warp's arrival below are collective
       if (!__all_sync(0xffffffffu, mbar_wait(accf_bar(b), bpar, abort, P.wait_limit_ns))) break;
       tc_fence_after();
       __syncwarp();
-      uint32_t v[32];
-      tmem_ld32(lane_taddr + uint32_t(b * 32), v);
+      uint32_t v[RT_G][32];
+#pragma unroll
+      for (int g = 0; g < RT_G; ++g)
+        tmem_ld32_nowait(lane_taddr + uint32_t((b * RT_G + g) * 32), v[g]);
+      tmem_wait_ld();
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acce_bar(b));  // the accumulator may be overwritten
-      bool active = i < P.m;
-      if (active && P.fill != 0) {
-        const int64_t ti = (i / P.tile_m) * int64_t(P.tile_m);
-        const int64_t tj = (j / P.tile_n) * int64_t(P.tile_n);
-        active = tile_is_active(P.fill, ti, tj, ::min((int64_t)P.tile_m, (int64_t)P.m - ti),
-                                ::min((int64_t)P.tile_n, (int64_t)P.n - tj), P.ro, P.co);
-      }
-      if (active) {
-        // limb L of S = sum of S_j 2^(8 (j - 4L)) over j = 4L .. 4L + 3 (below
-        // 2^47): two 32-bit shift-adds (each below 2^31) and one wide multiply-add
-        auto limb = [&](int j0) {
-          const uint32_t a = v[j0] + (v[j0 + 1] << 8);
-          const uint32_t b = v[j0 + 2] + (v[j0 + 3] << 8);
-          return (unsigned long long)b * 65536ull + a;
-        };
-        const int e = -(si + tauj);
-        double xr =
-            scale_pow2(crt_from_limbs<true>(limb(0), limb(4), limb(8), limb(12), P.rp), e);
-        double xi = 0.0;
-        if (CPLX)
-          xi = scale_pow2(crt_from_limbs<true>(limb(16), limb(20), limb(24), limb(28), P.rp), e);
-        if (si == kSigmaNonFinite || tauj == kSigmaNonFinite)
-          xr = xi = __longlong_as_double(kNaNBits);
-        store_c<DT>(P.C, i + int64_t(j) * P.ldc, xr, xi, P.alr, P.ali, P.ber, P.bei, read_c);
+#pragma unroll
+      for (int g = 0; g < RT_G; ++g) {
+        const int i = (rb * RT_G + g) * 128 + quarter * 32 + lane;
+        bool active = i < P.m;
+        if (active && P.fill != 0) {
+          const int64_t ti = (i / P.tile_m) * int64_t(P.tile_m);
+          const int64_t tj = (j / P.tile_n) * int64_t(P.tile_n);
+          active = tile_is_active(P.fill, ti, tj, ::min((int64_t)P.tile_m, (int64_t)P.m - ti),
+                                  ::min((int64_t)P.tile_n, (int64_t)P.n - tj), P.ro, P.co);
+        }
+        if (active) {
+          // limb L of S = sum of S_j 2^(8 (j - 4L)) over j = 4L .. 4L + 3 (below
+          // 2^47): two 32-bit shift-adds (each below 2^31) and one wide multiply-add
+          auto limb = [&](int j0) {
+            const uint32_t a = v[g][j0] + (v[g][j0 + 1] << 8);
+            const uint32_t bb = v[g][j0 + 2] + (v[g][j0 + 3] << 8);
+            return (unsigned long long)bb * 65536ull + a;
+          };
+          const int e = -(si[g] + tauj);
+          double xr =
+              scale_pow2(crt_from_limbs<true>(limb(0), limb(4), limb(8), limb(12), P.rp), e);
+          double xi = 0.0;
+          if (CPLX)
+            xi = scale_pow2(crt_from_limbs<true>(limb(16), limb(20), limb(24), limb(28), P.rp),
+                            e);
+          if (si[g] == kSigmaNonFinite || tauj == kSigmaNonFinite)
+            xr = xi = __longlong_as_double(kNaNBits);
+          store_c<DT>(P.C, i + int64_t(j) * P.ldc, xr, xi, P.alr, P.ali, P.ber, P.bei, read_c);
+        }
       }
     }
   }
@@ -2026,7 +2052,8 @@ __global__ void __launch_bounds__(RT_THREADS, 5)
   if (warp == 1) {
     __syncwarp();
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem_base)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                 "n"(2 * RT_G * 32)
                  : "memory");
   }
 }
@@ -2532,7 +2559,7 @@ cudaError_t launch_recon_tc(const GemmProblem& p, const oz::Layout& L, const oz:
   P = ReconTcParams{};
   P.m = L.rowsA;
   P.n = int(p.n);
-  P.row_blocks = (P.m + 127) / 128;
+  P.row_blocks = (P.m + 128 * RT_G - 1) / (128 * RT_G);
   P.total_units = (long long)P.row_blocks * P.n;
   P.planes = planes;
   P.kp = planes <= 32 ? 32 : 64;
@@ -2582,10 +2609,8 @@ cudaError_t launch_recon_tc(const GemmProblem& p, const oz::Layout& L, const oz:
   auto run = [&](auto kern) -> cudaError_t {
     const cudaError_t ea = set_dynamic_smem(reinterpret_cast<const void*>(kern), RT_SMEM);
     if (ea != cudaSuccess) return ea;
-    // five CTAs per SM (their shared memory and TMEM fit; measured against
-    // three and four on the complex sbs problem m = 200000, n = k = 2048:
-    // 9.0 against 10.1 and 9.3 ms)
-    const long long grid = std::min<long long>(P.total_units, 5LL * sm_count());
+    // three CTAs per SM (their shared memory fits, and so their TMEM)
+    const long long grid = std::min<long long>(P.total_units, 3LL * sm_count());
     kern<<<unsigned(grid), RT_THREADS, RT_SMEM, st>>>(map, P);
     return cudaGetLastError();
   };
