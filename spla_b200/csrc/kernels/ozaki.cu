@@ -2088,10 +2088,11 @@ bool mn_fits(const GemmProblem& p) {
 }
 
 // k-slices of the in-place row norms: about 2^18 threads in all (one per row
-// and slice), slices of at least 512 elements
+// and slice), slices of at least 512 elements, at most 4096 slices (the grid's
+// y extent)
 int norm_slices(int64_t rows, int64_t k) {
   if (rows >= kMnRows || k <= 512) return 1;
-  const int64_t want = ((int64_t(1) << 18) + rows - 1) / rows;
+  const int64_t want = std::min<int64_t>(((int64_t(1) << 18) + rows - 1) / rows, 4096);
   return int(std::max<int64_t>(1, std::min<int64_t>(want, (k + 511) / 512)));
 }
 

@@ -460,6 +460,7 @@ def test_tensor_core_reconstruction_matches_staged(dt, m, n, k, opA, fill, modul
     ("float64", 1, 1, 190, 210, 30000, 2, False),
     ("complex64", 0, 2, 150, 170, 20000, 0, False),
     ("float32", 0, 1, 100, 90, 50000, 0, False),
+    ("float64", 0, 0, 4, 8, 4_000_000, 0, False),         # 4096 k-slices (the grid's limit)
 ])
 def test_in_place_operands(dt, opA, opB, m, n, k, pad, offset):
     """op(A) = N and op(B) = T or C are read in place (m- and n-major rows):

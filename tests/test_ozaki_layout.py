@@ -46,7 +46,7 @@ def norm_slices(rows, k):
     """k-slices of the in-place row norms (about 2^18 threads, >= 512 elements each)"""
     if rows >= 65536 or k <= 512:
         return 1
-    return max(1, min(-(-(1 << 18) // rows), -(-k // 512)))
+    return max(1, min(-(-(1 << 18) // rows), 4096, -(-k // 512)))
 
 
 def partials(rows, k):
@@ -63,6 +63,10 @@ def test_in_place_operands_need_no_copy():
         assert abs(diff - partials(n, k)) <= 512
     # many rows: the norms are not sliced
     assert ws("complex128", 0, 70000, 64, 2048) - ws("complex128", 1, 70000, 64, 2048) == 0
+    # a few rows and a long k: at most 4096 slices (the launch grid's y extent)
+    m, k = 4, 4_000_000
+    diff = ws("float64", 0, m, 8, k) - ws("float64", 1, m, 8, k)
+    assert abs(diff - partials(m, k)) <= 512 and norm_slices(m, k) == 4096
 
 
 def test_modulus_count():
