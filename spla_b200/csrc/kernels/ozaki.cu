@@ -125,16 +125,12 @@ __device__ __forceinline__ void scaled_add(double& S, int& E, double S2, int E2)
   }
 }
 
+// Sum of squares of x[0 .. len), thread t taking t, t + blockDim.x, ...,
+// into (S, E, inv): batches of 8 independent loads (memory-level
+// parallelism), one exponent check per batch.
 template <typename TIn>
-__global__ void oz_row_scale(const TIn* __restrict__ X, int64_t ld_elems, int64_t len, int rows,
-                             int q_bits, int* __restrict__ sigma) {
-  const int row = blockIdx.x;
-  if (row >= rows) return;
-  const TIn* x = X + int64_t(row) * ld_elems;
-  double S = 0.0, inv = 0.0;  // sum of (v 2^-E)^2, and 2^-E
-  int E = -2100;              // below any exponent: the first batch sets it
-  // batches of 8 independent loads (memory-level parallelism), one exponent
-  // check per batch
+__device__ __forceinline__ void ssq_row(const TIn* __restrict__ x, int64_t len, double& S, int& E,
+                                        double& inv) {
   const int64_t step = blockDim.x;
   int64_t l = threadIdx.x;
   for (; l + 7 * step < len; l += 8 * step) {
@@ -166,8 +162,40 @@ __global__ void oz_row_scale(const TIn* __restrict__ X, int64_t ld_elems, int64_
     const double w = v * inv;
     S = fma(w, w, S);
   }
-  __shared__ double redS[32];
-  __shared__ int redE[32];
+}
+
+// Sum of squares of a sample of a row: nruns runs of run reals, gap apart;
+// blockDim.x / nruns threads per run (blockDim.x a multiple of nruns),
+// batches of 8 independent loads along it (the runs are short).
+template <typename TIn>
+__device__ __forceinline__ void ssq_sample(const TIn* __restrict__ x, int nruns, int64_t run,
+                                           int64_t gap, double& S, int& E, double& inv) {
+  const int gsz = int(blockDim.x) / nruns;
+  const int c = int(threadIdx.x) / gsz;
+  if (c >= nruns) return;
+  x += c * gap;
+  for (int64_t l = threadIdx.x % gsz; l < run; l += 8 * gsz) {
+    double v[8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) v[b] = l + b * gsz < run ? double(x[l + b * gsz]) : 0.0;
+    int em = exponent_of(v[0]);
+#pragma unroll
+    for (int b = 1; b < 8; ++b) em = max(em, exponent_of(v[b]));
+    if (em > E) {
+      S = ldexp(S, 2 * (E - em));
+      E = em;
+      inv = ldexp(1.0, -E);
+    }
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const double w = v[b] * inv;
+      S = fma(w, w, S);
+    }
+  }
+}
+
+// The block's (S, E) summed into thread 0's (blocks of at most 1024 threads)
+__device__ __forceinline__ void block_ssq(double& S, int& E, double* redS, int* redE) {
   for (int o = 16; o > 0; o >>= 1) {
     const double S2 = __shfl_xor_sync(0xffffffffu, S, o);
     const int E2 = __shfl_xor_sync(0xffffffffu, E, o);
@@ -187,6 +215,59 @@ __global__ void oz_row_scale(const TIn* __restrict__ X, int64_t ld_elems, int64_
       const int E2 = __shfl_xor_sync(0xffffffffu, E, o);
       scaled_add(S, E, S2, E2);
     }
+  }
+}
+
+// Estimated norms whose mantissa (in [0.5, 1)) lies within this relative
+// distance of either end of its octave take the exact norm instead.
+constexpr double kEstimateBand = 1.0 / 32;
+
+// One block per row (with a list, the blocks walk the rows list[0 .. *count
+// - 1], grid-stride; else block b takes row b); len reals per row.
+// With nruns > 0 the row's exponent is first estimated from a sample (nruns
+// runs of run reals, gap apart; the sum of squares extrapolated to len
+// reals) and kept when its norm's mantissa is clear of the octave's ends by
+// kEstimateBand (exact[row] = 0); otherwise, and for a zero or non-finite
+// sample, the whole row is read (exact[row] = 1) as without a sample.
+template <typename TIn>
+__global__ void oz_row_scale(const TIn* __restrict__ X, int64_t ld_elems, int64_t len, int rows,
+                             int q_bits, int* __restrict__ sigma,
+                             const int* __restrict__ list = nullptr,
+                             const int* __restrict__ count = nullptr, int nruns = 0,
+                             int64_t run = 0, int64_t gap = 0, int* __restrict__ exact = nullptr) {
+  __shared__ double redS[32];
+  __shared__ int redE[32];
+  __shared__ int use_estimate;
+  const int nwork = list ? *count : min(rows, int(gridDim.x));
+  for (int bi = blockIdx.x; bi < nwork; bi += gridDim.x) {
+    const int row = list ? list[bi] : bi;
+    const TIn* x = X + int64_t(row) * ld_elems;
+    double S = 0.0, inv = 0.0;  // sum of (v 2^-E)^2, and 2^-E
+    int E = -2100;              // below any exponent: the first batch sets it
+    if (nruns > 0) {
+      ssq_sample(x, nruns, run, gap, S, E, inv);
+      block_ssq(S, E, redS, redE);
+      if (threadIdx.x == 0) {
+        bool use = false;
+        if (S > 0.0 && S < 1e300) {
+          int e0 = 0;
+          const double f = frexp(sqrt(S * (double(len) / double(nruns * run))), &e0);
+          use = f > 0.5 * (1.0 + kEstimateBand) && f < 1.0 - kEstimateBand;
+          if (use) sigma[row] = q_bits - (e0 + E);
+        }
+        exact[row] = use ? 0 : 1;
+        use_estimate = use;
+      }
+      __syncthreads();
+      const bool done = use_estimate;
+      S = 0.0;
+      inv = 0.0;
+      E = -2100;
+      if (done) continue;  // block-uniform; the next row's first barrier
+                           // comes after this row's last read of use_estimate
+    }
+    ssq_row(x, len, S, E, inv);
+    block_ssq(S, E, redS, redE);
     if (threadIdx.x == 0) {
       if (!(S < 1e300)) {  // NaN or infinite input
         sigma[row] = kSigmaNonFinite;
@@ -198,6 +279,7 @@ __global__ void oz_row_scale(const TIn* __restrict__ X, int64_t ld_elems, int64_
         sigma[row] = 0;
       }
     }
+    __syncthreads();  // redS / redE are reused by the block's next row
   }
 }
 
@@ -313,12 +395,18 @@ __device__ __forceinline__ uint32_t pack4(float a, float b, float c, float d) {
 // The work of one slicing thread once its EL reals (of one row, starting at
 // real l0) are loaded: scaling by 2^sg, digits, and for every modulus the
 // residues written to res_row + l0 (mode 0) or, in mode 2, to the three
-// planes `plane` bytes apart at complex offset l0 / 2.
-template <typename TIn, int NDIG, int EL, int NMU, int MODE>
+// planes `plane` bytes apart at complex offset l0 / 2. SSQ: the sum of
+// squares of the scaled values is handed to on_ssq once the digits are made
+// (so that it is not kept in registers through the residue loop).
+struct NoSsq {
+  __device__ void operator()(double) const {}
+};
+template <typename TIn, int NDIG, int EL, int NMU, int MODE, bool SSQ = false,
+          typename OnSsq = NoSsq>
 __device__ __forceinline__ void slice_thread(double (&v)[EL], int sg, int8_t* res_row,
                                              int64_t l0, int64_t plane, int s_sum,
                                              int64_t res_mod_stride, const SliceConsts& sc,
-                                             int t_begin, int t_end) {
+                                             int t_begin, int t_end, OnSsq on_ssq = {}) {
   static_assert(EL == 8 || EL == 16, "8 or 16 reals per thread");
   static_assert(MODE == 0 || MODE == 2, "real rows or complex rows");
   constexpr int W = EL / 4;  // packed words per modulus
@@ -326,6 +414,7 @@ __device__ __forceinline__ void slice_thread(double (&v)[EL], int sg, int8_t* re
   const bool direct = sg > -1000 && sg < 1000;
   const double scale = direct ? __longlong_as_double((long long)(sg + 1023) << 52) : 1.0;
   unsigned long long dp[EL / 2][5];  // digits of the element pairs (see below)
+  double ssq = 0.0;
   {
     // pairs (2i, 2i + 1) in mode 0; in mode 2 the real parts pair up first,
     // then the imaginary parts: (re0, re1), (re2, re3), ..., (im0, im1), ...
@@ -342,11 +431,15 @@ __device__ __forceinline__ void slice_thread(double (&v)[EL], int sg, int8_t* re
 #pragma unroll
     for (int i = 0; i < EL / 2; ++i) {
       float d0[5], d1[5];
-      digits13<NDIG>(direct ? v[2 * i] * scale : ldexp(v[2 * i], sg), d0);
-      digits13<NDIG>(direct ? v[2 * i + 1] * scale : ldexp(v[2 * i + 1], sg), d1);
+      const double y0 = direct ? v[2 * i] * scale : ldexp(v[2 * i], sg);
+      const double y1 = direct ? v[2 * i + 1] * scale : ldexp(v[2 * i + 1], sg);
+      if constexpr (SSQ) ssq = fma(y1, y1, fma(y0, y0, ssq));
+      digits13<NDIG>(y0, d0);
+      digits13<NDIG>(y1, d1);
 #pragma unroll
       for (int j = 0; j < 5; ++j) dp[i][j] = f2_pack(d0[j], d1[j]);
     }
+    if constexpr (SSQ) on_ssq(ssq);
   }
   const unsigned long long M2 = f2_pack(kMagic, kMagic), NM2 = f2_pack(-kMagic, -kMagic);
   int8_t* const out0 = res_row + l0;
@@ -451,18 +544,10 @@ __device__ __forceinline__ void slice_thread(double (&v)[EL], int sg, int8_t* re
 // constants become fixed parameter operands); 0: t_begin .. t_end-1 in a loop.
 // MODE (0 or 2, the mode above) is a template parameter so that the unrolled
 // modulus loop carries no branch on it.
-template <typename TIn, bool VEC, int NDIG, int EL, int NMU, int MODE>
-__global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
-    oz_slice(const TIn* __restrict__ X, int64_t ld_doubles, int64_t len, int rows, int64_t kp,
-             const int* __restrict__ sigma, int s_sum, int8_t* __restrict__ res,
-             int64_t res_mod_stride, SliceConsts sc, int t_begin, int t_end) {
-  const int64_t groups = (MODE == 2 ? 2 * kp : kp) / EL;
-  const int64_t gid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  const int row = int(gid / groups);
-  if (row >= rows) return;
-  const int64_t l0 = (gid % groups) * EL;
-  const TIn* x = X + int64_t(row) * ld_doubles + l0;
-  double v[EL];
+// The EL reals of one row at real l0 (zeros past len); VEC: 16-byte loads.
+template <typename TIn, bool VEC, int EL>
+__device__ __forceinline__ void load_reals(const TIn* __restrict__ x, int64_t l0, int64_t len,
+                                           double (&v)[EL]) {
   if (VEC && l0 + EL <= len) {
     if constexpr (sizeof(TIn) == 8) {
 #pragma unroll
@@ -485,9 +570,105 @@ __global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
 #pragma unroll
     for (int i = 0; i < EL; ++i) v[i] = (l0 + i < len) ? double(x[i]) : 0.0;
   }
-  slice_thread<TIn, NDIG, EL, NMU, MODE>(v, sigma[row], res + int64_t(row) * kp, l0,
-                                         int64_t(rows) * kp, s_sum, res_mod_stride, sc, t_begin,
-                                         t_end);
+}
+
+// SSQ: also adds each row's sum of squares of the scaled values to
+// rowssq[row] (one atomic per row and block; blocks of 256 threads).
+template <typename TIn, bool VEC, int NDIG, int EL, int NMU, int MODE, bool SSQ = false>
+__global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
+    oz_slice(const TIn* __restrict__ X, int64_t ld_doubles, int64_t len, int rows, int64_t kp,
+             const int* __restrict__ sigma, int s_sum, int8_t* __restrict__ res,
+             int64_t res_mod_stride, SliceConsts sc, int t_begin, int t_end,
+             double* __restrict__ rowssq) {
+  const int64_t groups = (MODE == 2 ? 2 * kp : kp) / EL;
+  const int64_t gid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if constexpr (!SSQ) {
+    const int row = int(gid / groups);
+    if (row >= rows) return;
+    const int64_t l0 = (gid % groups) * EL;
+    double v[EL];
+    load_reals<TIn, VEC, EL>(X + int64_t(row) * ld_doubles + l0, l0, len, v);
+    slice_thread<TIn, NDIG, EL, NMU, MODE>(v, sigma[row], res + int64_t(row) * kp, l0,
+                                           int64_t(rows) * kp, s_sum, res_mod_stride, sc, t_begin,
+                                           t_end);
+  } else {
+    // Threads past the last row redo the last row's last groups (the same
+    // bytes to the same places) so that every thread takes part in the
+    // reductions; their sums count as zero. Aligned segments of W lanes (W
+    // the largest power of two dividing groups, at most 32; at least 8,
+    // groups being kp / 8 or kp / 16 with kp a multiple of 128) hold one row
+    // each: reduced by shuffles, then the block's segments of one row
+    // together, one atomic per row and block (atomics from every warp on the
+    // few rows the resident blocks share would serialise).
+    __shared__ double seg_sum[32];
+    __shared__ int seg_row[32];
+    const int W = int(groups & -groups) < 32 ? int(groups & -groups) : 32;
+    const int nseg = int(blockDim.x) / W;  // blocks of 256 threads: at most 32
+    const int row_in = int(gid / groups);
+    const int64_t g_in = gid % groups;
+    const bool past = row_in >= rows;
+    const int row = past ? rows - 1 : row_in;
+    const int64_t l0 = (past ? groups - W + (g_in & (W - 1)) : g_in) * EL;
+    double v[EL];
+    load_reals<TIn, VEC, EL>(X + int64_t(row) * ld_doubles + l0, l0, len, v);
+    auto on_ssq = [&](double ssq) {
+      if (past) ssq = 0.0;
+      for (int o = 16; o > 0; o >>= 1)
+        if (o < W) ssq += __shfl_xor_sync(0xffffffffu, ssq, o);
+      if ((threadIdx.x & (W - 1)) == 0) {
+        seg_sum[threadIdx.x / W] = ssq;
+        seg_row[threadIdx.x / W] = past ? -1 : row;
+      }
+    };
+    slice_thread<TIn, NDIG, EL, NMU, MODE, true>(v, sigma[row], res + int64_t(row) * kp, l0,
+                                                 int64_t(rows) * kp, s_sum, res_mod_stride, sc,
+                                                 t_begin, t_end, on_ssq);
+    __syncthreads();
+    if (int(threadIdx.x) < nseg) {
+      const int sgi = threadIdx.x, r = seg_row[sgi];
+      if (r >= 0 && (sgi == 0 || seg_row[sgi - 1] != r)) {  // first segment of its row
+        double t = 0.0;
+        for (int u = sgi; u < nseg && seg_row[u] == r; ++u) t += seg_sum[u];
+        atomicAdd(rowssq + r, t);
+      }
+    }
+  }
+}
+
+// oz_slice over the rows list[0 .. *count - 1] (grid-stride over their
+// thread groups): the rows the one-pass check sent back (see oz_onepass_check)
+template <typename TIn, bool VEC, int NDIG, int EL, int NMU, int MODE>
+__global__ void __launch_bounds__(256, EL == 8 ? 4 : 2)
+    oz_slice_rows(const TIn* __restrict__ X, int64_t ld_doubles, int64_t len, int rows,
+                  int64_t kp, const int* __restrict__ sigma, int s_sum,
+                  int8_t* __restrict__ res, int64_t res_mod_stride, SliceConsts sc,
+                  const int* __restrict__ list, const int* __restrict__ count) {
+  const int64_t groups = (MODE == 2 ? 2 * kp : kp) / EL;
+  const int64_t total = int64_t(*count) * groups;
+  for (int64_t gid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; gid < total;
+       gid += int64_t(gridDim.x) * blockDim.x) {
+    const int row = list[gid / groups];
+    const int64_t l0 = (gid % groups) * EL;
+    double v[EL];
+    load_reals<TIn, VEC, EL>(X + int64_t(row) * ld_doubles + l0, l0, len, v);
+    slice_thread<TIn, NDIG, EL, NMU, MODE>(v, sigma[row], res + int64_t(row) * kp, l0,
+                                           int64_t(rows) * kp, s_sum, res_mod_stride, sc, 0, NMU);
+  }
+}
+
+// One-pass row scaling: a row whose exponent was estimated (exact[i] = 0)
+// keeps it when its sum of squares at that scale lies within [lo, hi] (the
+// exponent is then the exact one, and clear of the rounding of the sum);
+// otherwise (the estimate was off, the row is zero or not finite, or the sum
+// lies near an exponent boundary) it is listed for its exact norm and a
+// second slicing.
+__global__ void oz_onepass_check(const double* __restrict__ ssq, const int* __restrict__ exact,
+                                 int rows, double lo, double hi, int* __restrict__ list,
+                                 int* __restrict__ count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows) return;
+  const double S = ssq[i];
+  if (!exact[i] && !(S >= lo && S <= hi)) list[atomicAdd(count, 1)] = i;
 }
 
 // --------------------------------------------------------------------------
@@ -2074,6 +2255,8 @@ struct Layout {
   int64_t ldAt;            // leading dimension of At (elements of A's type)
   size_t off_sigA, off_sigB, off_resA, off_resB, off_R, off_At, off_status, off_tiles;
   size_t off_partA, off_partB;  // k-slice partial sums of the in-place row norms
+  size_t off_ssq, off_list;     // one-pass row scaling (onepass_applies): scaled sums
+                                // of squares, rows sent back and their two counts
   size_t total;
 };
 
@@ -2137,6 +2320,10 @@ Layout layout_of(const GemmProblem& p, int moduli) {
   off = align256(off + (L.ksA > 1 ? size_t(L.ksA) * L.rowsA * (sizeof(double) + sizeof(int)) : 0));
   L.off_partB = off;
   off = align256(off + (L.ksB > 1 ? size_t(L.ksB) * L.rowsB * (sizeof(double) + sizeof(int)) : 0));
+  L.off_ssq = off;  // A's rows, then B's
+  off = align256(off + sizeof(double) * (size_t(L.rowsA) + L.rowsB));
+  L.off_list = off;  // lists of A's and B's rows, their exact flags, the two counts
+  off = align256(off + sizeof(int) * (2 * (size_t(L.rowsA) + L.rowsB) + 2));
   L.total = off;
   return L;
 }
@@ -2229,36 +2416,41 @@ bool slice_unroll() {
 template <typename TIn, bool VEC, int EL, int MODE>
 void launch_slice_el(int ndig, unsigned grid, cudaStream_t st, const TIn* X, int64_t ld,
                      int64_t len, int rows, int64_t kp, const int* sig, int s_sign, int8_t* res,
-                     int64_t stride, const oz::SliceConsts& sc, int t0, int t1) {
+                     int64_t stride, const oz::SliceConsts& sc, int t0, int t1, double* ssq) {
   using namespace oz;
   constexpr int kNU = sizeof(TIn) == 8 ? kDefaultModuli : kDefaultModuliFloat;
   constexpr int kDigU = sizeof(TIn) == 8 ? 4 : 3;  // digits of the default scaling
   if (t0 == 0 && t1 == kNU && sc.n == kNU && ndig == kDigU && slice_unroll()) {
-    oz_slice<TIn, VEC, kDigU, EL, kNU, MODE>
-        <<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1);
+    if (ssq)
+      oz_slice<TIn, VEC, kDigU, EL, kNU, MODE, true><<<grid, 256, 0, st>>>(
+          X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1, ssq);
+    else
+      oz_slice<TIn, VEC, kDigU, EL, kNU, MODE><<<grid, 256, 0, st>>>(
+          X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1, nullptr);
     return;
   }
   if (ndig <= 3)
-    oz_slice<TIn, VEC, 3, EL, 0, MODE>
-        <<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1);
+    oz_slice<TIn, VEC, 3, EL, 0, MODE><<<grid, 256, 0, st>>>(
+        X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1, nullptr);
   else if (ndig == 4)
-    oz_slice<TIn, VEC, 4, EL, 0, MODE>
-        <<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1);
+    oz_slice<TIn, VEC, 4, EL, 0, MODE><<<grid, 256, 0, st>>>(
+        X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1, nullptr);
   else
-    oz_slice<TIn, VEC, 5, EL, 0, MODE>
-        <<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1);
+    oz_slice<TIn, VEC, 5, EL, 0, MODE><<<grid, 256, 0, st>>>(
+        X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1, nullptr);
 }
 
+// ssq (unrolled default scaling only): also the rows' scaled sums of squares
 template <typename TIn, bool VEC>
 void launch_slice(int ndig, cudaStream_t st, const TIn* X, int64_t ld, int64_t len, int rows,
                   int64_t kp, const int* sig, int mode, int s_sign, int8_t* res, int64_t stride,
-                  const oz::SliceConsts& sc, int t0, int t1) {
+                  const oz::SliceConsts& sc, int t0, int t1, double* ssq = nullptr) {
   const int el = slice_elems();
   const int64_t kreal = mode == 2 ? 2 * kp : kp;  // reals per row a thread group covers
   const unsigned grid = unsigned((int64_t(rows) * (kreal / el) + 255) / 256);
   auto run = [&](auto el_tag, auto mode_tag) {
     launch_slice_el<TIn, VEC, decltype(el_tag)::value, decltype(mode_tag)::value>(
-        ndig, grid, st, X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1);
+        ndig, grid, st, X, ld, len, rows, kp, sig, s_sign, res, stride, sc, t0, t1, ssq);
   };
   using E8 = std::integral_constant<int, 8>;
   using E16 = std::integral_constant<int, 16>;
@@ -2399,11 +2591,39 @@ cudaError_t launch_slice_tc(const double* X, int64_t ld, int64_t len, int rows, 
   return cudaGetLastError();
 }
 
+// Slicer constants of the moduli, and the digit count covering |x| <= 2^Q:
+// 3 of 13 bits, 4 balanced of 15 bits, or 5 of 13.
+oz::SliceConsts slice_consts(const oz::Layout& L, const oz::Crt& crt, int* ndig_out) {
+  using namespace oz;
+  SliceConsts sc{};
+  sc.n = L.nmod;
+  sc.p0 = float(crt.p[0]);
+  for (int t = 0; t < L.nmod; ++t) {
+    const int pt = crt.p[t];
+    sc.neg_p[t] = f2_pack(-float(pt), -float(pt));
+    sc.inv_p[t] = f2_pack(1.0f / float(pt), 1.0f / float(pt));
+  }
+  const int ndig = crt.q_bits + 1 <= 39 ? 3 : (crt.q_bits + 1 <= 58 ? 4 : 5);
+  const long long base = ndig == 4 ? 32768 : 8192;
+  for (int t = 0; t < L.nmod; ++t) {
+    const int pt = crt.p[t];
+    long long w = 1;
+    for (int i = 0; i < 4; ++i) {
+      w = (w * base) % pt;  // base^(i+1) mod p
+      const float c = float(w > pt / 2 ? w - pt : w);
+      sc.c[t][i] = f2_pack(c, c);
+    }
+  }
+  *ndig_out = ndig;
+  return sc;
+}
+
 // Residues of moduli t0 .. t1-1 of A (which & 1) and B (which & 2).
 template <typename TIn>
 void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
                     const int* sigA, const int* sigB, int8_t* resA, int8_t* resB, int t0, int t1,
-                    int which, cudaStream_t st, int* status) {
+                    int which, cudaStream_t st, int* status, double* ssqA = nullptr,
+                    double* ssqB = nullptr) {
   using namespace oz;
   const TIn* A = static_cast<const TIn*>(p.A);
   const TIn* B = static_cast<const TIn*>(p.B);
@@ -2426,26 +2646,8 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
       return;
     }
   }
-  SliceConsts sc{};
-  sc.n = L.nmod;
-  sc.p0 = float(crt.p[0]);
-  for (int t = 0; t < L.nmod; ++t) {
-    const int pt = crt.p[t];
-    sc.neg_p[t] = f2_pack(-float(pt), -float(pt));
-    sc.inv_p[t] = f2_pack(1.0f / float(pt), 1.0f / float(pt));
-  }
-  // digits covering |x| <= 2^Q: 3 of 13 bits, 4 balanced of 15 bits, or 5 of 13
-  const int ndig = crt.q_bits + 1 <= 39 ? 3 : (crt.q_bits + 1 <= 58 ? 4 : 5);
-  const long long base = ndig == 4 ? 32768 : 8192;
-  for (int t = 0; t < L.nmod; ++t) {
-    const int pt = crt.p[t];
-    long long w = 1;
-    for (int i = 0; i < 4; ++i) {
-      w = (w * base) % pt;  // base^(i+1) mod p
-      const float c = float(w > pt / 2 ? w - pt : w);
-      sc.c[t][i] = f2_pack(c, c);
-    }
-  }
+  int ndig = 0;
+  const SliceConsts sc = slice_consts(L, crt, &ndig);
   const int vec_elems = 16 / int(sizeof(TIn));
   const bool vecA = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (ldA % vec_elems == 0);
   const bool vecB = (reinterpret_cast<uintptr_t>(B) % 16 == 0) && (ldB % vec_elems == 0);
@@ -2460,19 +2662,136 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
                          strideA, sc, t0, t1);
   else if ((which & 1) && vecA)
     launch_slice<TIn, true>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, mode, sumA, resA,
-                            strideA, sc, t0, t1);
+                            strideA, sc, t0, t1, ssqA);
   else if (which & 1)
     launch_slice<TIn, false>(ndig, st, A, ldA, L.K2, L.rowsA, L.kp, sigA, mode, sumA, resA,
-                             strideA, sc, t0, t1);
+                             strideA, sc, t0, t1, ssqA);
   if ((which & 2) && L.mnB)  // op(B) = T or C: n-major rows, conjugated for C
     launch_slice_mn<TIn>(ndig, st, B, p.ldb, L.rowsB, p.k, L.kp, sigB, mode, 1,
                          p.opB == 2 ? 1 : 0, resB, strideB, sc, t0, t1);
   else if ((which & 2) && vecB)
     launch_slice<TIn, true>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, mode, 1, resB, strideB,
-                            sc, t0, t1);
+                            sc, t0, t1, ssqB);
   else if (which & 2)
     launch_slice<TIn, false>(ndig, st, B, ldB, L.K2, L.rowsB, L.kp, sigB, mode, 1, resB, strideB,
-                             sc, t0, t1);
+                             sc, t0, t1, ssqB);
+}
+
+// One-pass row scaling. The two-pass order reads every row twice: once for
+// its norm (the scale exponent), once to slice it. Here the exponent comes
+// from a sample of each row (16 evenly spread runs, 1/16 of its reals, the
+// sum of squares extrapolated to the whole row) unless the estimated norm
+// lies within kEstimateBand of a power of two, or the sample is zero or not
+// finite: such rows (all of them for rows normalised to 1) take the exact
+// norm at once. The default slicer also sums the squares of the scaled
+// values, and an estimated exponent stands when that sum lies in
+// [2^(2Q-2), 2^(2Q)) with a relative margin of 2^-30 at both ends (far above
+// the rounding of either sum): the scaled norm then lies in [2^(Q-1), 2^Q),
+// which is what the exact exponent gives. Other rows (a sample that
+// misjudged the row by more than the band) get the exact norm and are
+// sliced again. Each row thus ends with the exponent and residues of the
+// two-pass order, whatever the order of the atomic sums. Used for k-major A
+// and B, the default modulus count and unrolled slicer, one modulus group
+// and rows of at least kOnePassMinLen reals; SPLAB_OZAKI_ONEPASS=0 (read per
+// call) keeps the two-pass order.
+constexpr int64_t kOnePassMinLen = 131072;
+constexpr int kOnePassRuns = 16;
+
+bool onepass_applies(const oz::Layout& L, const GemmProblem& p, int groups) {
+  const char* v = std::getenv("SPLAB_OZAKI_ONEPASS");
+  if (v && v[0] == '0') return false;
+  const int nu = dtype_is_double(p.dtype) ? oz::kDefaultModuli : oz::kDefaultModuliFloat;
+  return p.k > 0 && !L.mn && !L.mnB && groups == 1 && L.nmod == nu && slice_unroll() &&
+         !slice_tc_enabled() && L.K2 >= kOnePassMinLen;
+}
+
+// Exponents of A's (which & 1) and B's (which & 2) rows, estimated from the
+// sample where that is safe, else exact (exact[row] = 1; p reads A k-major)
+template <typename TIn>
+void onepass_estimate(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
+                      int* sigA, int* sigB, int* exactA, int* exactB, int which,
+                      cudaStream_t st) {
+  const int64_t run = (L.K2 / (16 * kOnePassRuns) + 7) / 8 * 8;  // reals per run
+  const int64_t gap = L.K2 / kOnePassRuns;                         // run starts
+  const int64_t ldA = cplx ? 2 * p.lda : p.lda, ldB = cplx ? 2 * p.ldb : p.ldb;
+  if (which & 1)
+    oz::oz_row_scale<TIn><<<L.rowsA, 256, 0, st>>>(static_cast<const TIn*>(p.A), ldA, L.K2,
+                                                   L.rowsA, crt.q_bits, sigA, nullptr, nullptr,
+                                                   kOnePassRuns, run, gap, exactA);
+  if (which & 2)
+    oz::oz_row_scale<TIn><<<L.rowsB, 256, 0, st>>>(static_cast<const TIn*>(p.B), ldB, L.K2,
+                                                   L.rowsB, crt.q_bits, sigB, nullptr, nullptr,
+                                                   kOnePassRuns, run, gap, exactB);
+}
+
+template <typename TIn, bool VEC, int EL, int MODE>
+void launch_slice_rows_el(cudaStream_t st, const TIn* X, int64_t ld, int64_t len, int rows,
+                          int64_t kp, const int* sig, int s_sign, int8_t* res, int64_t stride,
+                          const oz::SliceConsts& sc, const int* list, const int* count) {
+  using namespace oz;
+  constexpr int kNU = sizeof(TIn) == 8 ? kDefaultModuli : kDefaultModuliFloat;
+  constexpr int kDigU = sizeof(TIn) == 8 ? 4 : 3;
+  const unsigned grid = unsigned((EL == 8 ? 4 : 2) * sm_count());  // one resident wave
+  oz_slice_rows<TIn, VEC, kDigU, EL, kNU, MODE>
+      <<<grid, 256, 0, st>>>(X, ld, len, rows, kp, sig, s_sign, res, stride, sc, list, count);
+}
+
+// The listed rows of one operand: exact exponent, then residues again
+template <typename TIn>
+void onepass_redo(const oz::Layout& L, const oz::Crt& crt, const oz::SliceConsts& sc,
+                  const TIn* X, int64_t ld, int rows, int* sig, int s_sign, int8_t* res,
+                  int64_t stride, int mode, const int* list, const int* count, cudaStream_t st) {
+  oz::oz_row_scale<TIn><<<unsigned(std::min(rows, 2 * oz::sm_count())), 256, 0, st>>>(
+      X, ld, L.K2, rows, crt.q_bits, sig, list, count);
+  const bool vec = reinterpret_cast<uintptr_t>(X) % 16 == 0 && ld % (16 / int(sizeof(TIn))) == 0;
+  auto run = [&](auto vec_tag, auto el_tag, auto mode_tag) {
+    launch_slice_rows_el<TIn, decltype(vec_tag)::value, decltype(el_tag)::value,
+                         decltype(mode_tag)::value>(st, X, ld, L.K2, rows, L.kp, sig, s_sign,
+                                                    res, stride, sc, list, count);
+  };
+  using T = std::true_type;
+  using F = std::false_type;
+  using E8 = std::integral_constant<int, 8>;
+  using E16 = std::integral_constant<int, 16>;
+  using M0 = std::integral_constant<int, 0>;
+  using M2 = std::integral_constant<int, 2>;
+  const bool e16 = slice_elems() == 16;
+  if (vec) {
+    if (e16) mode == 2 ? run(T{}, E16{}, M2{}) : run(T{}, E16{}, M0{});
+    else mode == 2 ? run(T{}, E8{}, M2{}) : run(T{}, E8{}, M0{});
+  } else {
+    if (e16) mode == 2 ? run(F{}, E16{}, M2{}) : run(F{}, E16{}, M0{});
+    else mode == 2 ? run(F{}, E8{}, M2{}) : run(F{}, E8{}, M0{});
+  }
+}
+
+// Check of A's and B's rows after slicing with their sums of squares, and
+// the second pass over the rows it lists
+template <typename TIn>
+void onepass_fixup(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
+                   int* sigA, int* sigB, int8_t* resA, int8_t* resB, double* ssq, int* list,
+                   cudaStream_t st) {
+  using namespace oz;
+  const double lo = std::ldexp(1.0 + std::ldexp(1.0, -30), 2 * crt.q_bits - 2);
+  const double hi = std::ldexp(1.0 - std::ldexp(1.0, -30), 2 * crt.q_bits);
+  int* listA = list;
+  int* listB = list + L.rowsA;
+  const int* exactA = list + L.rowsA + L.rowsB;
+  const int* exactB = exactA + L.rowsA;
+  int* cnt = list + 2 * (L.rowsA + L.rowsB);  // A's count, B's count
+  oz_onepass_check<<<unsigned((L.rowsA + 255) / 256), 256, 0, st>>>(ssq, exactA, L.rowsA, lo, hi,
+                                                                   listA, cnt);
+  oz_onepass_check<<<unsigned((L.rowsB + 255) / 256), 256, 0, st>>>(
+      ssq + L.rowsA, exactB, L.rowsB, lo, hi, listB, cnt + 1);
+  int ndig = 0;
+  const SliceConsts sc = slice_consts(L, crt, &ndig);
+  const int mode = cplx ? 2 : 0;
+  const int64_t ldA = cplx ? 2 * p.lda : p.lda, ldB = cplx ? 2 * p.ldb : p.ldb;
+  onepass_redo<TIn>(L, crt, sc, static_cast<const TIn*>(p.A), ldA, L.rowsA, sigA,
+                    p.opA == 2 ? -1 : 1, resA, int64_t(L.nsub) * L.rowsA * L.kp, mode, listA,
+                    cnt, st);
+  onepass_redo<TIn>(L, crt, sc, static_cast<const TIn*>(p.B), ldB, L.rowsB, sigB, 1, resB,
+                    int64_t(L.nsub) * L.nb * L.kp, mode, listB, cnt + 1, st);
 }
 
 // Side streams may be used by this host thread (off while a batch captures
@@ -2683,9 +3002,13 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
     const char* v = std::getenv("SPLAB_OZAKI_SIDE_NORMS");
     return !(v && v[0] == '0');
   }();
-  PipeStreams* ps = (p.k > 0 && (groups > 1 || (big && side_norms)) && t_side_streams)
-                        ? pipe_streams()
-                        : nullptr;
+  const bool onepass = onepass_applies(L, p, groups);
+  double* ssq = reinterpret_cast<double*>(w + L.off_ssq);
+  int* oplist = reinterpret_cast<int*>(w + L.off_list);
+  PipeStreams* ps =
+      (p.k > 0 && (groups > 1 || (big && side_norms)) && t_side_streams)
+          ? pipe_streams()
+          : nullptr;
   std::unique_lock<std::mutex> lk;
   if (ps) lk = std::unique_lock<std::mutex>(ps->mu);
   auto scale = [&](int which, cudaStream_t s) {
@@ -2700,7 +3023,31 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
     if ((e = transpose_a(p_in, L, w + L.off_At, st)) != cudaSuccess) return e;
     phase_mark(15, true, st);
   }
-  if (p.k > 0 && ps) {
+  if (onepass) {
+    phase_mark(16, false, st);
+    if ((e = cudaMemsetAsync(ssq, 0, sizeof(double) * (size_t(L.rowsA) + L.rowsB), st)) !=
+            cudaSuccess ||
+        (e = cudaMemsetAsync(oplist + 2 * (L.rowsA + L.rowsB), 0, 2 * sizeof(int), st)) !=
+            cudaSuccess)
+      return e;
+    // B's exponents on the side stream when there is one: rows that take the
+    // exact norm (normalised rows, say) are read beside A's slicing
+    int* exactA = oplist + L.rowsA + L.rowsB;
+    auto estimate = [&](int which, cudaStream_t s) {
+      if (dbl)
+        onepass_estimate<double>(L, crt, p, cplx, sigA, sigB, exactA, exactA + L.rowsA, which, s);
+      else
+        onepass_estimate<float>(L, crt, p, cplx, sigA, sigB, exactA, exactA + L.rowsA, which, s);
+    };
+    estimate(ps ? 1 : 3, st);
+    phase_mark(16, true, st);
+    if (ps) {
+      if ((e = cudaEventRecord(ps->ev_start, st)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(ps->lo, ps->ev_start, 0)) != cudaSuccess) return e;
+      estimate(2, ps->lo);
+      if ((e = cudaEventRecord(ps->ev_scaled, ps->lo)) != cudaSuccess) return e;
+    }
+  } else if (p.k > 0 && ps) {
     // A's norms alone (both are pure reads and would share the bandwidth),
     // then B's norms on the side stream while A is sliced
     phase_mark(16, false, st);
@@ -2729,13 +3076,16 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
     phase_mark(1, false, st);
     phase_mark(1, true, st);
   } else {
+    // with one-pass scaling the slicer also sums the rows' scaled squares
+    double* ssqA = onepass ? ssq : nullptr;
+    double* ssqB = onepass ? ssq + L.rowsA : nullptr;
     auto slice = [&](int t0, int t1, int which, cudaStream_t s) {
       if (dbl)
         slice_operands<double>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, which, s,
-                               status);
+                               status, ssqA, ssqB);
       else
         slice_operands<float>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, which, s,
-                              status);
+                              status, ssqA, ssqB);
     };
     CUtensorMap mapA, mapB;
     if (!make_map(&mapA, resA, L.kp, int64_t(L.nmod) * L.nsub * L.rowsA, BM) ||
@@ -2882,6 +3232,14 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
       phase_mark(18, false, st);
       slice(0, L.nmod, 2, st);
       phase_mark(18, true, st);
+      if (onepass) {
+        phase_mark(19, false, st);
+        if (dbl)
+          onepass_fixup<double>(L, crt, p, cplx, sigA, sigB, resA, resB, ssq, oplist, st);
+        else
+          onepass_fixup<float>(L, crt, p, cplx, sigA, sigB, resA, resB, ssq, oplist, st);
+        phase_mark(19, true, st);
+      }
       phase_mark(0, true, st);
       phase_mark(1, false, st);
       phase_mark(3, false, st);

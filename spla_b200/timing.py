@@ -3,12 +3,15 @@
 
     python -m spla_b200.timing complex128:2:1024:1024:250000 [more specs]
     python -m spla_b200.timing --sweep     # every path and AUTO on a grid
+    python -m spla_b200.timing --normalised complex128:2:1024:1024:250000
 
 A spec is dtype:path:m:n:k[:opA] with dtype in {float32, float64, complex64,
 complex128} and path 0 auto, 1 DMMA, 2 Ozaki, 3 3xTF32; the problem is
 C = op(A) B with op = conjugate transpose (complex) or transpose (real)
 unless opA is given (0 = N: A is m x k, the pgemm_sbs shape), Gaussian
-operands scaled by 1/sqrt(k). One JSON line per spec: total time,
+operands scaled by 1/sqrt(k), or with --normalised every row of op(A) and
+column of B scaled to norm 1 (norms on a power of two: the rows whose
+exponents the Ozaki path's one-pass scaling cannot estimate). One JSON line per spec: total time,
 TFLOP/s and the phase times the path reports (scale/slice, GEMM span,
 reduction or reconstruction, then one entry per GEMM launch) and, for the
 Ozaki path, the parts of the slicing phase.
@@ -19,11 +22,11 @@ import ctypes as ct
 import json
 import sys
 
-NPHASE = 3 + 16
+NPHASE = 3 + 17
 
 
 def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: int = 2,
-        moduli: int = 0, opA: int | None = None) -> dict:
+        moduli: int = 0, opA: int | None = None, normalised: bool = False) -> dict:
     import torch
     import spla_b200 as spla
     L = spla.lib()
@@ -34,6 +37,10 @@ def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: i
     B = torch.randn(n * k, dtype=tdt, device="cuda", generator=g) * (0.5 / k) ** 0.5
     C = torch.zeros(m * n, dtype=tdt, device="cuda")
     op = (2 if A.is_complex() else 1) if opA is None else opA
+    if normalised:  # every row of op(A) and column of B of norm 1
+        Av = A.view(k, m).T if op == 0 else A.view(m, k)
+        Av.div_(torch.linalg.vector_norm(Av, dim=1, keepdim=True))
+        B.view(n, k).div_(torch.linalg.vector_norm(B.view(n, k), dim=1, keepdim=True))
     lda = m if op == 0 else k
     ws_bytes = spla.splab_gemm_workspace_size(dtype, path, op, 0, m, n, k, moduli)
     ws = torch.empty(max(1, ws_bytes), dtype=torch.uint8, device="cuda")
@@ -82,8 +89,9 @@ def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: i
             "phases_ms": [round(x, 3) for x in ph[:3]],
             "gemm_launch_ms": [round(x, 3) for x in ph[3:15] if x > 0.05],
             "slicing_ms": {"a_copy": round(ph[15], 3), "norms": round(ph[16], 3),
-                           "residues_a": round(ph[17], 3), "residues_b": round(ph[18], 3)},
-            "workspace_GB": round(ws_bytes / 1e9, 2)}
+                           "residues_a": round(ph[17], 3), "residues_b": round(ph[18], 3),
+                           "onepass_redo": round(ph[19], 3)},
+            "workspace_GB": round(ws_bytes / 1e9, 2), "normalised": normalised}
 
 
 def sweep():
@@ -106,10 +114,11 @@ def main(argv):
     if argv == ["--sweep"]:
         sweep()
         return
-    for spec in argv:
+    normalised = "--normalised" in argv
+    for spec in (a for a in argv if a != "--normalised"):
         d, p, m, n, k, *op = spec.split(":")
         print(json.dumps(run(d, int(p), int(m), int(n), int(k),
-                             opA=int(op[0]) if op else None)), flush=True)
+                             opA=int(op[0]) if op else None, normalised=normalised)), flush=True)
 
 
 if __name__ == "__main__":

@@ -561,3 +561,128 @@ def test_in_place_non_finite_and_extreme_rows():
     gb = got[rows][:, [c for c in range(n) if c != 6]]
     rb = ref[rows][:, [c for c in range(n) if c != 6]]
     assert rel(gb[block_ok], rb[block_ok]) <= 1e-14
+
+
+@pytest.mark.parametrize("dt,opA,m,n,k", [
+    ("complex128", 2, 136, 72, 70000),   # 2k = 140000 reals per row
+    ("complex128", 1, 130, 66, 66000),   # A^T B
+    ("float64", 1, 120, 70, 140000),
+    ("complex64", 2, 140, 64, 70000),
+    ("float32", 1, 100, 60, 150000),
+])
+def test_one_pass_row_scaling_matches_two_pass(dt, opA, m, n, k):
+    """Long k-major rows take their scale exponents from a sample of each row
+    (16 evenly spread runs), checked after slicing by the sum of squares of
+    the scaled values; rows the sample misjudges get the exact norm and are
+    sliced again; rows whose estimate lies next to a power of two take the
+    exact norm at once. Rows built to defeat the sample (all their weight
+    outside it, a NaN or an infinity outside it, zero rows, norms exactly a
+    power of two, rows normalised to 1, 1e300 and 1e-300, a steep profile
+    along k) end with the two-pass
+    exponents and residues: C is bit-identical to SPLAB_OZAKI_ONEPASS=0 (bytes
+    compared, NaN included), the one-pass sequence is seen to run (its
+    fix-up phase event is recorded), and the finite part of C matches the
+    device double-double product."""
+    import ctypes as ct
+    import torch
+    cplx = dt.startswith("complex")
+    rt = torch.float64 if dt in ("complex128", "float64") else torch.float32
+    r = 2 if cplx else 1
+    K2 = r * k
+    g = torch.Generator(device="cuda")
+    g.manual_seed(13)
+    s = (1.0 / K2) ** 0.5
+    A = torch.randn(r * k * m, dtype=rt, device="cuda", generator=g) * s
+    B = torch.randn(r * k * n, dtype=rt, device="cuda", generator=g) * s
+    Ar, Br = A.view(m, K2), B.view(n, K2)  # row i of op(A) / column j of op(B): K2 reals
+    # the sample: 16 runs of about K2 / 256 reals starting K2 // 16 apart, so
+    # real K2 // 32 lies outside every run
+    out = K2 // 16 // 2
+    big = 1e30 if rt == torch.float64 else 1e15
+    Ar[0].zero_(); Ar[0, out] = 3.0                      # all weight outside the sample
+    Ar[1, out + 1] = 1e6                                 # one large element outside it
+    Ar[2, out] = float("nan")
+    Ar[3, out + 2] = float("inf")
+    Ar[4].zero_()                                         # zero row
+    Ar[5].zero_(); Ar[5, 0] = 2.0 ** 40                  # norm exactly a power of two
+    Ar[6].zero_(); Ar[6, 0] = 0.6; Ar[6, 1] = 0.8         # norm 1 up to rounding
+    Ar[7] *= 1e300 if rt == torch.float64 else 1e30
+    Ar[8] *= 1e-300 if rt == torch.float64 else 1e-30
+    Ar[9] *= torch.exp(-20.0 * torch.arange(K2, device="cuda", dtype=rt) / K2)  # steep decay
+    Ar[10, : K2 // 2] *= 1e-8                            # small prefix, large rest
+    Ar[11, K2 // 2:] *= big                              # large end
+    # rows normalised to 1 and to 2^-3: estimates next to a power of two
+    # take the exact norm at once
+    Ar[12:40] /= torch.linalg.vector_norm(Ar[12:40], dim=1, keepdim=True)
+    Ar[30:40] *= 0.125
+    Br[0].zero_(); Br[0, out] = -1.0
+    Br[1, out + 3] = float("nan")
+    Br[2].zero_()
+    Br[3] *= 1e-300 if rt == torch.float64 else 1e-30
+    Br[4, K2 - 1] = 1e8
+    C0 = torch.rand(r * m * n, dtype=rt, device="cuda", generator=g) * 2 - 1
+    alpha, beta = ((0.5 - 0.25j), (1.0 + 0.5j)) if cplx else (0.5, -1.0)
+    ws_bytes = spla.splab_gemm_workspace_size(dt, spla.PATH_OZAKI, opA, 0, m, n, k)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    L = spla.lib()
+    nphase = 20
+    st = torch.cuda.Stream()
+    outs, redo = [], []
+    for onepass in ("1", "0"):
+        os.environ["SPLAB_OZAKI_ONEPASS"] = onepass
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nphase)]
+        for e in ev:
+            e.record(st)
+        st.synchronize()
+        handles = (ct.c_void_p * (2 * nphase))(*[e.cuda_event for e in ev])
+        C = C0.clone()
+        torch.cuda.synchronize()
+        L.splab_set_phase_events(handles, nphase)
+        try:
+            rc = spla.splab_gemm(dt, spla.PATH_OZAKI, opA, 0, m, n, k, alpha, A, k, B, k, beta, C,
+                                 m, workspace=ws, workspace_bytes=ws_bytes, stream=st.cuda_stream)
+        finally:
+            L.splab_set_phase_events(None, 0)
+            os.environ.pop("SPLAB_OZAKI_ONEPASS", None)
+        assert rc == 0
+        st.synchronize()
+        outs.append(C.cpu().numpy())
+        # phase 19 (the one-pass fix-up) ends after phase 18 (B's residues)
+        # only when it ran; else its end event keeps the earlier record
+        redo.append(ev[37].elapsed_time(ev[39]) if onepass == "1"
+                    else ev[39].elapsed_time(ev[37]))
+    assert redo[0] > 0.0 and redo[1] > 0.0, redo
+    assert np.array_equal(outs[0].view(np.uint8), outs[1].view(np.uint8))
+    # the finite part against the device double-double product
+    Rdt = torch.complex128 if cplx else torch.float64
+    R = torch.zeros(m * n, dtype=Rdt, device="cuda")
+    Ad, Bd = A.double(), B.double()
+    if cplx:
+        Ad, Bd = torch.view_as_complex(Ad.view(-1, 2)), torch.view_as_complex(Bd.view(-1, 2))
+    assert spla.gemm_dd("complex128" if cplx else "float64", opA, 0, m, n, k, Ad, k, Bd, k, R,
+                        m) == 0
+    torch.cuda.synchronize()
+    c0 = C0.double().cpu().numpy()
+    got = outs[0].astype(np.float64)
+    if cplx:
+        got = got.view(np.complex128)
+        c0 = c0.view(np.complex128)
+    ref = (alpha * R.cpu().numpy() + beta * c0).reshape(n, m).T
+    got = got.reshape(n, m).T
+    bad = np.zeros((m, n), bool)
+    bad[[2, 3], :] = True
+    bad[:, 1] = True
+    assert np.isnan(got[bad]).all()
+    # normwise: |C - ref| <= tol (|alpha| |a_i| |b_j| + |beta c0|), with the
+    # norms taken without overflow (rows near 1e300)
+    def norms(X, rows):
+        x = X.double().view(rows, K2).cpu().numpy()
+        mx = np.abs(x).max(axis=1)
+        mx[~(mx > 0)] = 1.0
+        return mx * np.linalg.norm(x / mx[:, None], axis=1)
+    na, nb = norms(A, m), norms(B, n)
+    tol = 1e-14 if rt == torch.float64 else 1e-6
+    bound = tol * (abs(alpha) * na[:, None] * nb[None, :] +
+                   abs(beta) * np.abs(c0.reshape(n, m).T))
+    ok = ~bad
+    assert (np.abs(got - ref)[ok] <= bound[ok]).all()
