@@ -675,11 +675,12 @@ def test_one_pass_row_scaling_matches_two_pass(dt, opA, m, n, k):
     assert np.isnan(got[bad]).all()
     # normwise: |C - ref| <= tol (|alpha| |a_i| |b_j| + |beta c0|), with the
     # norms taken without overflow (rows near 1e300)
-    def norms(X, rows):
+    def norms(X, rows):  # NaN for the rows holding a NaN or an infinity
         x = X.double().view(rows, K2).cpu().numpy()
         mx = np.abs(x).max(axis=1)
-        mx[~(mx > 0)] = 1.0
-        return mx * np.linalg.norm(x / mx[:, None], axis=1)
+        mx[~((mx > 0) & np.isfinite(mx))] = 1.0
+        with np.errstate(invalid="ignore"):
+            return mx * np.linalg.norm(x / mx[:, None], axis=1)
     na, nb = norms(A, m), norms(B, n)
     tol = 1e-14 if rt == torch.float64 else 1e-6
     bound = tol * (abs(alpha) * na[:, None] * nb[None, :] +
