@@ -2255,7 +2255,7 @@ struct Layout {
   int64_t ldAt;            // leading dimension of At (elements of A's type)
   size_t off_sigA, off_sigB, off_resA, off_resB, off_R, off_At, off_status, off_tiles;
   size_t off_partA, off_partB;  // k-slice partial sums of the in-place row norms
-  size_t off_ssq, off_list;     // one-pass row scaling (onepass_applies): scaled sums
+  size_t off_ssq, off_list;     // one-pass row scaling (onepass_operands): scaled sums
                                 // of squares, rows sent back and their two counts
   size_t total;
 };
@@ -2690,19 +2690,24 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
 // which is what the exact exponent gives. Other rows (a sample that
 // misjudged the row by more than the band) get the exact norm and are
 // sliced again. Each row thus ends with the exponent and residues of the
-// two-pass order, whatever the order of the atomic sums. Used for k-major A
-// and B, the default modulus count and unrolled slicer, one modulus group
-// and rows of at least kOnePassMinLen reals; SPLAB_OZAKI_ONEPASS=0 (read per
-// call) keeps the two-pass order.
+// two-pass order, whatever the order of the atomic sums. Used for each
+// k-major operand (an operand read in place keeps its norms) with the
+// default modulus count and unrolled slicer, one modulus group and rows of
+// at least kOnePassMinLen reals; SPLAB_OZAKI_ONEPASS=0 (read per call) keeps
+// the two-pass order.
 constexpr int64_t kOnePassMinLen = 131072;
 constexpr int kOnePassRuns = 16;
 
-bool onepass_applies(const oz::Layout& L, const GemmProblem& p, int groups) {
+// The operands scaled in one pass: bit 1 A, bit 2 B (k-major ones only; the
+// rows read in place keep their k-sliced norms)
+int onepass_operands(const oz::Layout& L, const GemmProblem& p, int groups) {
   const char* v = std::getenv("SPLAB_OZAKI_ONEPASS");
-  if (v && v[0] == '0') return false;
+  if (v && v[0] == '0') return 0;
   const int nu = dtype_is_double(p.dtype) ? oz::kDefaultModuli : oz::kDefaultModuliFloat;
-  return p.k > 0 && !L.mn && !L.mnB && groups == 1 && L.nmod == nu && slice_unroll() &&
-         !slice_tc_enabled() && L.K2 >= kOnePassMinLen;
+  if (!(p.k > 0 && groups == 1 && L.nmod == nu && slice_unroll() && !slice_tc_enabled() &&
+        L.K2 >= kOnePassMinLen))
+    return 0;
+  return (L.mn ? 0 : 1) | (L.mnB ? 0 : 2);
 }
 
 // Exponents of A's (which & 1) and B's (which & 2) rows, estimated from the
@@ -2765,12 +2770,12 @@ void onepass_redo(const oz::Layout& L, const oz::Crt& crt, const oz::SliceConsts
   }
 }
 
-// Check of A's and B's rows after slicing with their sums of squares, and
-// the second pass over the rows it lists
+// Check of A's (which & 1) and B's (which & 2) rows after slicing with their
+// sums of squares, and the second pass over the rows it lists
 template <typename TIn>
 void onepass_fixup(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p, bool cplx,
                    int* sigA, int* sigB, int8_t* resA, int8_t* resB, double* ssq, int* list,
-                   cudaStream_t st) {
+                   int which, cudaStream_t st) {
   using namespace oz;
   const double lo = std::ldexp(1.0 + std::ldexp(1.0, -30), 2 * crt.q_bits - 2);
   const double hi = std::ldexp(1.0 - std::ldexp(1.0, -30), 2 * crt.q_bits);
@@ -2779,19 +2784,23 @@ void onepass_fixup(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p
   const int* exactA = list + L.rowsA + L.rowsB;
   const int* exactB = exactA + L.rowsA;
   int* cnt = list + 2 * (L.rowsA + L.rowsB);  // A's count, B's count
-  oz_onepass_check<<<unsigned((L.rowsA + 255) / 256), 256, 0, st>>>(ssq, exactA, L.rowsA, lo, hi,
-                                                                   listA, cnt);
-  oz_onepass_check<<<unsigned((L.rowsB + 255) / 256), 256, 0, st>>>(
-      ssq + L.rowsA, exactB, L.rowsB, lo, hi, listB, cnt + 1);
+  if (which & 1)
+    oz_onepass_check<<<unsigned((L.rowsA + 255) / 256), 256, 0, st>>>(ssq, exactA, L.rowsA, lo,
+                                                                     hi, listA, cnt);
+  if (which & 2)
+    oz_onepass_check<<<unsigned((L.rowsB + 255) / 256), 256, 0, st>>>(
+        ssq + L.rowsA, exactB, L.rowsB, lo, hi, listB, cnt + 1);
   int ndig = 0;
   const SliceConsts sc = slice_consts(L, crt, &ndig);
   const int mode = cplx ? 2 : 0;
   const int64_t ldA = cplx ? 2 * p.lda : p.lda, ldB = cplx ? 2 * p.ldb : p.ldb;
-  onepass_redo<TIn>(L, crt, sc, static_cast<const TIn*>(p.A), ldA, L.rowsA, sigA,
-                    p.opA == 2 ? -1 : 1, resA, int64_t(L.nsub) * L.rowsA * L.kp, mode, listA,
-                    cnt, st);
-  onepass_redo<TIn>(L, crt, sc, static_cast<const TIn*>(p.B), ldB, L.rowsB, sigB, 1, resB,
-                    int64_t(L.nsub) * L.nb * L.kp, mode, listB, cnt + 1, st);
+  if (which & 1)
+    onepass_redo<TIn>(L, crt, sc, static_cast<const TIn*>(p.A), ldA, L.rowsA, sigA,
+                      p.opA == 2 ? -1 : 1, resA, int64_t(L.nsub) * L.rowsA * L.kp, mode, listA,
+                      cnt, st);
+  if (which & 2)
+    onepass_redo<TIn>(L, crt, sc, static_cast<const TIn*>(p.B), ldB, L.rowsB, sigB, 1, resB,
+                      int64_t(L.nsub) * L.nb * L.kp, mode, listB, cnt + 1, st);
 }
 
 // Side streams may be used by this host thread (off while a batch captures
@@ -3002,7 +3011,7 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
     const char* v = std::getenv("SPLAB_OZAKI_SIDE_NORMS");
     return !(v && v[0] == '0');
   }();
-  const bool onepass = onepass_applies(L, p, groups);
+  const int onepass = onepass_operands(L, p, groups);
   double* ssq = reinterpret_cast<double*>(w + L.off_ssq);
   int* oplist = reinterpret_cast<int*>(w + L.off_list);
   PipeStreams* ps =
@@ -3023,43 +3032,43 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
     if ((e = transpose_a(p_in, L, w + L.off_At, st)) != cudaSuccess) return e;
     phase_mark(15, true, st);
   }
-  if (onepass) {
-    phase_mark(16, false, st);
-    if ((e = cudaMemsetAsync(ssq, 0, sizeof(double) * (size_t(L.rowsA) + L.rowsB), st)) !=
-            cudaSuccess ||
-        (e = cudaMemsetAsync(oplist + 2 * (L.rowsA + L.rowsB), 0, 2 * sizeof(int), st)) !=
-            cudaSuccess)
-      return e;
-    // B's exponents on the side stream when there is one: rows that take the
-    // exact norm (normalised rows, say) are read beside A's slicing
-    int* exactA = oplist + L.rowsA + L.rowsB;
-    auto estimate = [&](int which, cudaStream_t s) {
+  // row exponents of A (which & 1) and B (which & 2): estimated for the
+  // operands scaled in one pass, else the exact norms
+  int* exactA = oplist + L.rowsA + L.rowsB;
+  auto exponents = [&](int which, cudaStream_t s) {
+    if (which & onepass) {
       if (dbl)
-        onepass_estimate<double>(L, crt, p, cplx, sigA, sigB, exactA, exactA + L.rowsA, which, s);
+        onepass_estimate<double>(L, crt, p, cplx, sigA, sigB, exactA, exactA + L.rowsA,
+                                 which & onepass, s);
       else
-        onepass_estimate<float>(L, crt, p, cplx, sigA, sigB, exactA, exactA + L.rowsA, which, s);
-    };
-    estimate(ps ? 1 : 3, st);
-    phase_mark(16, true, st);
-    if (ps) {
-      if ((e = cudaEventRecord(ps->ev_start, st)) != cudaSuccess) return e;
-      if ((e = cudaStreamWaitEvent(ps->lo, ps->ev_start, 0)) != cudaSuccess) return e;
-      estimate(2, ps->lo);
-      if ((e = cudaEventRecord(ps->ev_scaled, ps->lo)) != cudaSuccess) return e;
+        onepass_estimate<float>(L, crt, p, cplx, sigA, sigB, exactA, exactA + L.rowsA,
+                                which & onepass, s);
     }
-  } else if (p.k > 0 && ps) {
-    // A's norms alone (both are pure reads and would share the bandwidth),
-    // then B's norms on the side stream while A is sliced
+    if (which & ~onepass) scale(which & ~onepass, s);
+  };
+  if (onepass && ((e = cudaMemsetAsync(ssq, 0, sizeof(double) * (size_t(L.rowsA) + L.rowsB),
+                                       st)) != cudaSuccess ||
+                  (e = cudaMemsetAsync(oplist + 2 * (L.rowsA + L.rowsB), 0, 2 * sizeof(int),
+                                       st)) != cudaSuccess))
+    return e;
+  const bool side_exponents = p.k > 0 && ps && onepass != 1;
+  if (side_exponents) {
+    // A's exponents alone (norms are pure reads and would share the
+    // bandwidth), then B's on the side stream while A is sliced
     phase_mark(16, false, st);
-    scale(1, st);
+    exponents(1, st);
     phase_mark(16, true, st);
     if ((e = cudaEventRecord(ps->ev_start, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(ps->lo, ps->ev_start, 0)) != cudaSuccess) return e;
-    scale(2, ps->lo);
+    exponents(2, ps->lo);
     if ((e = cudaEventRecord(ps->ev_scaled, ps->lo)) != cudaSuccess) return e;
   } else if (p.k > 0) {
+    // B's exact norms first, alone, when only A is scaled in one pass: beside
+    // A's slicing with its sums of squares they measured slower (op(A) = C,
+    // op(B) = C at the headline size: 18.2 against 18.0 ms for two passes)
     phase_mark(16, false, st);
-    scale(3, st);
+    exponents(2, st);
+    exponents(1, st);
     phase_mark(16, true, st);
   } else {
     cudaMemsetAsync(sigA, 0, sizeof(int) * L.rowsA, st);
@@ -3077,8 +3086,8 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
     phase_mark(1, true, st);
   } else {
     // with one-pass scaling the slicer also sums the rows' scaled squares
-    double* ssqA = onepass ? ssq : nullptr;
-    double* ssqB = onepass ? ssq + L.rowsA : nullptr;
+    double* ssqA = (onepass & 1) ? ssq : nullptr;
+    double* ssqB = (onepass & 2) ? ssq + L.rowsA : nullptr;
     auto slice = [&](int t0, int t1, int which, cudaStream_t s) {
       if (dbl)
         slice_operands<double>(L, crt, p, cplx, sigA, sigB, resA, resB, t0, t1, which, s,
@@ -3228,16 +3237,19 @@ cudaError_t ozaki_gemm(const GemmProblem& p_in, int moduli, void* ws, size_t ws_
       slice(0, L.nmod, 1, st);  // A on the caller's stream
       phase_mark(17, true, st);
       // B once its row norms are done (on the side stream when there is one)
-      if (ps && (e = cudaStreamWaitEvent(st, ps->ev_scaled, 0)) != cudaSuccess) return e;
+      if (side_exponents && (e = cudaStreamWaitEvent(st, ps->ev_scaled, 0)) != cudaSuccess)
+        return e;
       phase_mark(18, false, st);
       slice(0, L.nmod, 2, st);
       phase_mark(18, true, st);
       if (onepass) {
         phase_mark(19, false, st);
         if (dbl)
-          onepass_fixup<double>(L, crt, p, cplx, sigA, sigB, resA, resB, ssq, oplist, st);
+          onepass_fixup<double>(L, crt, p, cplx, sigA, sigB, resA, resB, ssq, oplist, onepass,
+                                st);
         else
-          onepass_fixup<float>(L, crt, p, cplx, sigA, sigB, resA, resB, ssq, oplist, st);
+          onepass_fixup<float>(L, crt, p, cplx, sigA, sigB, resA, resB, ssq, oplist, onepass,
+                               st);
         phase_mark(19, true, st);
       }
       phase_mark(0, true, st);

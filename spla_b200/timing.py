@@ -5,10 +5,11 @@
     python -m spla_b200.timing --sweep     # every path and AUTO on a grid
     python -m spla_b200.timing --normalised complex128:2:1024:1024:250000
 
-A spec is dtype:path:m:n:k[:opA] with dtype in {float32, float64, complex64,
-complex128} and path 0 auto, 1 DMMA, 2 Ozaki, 3 3xTF32; the problem is
-C = op(A) B with op = conjugate transpose (complex) or transpose (real)
-unless opA is given (0 = N: A is m x k, the pgemm_sbs shape), Gaussian
+A spec is dtype:path:m:n:k[:opA[:opB]] with dtype in {float32, float64,
+complex64, complex128} and path 0 auto, 1 DMMA, 2 Ozaki, 3 3xTF32; the
+problem is C = op(A) op(B) with op(A) = conjugate transpose (complex) or
+transpose (real) unless opA is given (0 = N: A is m x k, the pgemm_sbs
+shape) and op(B) = N unless opB is given (1 = T, 2 = C: B is n x k), Gaussian
 operands scaled by 1/sqrt(k), or with --normalised every row of op(A) and
 column of B scaled to norm 1 (norms on a power of two: the rows whose
 exponents the Ozaki path's one-pass scaling cannot estimate). One JSON line per spec: total time,
@@ -26,7 +27,8 @@ NPHASE = 3 + 17
 
 
 def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: int = 2,
-        moduli: int = 0, opA: int | None = None, normalised: bool = False) -> dict:
+        moduli: int = 0, opA: int | None = None, normalised: bool = False,
+        opB: int = 0) -> dict:
     import torch
     import spla_b200 as spla
     L = spla.lib()
@@ -37,12 +39,14 @@ def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: i
     B = torch.randn(n * k, dtype=tdt, device="cuda", generator=g) * (0.5 / k) ** 0.5
     C = torch.zeros(m * n, dtype=tdt, device="cuda")
     op = (2 if A.is_complex() else 1) if opA is None else opA
-    if normalised:  # every row of op(A) and column of B of norm 1
+    if normalised:  # every row of op(A) and column of op(B) of norm 1
         Av = A.view(k, m).T if op == 0 else A.view(m, k)
         Av.div_(torch.linalg.vector_norm(Av, dim=1, keepdim=True))
-        B.view(n, k).div_(torch.linalg.vector_norm(B.view(n, k), dim=1, keepdim=True))
+        Bv = B.view(n, k) if opB == 0 else B.view(k, n).T
+        Bv.div_(torch.linalg.vector_norm(Bv, dim=1, keepdim=True))
     lda = m if op == 0 else k
-    ws_bytes = spla.splab_gemm_workspace_size(dtype, path, op, 0, m, n, k, moduli)
+    ldb = k if opB == 0 else n
+    ws_bytes = spla.splab_gemm_workspace_size(dtype, path, op, opB, m, n, k, moduli)
     ws = torch.empty(max(1, ws_bytes), dtype=torch.uint8, device="cuda")
     st = torch.cuda.Stream()
     pev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * NPHASE)]
@@ -52,7 +56,7 @@ def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: i
     handles = (ct.c_void_p * (2 * NPHASE))(*[e.cuda_event for e in pev])
 
     def step():
-        rc = spla.splab_gemm(dtype, path, op, 0, m, n, k, 1.0, A, lda, B, k, 0.0, C, m,
+        rc = spla.splab_gemm(dtype, path, op, opB, m, n, k, 1.0, A, lda, B, ldb, 0.0, C, m,
                              moduli=moduli, workspace=ws, workspace_bytes=ws_bytes,
                              stream=st.cuda_stream)
         if rc != 0:
@@ -84,8 +88,8 @@ def run(dtype: str, path: int, m: int, n: int, k: int, steps: int = 5, warmup: i
     ph = [x / steps for x in tot]
     flops = (8.0 if A.is_complex() else 2.0) * m * n * k
     return {"dtype": dtype, "path": path,
-            "resolved_path": L.splab_gemm_path(spla._dtype_of(dtype=dtype), path, op, 0, m, n, k),
-            "opA": op, "m": m, "n": n, "k": k, "ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 1),
+            "resolved_path": L.splab_gemm_path(spla._dtype_of(dtype=dtype), path, op, opB, m, n, k),
+            "opA": op, "opB": opB, "m": m, "n": n, "k": k, "ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 1),
             "phases_ms": [round(x, 3) for x in ph[:3]],
             "gemm_launch_ms": [round(x, 3) for x in ph[3:15] if x > 0.05],
             "slicing_ms": {"a_copy": round(ph[15], 3), "norms": round(ph[16], 3),
@@ -118,7 +122,8 @@ def main(argv):
     for spec in (a for a in argv if a != "--normalised"):
         d, p, m, n, k, *op = spec.split(":")
         print(json.dumps(run(d, int(p), int(m), int(n), int(k),
-                             opA=int(op[0]) if op else None, normalised=normalised)), flush=True)
+                             opA=int(op[0]) if op else None, normalised=normalised,
+                             opB=int(op[1]) if len(op) > 1 else 0)), flush=True)
 
 
 if __name__ == "__main__":

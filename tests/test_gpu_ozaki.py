@@ -687,3 +687,93 @@ def test_one_pass_row_scaling_matches_two_pass(dt, opA, m, n, k):
                    abs(beta) * np.abs(c0.reshape(n, m).T))
     ok = ~bad
     assert (np.abs(got - ref)[ok] <= bound[ok]).all()
+
+
+@pytest.mark.parametrize("dt,opA,opB,m,n,k", [
+    ("complex128", 0, 0, 150, 90, 70000),   # A read in place, B in one pass
+    ("complex128", 2, 2, 120, 100, 66000),  # A in one pass, B read in place (conjugated)
+    ("float64", 1, 1, 110, 96, 140000),
+    ("complex64", 0, 0, 96, 130, 70000),
+])
+def test_one_pass_beside_an_operand_read_in_place(dt, opA, opB, m, n, k):
+    """With one operand read in place (its norms k-sliced along m- or n-major
+    rows) the other, k-major, is still scaled in one pass: C is bit-identical
+    to SPLAB_OZAKI_ONEPASS=0, the fix-up phase runs, and C matches the device
+    double-double product."""
+    import ctypes as ct
+    import torch
+    cplx = dt.startswith("complex")
+    rt = torch.float64 if dt in ("complex128", "float64") else torch.float32
+    r = 2 if cplx else 1
+    K2 = r * k
+    g = torch.Generator(device="cuda")
+    g.manual_seed(17)
+    s = (1.0 / K2) ** 0.5
+    A = torch.randn(r * k * m, dtype=rt, device="cuda", generator=g) * s
+    B = torch.randn(r * k * n, dtype=rt, device="cuda", generator=g) * s
+    lda, ldb = (m if opA == 0 else k), (k if opB == 0 else n)
+    out = K2 // 32  # outside every sampled run
+    if opA != 0:  # A k-major: rows of op(A) contiguous
+        Ar = A.view(m, K2)
+        Ar[0].zero_(); Ar[0, out] = 2.0
+        Ar[1, out] = float("nan")
+        Ar[2:20] /= torch.linalg.vector_norm(Ar[2:20], dim=1, keepdim=True)
+    if opB == 0:  # B k-major
+        Br = B.view(n, K2)
+        Br[0].zero_(); Br[0, out] = -3.0
+        Br[1, out + 1] = float("inf")
+        Br[2:20] /= torch.linalg.vector_norm(Br[2:20], dim=1, keepdim=True)
+    C0 = torch.rand(r * m * n, dtype=rt, device="cuda", generator=g) * 2 - 1
+    alpha, beta = ((0.5 - 0.25j), (1.0 + 0.5j)) if cplx else (0.5, -1.0)
+    ws_bytes = spla.splab_gemm_workspace_size(dt, spla.PATH_OZAKI, opA, opB, m, n, k)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    L = spla.lib()
+    nphase = 20
+    st = torch.cuda.Stream()
+    outs, ran = [], []
+    for onepass in ("1", "0"):
+        os.environ["SPLAB_OZAKI_ONEPASS"] = onepass
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nphase)]
+        for e in ev:
+            e.record(st)
+        st.synchronize()
+        handles = (ct.c_void_p * (2 * nphase))(*[e.cuda_event for e in ev])
+        C = C0.clone()
+        torch.cuda.synchronize()
+        L.splab_set_phase_events(handles, nphase)
+        try:
+            rc = spla.splab_gemm(dt, spla.PATH_OZAKI, opA, opB, m, n, k, alpha, A, lda, B, ldb,
+                                 beta, C, m, workspace=ws, workspace_bytes=ws_bytes,
+                                 stream=st.cuda_stream)
+        finally:
+            L.splab_set_phase_events(None, 0)
+            os.environ.pop("SPLAB_OZAKI_ONEPASS", None)
+        assert rc == 0
+        st.synchronize()
+        outs.append(C.cpu().numpy())
+        ran.append(ev[37].elapsed_time(ev[39]) if onepass == "1" else ev[39].elapsed_time(ev[37]))
+    assert ran[0] > 0.0 and ran[1] > 0.0, ran
+    assert np.array_equal(outs[0].view(np.uint8), outs[1].view(np.uint8))
+    Rdt = torch.complex128 if cplx else torch.float64
+    R = torch.zeros(m * n, dtype=Rdt, device="cuda")
+    Ad, Bd = A.double(), B.double()
+    if cplx:
+        Ad, Bd = torch.view_as_complex(Ad.view(-1, 2)), torch.view_as_complex(Bd.view(-1, 2))
+    assert spla.gemm_dd("complex128" if cplx else "float64", opA, opB, m, n, k, Ad, lda, Bd, ldb,
+                        R, m) == 0
+    torch.cuda.synchronize()
+    c0 = C0.double().cpu().numpy()
+    got = outs[0].astype(np.float64)
+    if cplx:
+        got, c0 = got.view(np.complex128), c0.view(np.complex128)
+    ref = alpha * R.cpu().numpy() + beta * c0
+    bad = np.zeros((n, m), bool)  # column-major C: [column][row]
+    if opA != 0:
+        bad[:, 1] = True
+    if opB == 0:
+        bad[1, :] = True
+    got, ref, bad = got.reshape(n, m), ref.reshape(n, m), bad
+    assert np.isnan(got[bad]).all()
+    tol = 1e-14 if rt == torch.float64 else 1e-6
+    ok = ~bad
+    assert oracle.rel_fro(got[ok], ref[ok]) <= tol
