@@ -563,14 +563,15 @@ def test_in_place_non_finite_and_extreme_rows():
     assert rel(gb[block_ok], rb[block_ok]) <= 1e-14
 
 
-@pytest.mark.parametrize("dt,opA,m,n,k", [
-    ("complex128", 2, 136, 72, 70000),   # 2k = 140000 reals per row
-    ("complex128", 1, 130, 66, 66000),   # A^T B
-    ("float64", 1, 120, 70, 140000),
-    ("complex64", 2, 140, 64, 70000),
-    ("float32", 1, 100, 60, 150000),
+@pytest.mark.parametrize("dt,opA,m,n,k,pad,offset", [
+    ("complex128", 2, 136, 72, 70000, 0, False),   # 2k = 140000 reals per row
+    ("complex128", 1, 130, 66, 66000, 3, True),    # A^T B; padded, 8 bytes off 16
+    ("float64", 1, 120, 70, 140000, 0, False),
+    ("float64", 1, 97, 33, 131072, 5, True),       # the shortest rows that take it
+    ("complex64", 2, 140, 64, 70000, 0, False),
+    ("float32", 1, 100, 60, 150000, 2, False),
 ])
-def test_one_pass_row_scaling_matches_two_pass(dt, opA, m, n, k):
+def test_one_pass_row_scaling_matches_two_pass(dt, opA, m, n, k, pad, offset):
     """Long k-major rows take their scale exponents from a sample of each row
     (16 evenly spread runs), checked after slicing by the sum of squares of
     the scaled values; rows the sample misjudges get the exact norm and are
@@ -582,7 +583,8 @@ def test_one_pass_row_scaling_matches_two_pass(dt, opA, m, n, k):
     exponents and residues: C is bit-identical to SPLAB_OZAKI_ONEPASS=0 (bytes
     compared, NaN included), the one-pass sequence is seen to run (its
     fix-up phase event is recorded), and the finite part of C matches the
-    device double-double product."""
+    device double-double product; with padded leading dimensions and base
+    addresses only 8 bytes aligned (scalar loads) as well."""
     import ctypes as ct
     import torch
     cplx = dt.startswith("complex")
@@ -592,9 +594,13 @@ def test_one_pass_row_scaling_matches_two_pass(dt, opA, m, n, k):
     g = torch.Generator(device="cuda")
     g.manual_seed(13)
     s = (1.0 / K2) ** 0.5
-    A = torch.randn(r * k * m, dtype=rt, device="cuda", generator=g) * s
-    B = torch.randn(r * k * n, dtype=rt, device="cuda", generator=g) * s
-    Ar, Br = A.view(m, K2), B.view(n, K2)  # row i of op(A) / column j of op(B): K2 reals
+    ld = k + pad
+    Abuf = torch.randn(r * ld * m + 1, dtype=rt, device="cuda", generator=g) * s
+    Bbuf = torch.randn(r * ld * n + 1, dtype=rt, device="cuda", generator=g) * s
+    A = Abuf[1:] if offset else Abuf[:-1]  # one real off: 8 (4) bytes off 16
+    B = Bbuf[1:] if offset else Bbuf[:-1]
+    # row i of op(A) / column j of op(B): K2 reals of a row of r * ld
+    Ar, Br = A.view(m, r * ld)[:, :K2], B.view(n, r * ld)[:, :K2]
     # the sample: 16 runs of about K2 / 256 reals starting K2 // 16 apart, so
     # real K2 // 32 lies outside every run
     out = K2 // 16 // 2
@@ -639,7 +645,7 @@ def test_one_pass_row_scaling_matches_two_pass(dt, opA, m, n, k):
         torch.cuda.synchronize()
         L.splab_set_phase_events(handles, nphase)
         try:
-            rc = spla.splab_gemm(dt, spla.PATH_OZAKI, opA, 0, m, n, k, alpha, A, k, B, k, beta, C,
+            rc = spla.splab_gemm(dt, spla.PATH_OZAKI, opA, 0, m, n, k, alpha, A, ld, B, ld, beta, C,
                                  m, workspace=ws, workspace_bytes=ws_bytes, stream=st.cuda_stream)
         finally:
             L.splab_set_phase_events(None, 0)
@@ -656,10 +662,10 @@ def test_one_pass_row_scaling_matches_two_pass(dt, opA, m, n, k):
     # the finite part against the device double-double product
     Rdt = torch.complex128 if cplx else torch.float64
     R = torch.zeros(m * n, dtype=Rdt, device="cuda")
-    Ad, Bd = A.double(), B.double()
+    Ad, Bd = A.double().clone(), B.double().clone()  # storage offset 0
     if cplx:
         Ad, Bd = torch.view_as_complex(Ad.view(-1, 2)), torch.view_as_complex(Bd.view(-1, 2))
-    assert spla.gemm_dd("complex128" if cplx else "float64", opA, 0, m, n, k, Ad, k, Bd, k, R,
+    assert spla.gemm_dd("complex128" if cplx else "float64", opA, 0, m, n, k, Ad, ld, Bd, ld, R,
                         m) == 0
     torch.cuda.synchronize()
     c0 = C0.double().cpu().numpy()
@@ -676,15 +682,16 @@ def test_one_pass_row_scaling_matches_two_pass(dt, opA, m, n, k):
     # normwise: |C - ref| <= tol (|alpha| |a_i| |b_j| + |beta c0|), with the
     # norms taken without overflow (rows near 1e300)
     def norms(X, rows):  # NaN for the rows holding a NaN or an infinity
-        x = X.double().view(rows, K2).cpu().numpy()
+        x = X.double().view(rows, r * ld)[:, :K2].cpu().numpy()
         mx = np.abs(x).max(axis=1)
         mx[~((mx > 0) & np.isfinite(mx))] = 1.0
         with np.errstate(invalid="ignore"):
             return mx * np.linalg.norm(x / mx[:, None], axis=1)
     na, nb = norms(A, m), norms(B, n)
     tol = 1e-14 if rt == torch.float64 else 1e-6
-    bound = tol * (abs(alpha) * na[:, None] * nb[None, :] +
-                   abs(beta) * np.abs(c0.reshape(n, m).T))
+    with np.errstate(invalid="ignore"):  # NaN bounds for the NaN rows
+        bound = tol * (abs(alpha) * na[:, None] * nb[None, :] +
+                       abs(beta) * np.abs(c0.reshape(n, m).T))
     ok = ~bad
     assert (np.abs(got - ref)[ok] <= bound[ok]).all()
 
