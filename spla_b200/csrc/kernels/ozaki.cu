@@ -328,12 +328,13 @@ __device__ __forceinline__ void digits13(double y, float (&d)[5]) {
     const double xl_d = fma(t - kM52, -1073741824.0, y);  // exact, |xl_d| <= 2^29
     const int xl = int(__double2loint(xl_d + kM52));
     const int xh = int(__double_as_longlong(t) - kM52Bits);  // |xh| <= 2^28 + 1
-    const int d0 = ((xl + 0x4000) & 0x7FFF) - 0x4000;
-    const int d2 = ((xh + 0x4000) & 0x7FFF) - 0x4000;
-    d[0] = small_int_to_float(d0);
-    d[1] = small_int_to_float((xl - d0) >> 15);
-    d[2] = small_int_to_float(d2);
-    d[3] = small_int_to_float((xh - d2) >> 15);
+    // balanced digits: with u = x + 2^14, d_lo = (u mod 2^15) - 2^14 and
+    // d_hi = (x - d_lo) / 2^15 = floor(u / 2^15)
+    const int u0 = xl + 0x4000, u2 = xh + 0x4000;
+    d[0] = small_int_to_float((u0 & 0x7FFF) - 0x4000);
+    d[1] = small_int_to_float(u0 >> 15);
+    d[2] = small_int_to_float((u2 & 0x7FFF) - 0x4000);
+    d[3] = small_int_to_float(u2 >> 15);
     d[4] = 0.0f;
     return;
   }
