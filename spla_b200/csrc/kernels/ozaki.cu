@@ -2687,7 +2687,8 @@ void slice_operands(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& 
 // norm at once. The default slicer also sums the squares of the scaled
 // values, and an estimated exponent stands when that sum lies in
 // [2^(2Q-2), 2^(2Q)) with a relative margin of 2^-30 at both ends (far above
-// the rounding of either sum): the scaled norm then lies in [2^(Q-1), 2^Q),
+// the rounding of either sum; see onepass_fixup): the scaled norm then lies in
+// [2^(Q-1), 2^Q),
 // which is what the exact exponent gives. Other rows (a sample that
 // misjudged the row by more than the band) get the exact norm and are
 // sliced again. Each row thus ends with the exponent and residues of the
@@ -2778,8 +2779,13 @@ void onepass_fixup(const oz::Layout& L, const oz::Crt& crt, const GemmProblem& p
                    int* sigA, int* sigB, int8_t* resA, int8_t* resB, double* ssq, int* list,
                    int which, cudaStream_t st) {
   using namespace oz;
-  const double lo = std::ldexp(1.0 + std::ldexp(1.0, -30), 2 * crt.q_bits - 2);
-  const double hi = std::ldexp(1.0 - std::ldexp(1.0, -30), 2 * crt.q_bits);
+  // the two sums of squares (norm kernel: runs of K2 / 256 terms per thread,
+  // then trees; slicer: 8 terms per thread, trees, K2 / 2048 atomics per
+  // row) differ by at most about (K2 / 256 + K2 / 2048 + 64) units of 2^-53
+  // relative; the margin is 2^-30, or K2 2^-59 for rows beyond 2^29 reals
+  const double delta = std::max(std::ldexp(1.0, -30), std::ldexp(double(L.K2), -59));
+  const double lo = std::ldexp(1.0 + delta, 2 * crt.q_bits - 2);
+  const double hi = std::ldexp(1.0 - delta, 2 * crt.q_bits);
   int* listA = list;
   int* listB = list + L.rowsA;
   const int* exactA = list + L.rowsA + L.rowsB;
