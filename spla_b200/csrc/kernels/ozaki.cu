@@ -2387,6 +2387,8 @@ size_t ozaki_workspace_bytes(const GemmProblem& p, int moduli) {
   return oz::layout_of(p, moduli).total;
 }
 
+bool ozaki_copies_a(const GemmProblem& p) { return p.opA == 0 && !oz::mn_fits(p); }
+
 bool ozaki_supported(const GemmProblem& p) {
   // op(B) = T or C: B is read in place, which needs the slicer's tiles to fit
   return (p.opB == 0 || ((p.opB == 1 || p.opB == 2) && oz::mn_fits(p))) &&

@@ -12,11 +12,16 @@ namespace splab {
 // moduli (0 = default).
 size_t ozaki_workspace_bytes(const GemmProblem& prob, int moduli);
 
-// C <- alpha * op(A) * op(B) + beta * C for double / complex double through
-// INT8 residue GEMMs on tcgen05 and Chinese-remainder reconstruction.
-// True when the Ozaki path handles this problem (double / complex double,
-// op(A) in {T, C}, op(B) = N).
+// C <- alpha * op(A) * op(B) + beta * C for the four dtypes through INT8
+// residue GEMMs on tcgen05 and Chinese-remainder reconstruction.
+// True when the Ozaki path handles this problem: any op(A); op(B) = N, or
+// op(B) in {T, C} read in place (k within the transposing slicer's grid);
+// m <= 2^24, n <= 2^23.
 bool ozaki_supported(const GemmProblem& prob);
+
+// True when op(A) = N is too long along k to be read in place, so that A is
+// first copied k-major into the workspace.
+bool ozaki_copies_a(const GemmProblem& prob);
 
 // Status word of the last ozaki_gemm on this workspace (synchronises
 // `stream`): 0 = ok, 1 = a bounded device wait gave up.

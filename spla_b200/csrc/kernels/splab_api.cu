@@ -95,14 +95,15 @@ GemmProblem make_problem(int dtype, int opA, int opB, int64_t m, int64_t n, int6
 }
 
 // Path selection. An explicit path is taken when it supports the problem
-// (the tensor-core paths need op(A) in {T, C}, op(B) = N; 3xTF32 float dtypes
-// only), else the FP64 DMMA kernel runs. AUTO takes the path with the least
+// (Ozaki: every op pair whose in-place operands fit its slicer's grid;
+// 3xTF32: float dtypes only), else the FP64 DMMA kernel runs. AUTO takes the path with the least
 // modelled time among the supported ones whose workspace fits in a quarter of
 // the device memory. The model's constants were measured on B200 (complex and
 // real, m = n from 128 to 2048, k from 8192 to 65536, and the k = 250000
 // configurations): DMMA at 33 / 29 TFLOP/s (complex / real) plus 0.05 ms; the
 // Ozaki path as slicing (6.0e-13 s per real element and modulus, plus the
-// norms' read at 6 TB/s), INT8 GEMM at 2.8 POP/s scaled by how evenly its work
+// norms' read at 6 TB/s, which rows of 131072 reals or more mostly skip: a
+// 1/16 sample), INT8 GEMM at 2.8 POP/s scaled by how evenly its work
 // units fill the 74 CTA pairs, reconstruction (3e-12 s per real output and
 // modulus) and 0.08 ms; 3xTF32 as splitting (bytes at 5.5 TB/s), three TF32
 // products at 480 TFLOP/s scaled by the same fill, and 0.05 ms. The choice only
@@ -132,15 +133,23 @@ double ozaki_ms(const GemmProblem& p) {
   const double kp = std::ceil(p.k / 128.0) * 128.0;
   const double reals = double(p.m + p.n) * K2;
   // per real element and modulus: complex rows feed three residue planes
-  const double slice =
-      (c ? 6.0e-13 : 4.0e-13) * reals * nmod + reals * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12;
+  // norms: one read per operand; a k-major one with rows of 131072 reals or
+  // more only reads a 1/16 sample (one-pass scaling)
+  const double esz = dtype_is_double(p.dtype) ? 8 : 4;
+  auto norm_rows = [&](double rows, bool k_major) {
+    return rows * K2 * esz / 6e12 / (k_major && K2 >= 131072 ? 16.0 : 1.0);
+  };
+  const double slice = (c ? 6.0e-13 : 4.0e-13) * reals * nmod +
+                       norm_rows(p.m, !(p.opA == 0 && !ozaki_copies_a(p))) +
+                       norm_rows(p.n, p.opB == 0);
   const double tiles = std::ceil(p.m / 256.0) * std::ceil(p.n / 256.0) * nsub;
   const double chunks = std::ceil(kp / 128.0 / 976.0);
   const double gemm = 2.0 * nmod * nsub * p.m * p.n * kp / (2.8e15 * fill(nmod * chunks * tiles));
   const double recon = (c ? 3e-12 * 2.0 : 2e-12) * p.m * double(p.n) * nmod;
-  // op(A) = N: A is first copied k-major (one read, one write)
+  // op(A) = N beyond the in-place reach: A is first copied k-major (one read,
+  // one write)
   const double transpose =
-      p.opA == 0 ? 2.0 * p.m * K2 * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12 : 0.0;
+      ozaki_copies_a(p) ? 2.0 * p.m * K2 * (dtype_is_double(p.dtype) ? 8 : 4) / 6e12 : 0.0;
   return (slice + gemm + recon + transpose) * 1e3 + 0.08;
 }
 
