@@ -15,6 +15,11 @@ headline metric). One step = one contraction of the whole problem.
   paths : TFLOP/s and relative Frobenius error of each contraction path on the
           whole C, against the device double-double product (splab_gemm_dd),
           which is itself checked against the CPU Dot2 oracle on three columns.
+  suite : at one GPU and the default shape, the other configurations of the
+          benchmark suite (real-double ssb, sbs, the 64-instance batches,
+          the adjoint, ssbtr), each run afterwards by `bench.py --workload NAME` in a child
+          process with its own TFLOP/s, timing and whole-C error (--no-suite
+          skips them).
 
 Multi-GPU (torchrun, one rank per GPU): every rank runs its own replica of the
 single-rank problem (the single-rank path has no exchange step); value is the
@@ -516,6 +521,172 @@ def workload_sbs(torch, spla, steps, warmup, path=None):
                        "path": ("auto: " if path is None else "") + name}}
 
 
+def workload_dssb(torch, spla, steps, warmup, path=None):
+    """pdgemm_ssb real double, C = A^T B, k = 20000, m = n = 256, A and B
+    U[-1, 1], C on a 1x1 grid of 64 x 64 blocks, beta = 0 (the reference's
+    CPU-runnable configuration), on the context's path (AUTO by default)."""
+    m = n = 256
+    k = 20000
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20250001)
+    A = torch.rand((m, k), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    B = torch.rand((n, k), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    C = torch.zeros((n, m), dtype=torch.float64, device="cuda")
+    ctx = spla.Context(spla.PU_GPU)
+    if path is not None:
+        ctx.set_fp64_path(path)
+    resolved = spla.lib().splab_gemm_path(1, spla.PATH_AUTO if path is None else path, 1, 0, m,
+                                          n, k)
+    dist = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 64,
+                                                             64)
+
+    def step():
+        spla.pgemm_ssb(m, n, k, spla.OP_TRANSPOSE, 1.0, A, k, B, k, 0.0, C, m, 0, 0, dist, ctx)
+
+    for _ in range(warmup):
+        step()
+    e0, e1 = _events(torch)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    R = torch.zeros((n, m), dtype=torch.float64, device="cuda")
+    assert spla.gemm_dd(1, 1, 0, m, n, k, A, k, B, k, R, m) == 0
+    torch.cuda.synchronize()
+    err = float(torch.linalg.vector_norm(C - R) / torch.linalg.vector_norm(R))
+    name = {1: "FP64 DMMA", 2: "Ozaki INT8", 3: "3xTF32"}[resolved]
+    return {"metric": "DGEMM-SSB TFLOP/s (pdgemm_ssb, real double, A^T B)",
+            "value": 2.0 * m * n * k / (ms / 1e3) / 1e12, "unit": "TFLOP/s", "ms_per_step": ms,
+            "rel_err_whole_c_vs_double_double": err,
+            "config": {"workload": "pdgemm_ssb m=n=256 k=20000 op=T, 1x1 grid 64x64 blocks, "
+                                   "U[-1,1]",
+                       "path": ("auto: " if path is None else "") + name,
+                       "l2": "inputs (82 MB) fit in L2: a per-call figure of a small problem"}}
+
+
+def workload_adjoint(torch, spla, steps, warmup, path=None):
+    """Differentiable ssb -> loss: C = A^H B (complex double, k = 100000,
+    m = n = 512, Gaussian/sqrt(k)), L = ||C - I||_F^2, forward and backward
+    (dA = B dC^H, dB = A dC on the sbs kernels) through
+    spla_b200.autograd on the context's path (AUTO by default). One step is
+    one forward and one backward (three contractions of 8 m n k flops).
+    Checks: the gradients against torch autograd through torch.matmul (cuBLAS
+    FP64), and central differences along 4 random unit directions per operand
+    with Re<grad, dX> (dX the realised step), at h = 1e-6 in the
+    cancellation-free form of the quadratic loss (L(X+) - L(X-) =
+    Re<C+ + C- - 2I, forward(dX)>) and at h = 1e-3 in the plain
+    two-evaluation form."""
+    from spla_b200.autograd import ssb, ssb_autograd
+    m = n = 512
+    k = 100000
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20250005)
+    s = (1.0 / (2.0 * k)) ** 0.5
+    A = torch.randn((m, k), dtype=torch.complex128, device="cuda", generator=g) * s
+    B = torch.randn((n, k), dtype=torch.complex128, device="cuda", generator=g) * s
+    ctx = spla.Context(spla.PU_GPU)
+    if path is not None:
+        ctx.set_fp64_path(path)
+    resolved = spla.lib().splab_gemm_path(3, spla.PATH_AUTO if path is None else path, 2, 0, m,
+                                          n, k)
+    eye = torch.eye(m, n, dtype=torch.complex128, device="cuda")
+    Ar = A.clone().requires_grad_(True)
+    Br = B.clone().requires_grad_(True)
+
+    def step():
+        Ar.grad = Br.grad = None
+        C = ssb_autograd(Ar, Br, ctx)
+        (C - eye).abs().pow(2).sum().backward()
+
+    for _ in range(warmup):
+        step()
+    e0, e1 = _events(torch)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    gA, gB = Ar.grad.detach(), Br.grad.detach()
+    At = A.clone().requires_grad_(True)
+    Bt = B.clone().requires_grad_(True)
+    ((At.conj() @ Bt.T - eye).abs().pow(2).sum()).backward()
+    grad_err = max(float((gA - At.grad).norm() / At.grad.norm()),
+                   float((gB - Bt.grad).norm() / Bt.grad.norm()))
+    del At, Bt
+
+    def loss(C):
+        return float((C - eye).abs().pow(2).sum())
+
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(17)
+    fd_stable = fd_plain = 0.0
+    for which in ("A", "B"):
+        X, grad = (A, gA) if which == "A" else (B, gB)
+        fwd = (lambda Xv: ssb(Xv, B, ctx)) if which == "A" else (lambda Xv: ssb(A, Xv, ctx))
+        for _ in range(4):
+            V = torch.randn(X.shape, dtype=X.dtype, device="cuda", generator=gen)
+            V /= V.norm()
+            Xp, Xm = X + 1e-6 * V, X - 1e-6 * V
+            dX = Xp - Xm
+            an = float((grad.conj() * dX).sum().real)
+            Cp, Cm = fwd(Xp), fwd(Xm)
+            st = float(((Cp + Cm - 2 * eye).conj() * fwd(dX)).sum().real)
+            fd_stable = max(fd_stable, abs(st - an) / abs(an))
+            Xp, Xm = X + 1e-3 * V, X - 1e-3 * V
+            dX = Xp - Xm
+            an = float((grad.conj() * dX).sum().real)
+            fd_plain = max(fd_plain, abs(loss(fwd(Xp)) - loss(fwd(Xm)) - an) / abs(an))
+    name = {1: "FP64 DMMA", 2: "Ozaki INT8", 3: "3xTF32"}[resolved]
+    return {"metric": "ssb adjoint TFLOP/s (forward + backward, complex double)",
+            "value": 3 * 8.0 * m * n * k / (ms / 1e3) / 1e12, "unit": "TFLOP/s",
+            "ms_per_step": ms, "grad_rel_err_vs_torch_cublas": grad_err,
+            "fd_central_h1e-6_cancellation_free_max_rel": fd_stable,
+            "fd_central_h1e-3_plain_max_rel": fd_plain,
+            "config": {"workload": "C = A^H B k=100000 m=n=512, L = ||C - I||_F^2, dA = B dC^H, "
+                                   "dB = A dC (sbs kernels) via torch.autograd.Function",
+                       "path": ("auto: " if path is None else "") + name}}
+
+
+# The configurations of the benchmark suite beside the headline one, each run in
+# its own process (its own device memory) after the headline line's figures are
+# taken: (name, what it stands for).
+SUITE = [("dssb", "pdgemm_ssb real double k=20000 m=n=256 (AUTO)"),
+         ("sbs", "pzgemm_sbs subspace rotation mLocal=200000 n=k=2048 (AUTO)"),
+         ("batch", "64 x pzgemm_ssb, one grouped persistent DMMA launch per sub-batch, autotuned"),
+         ("batch_ozaki", "the same 64 instances on the Ozaki INT8 path"),
+         ("batch_c64_tf32x3", "the 64 instances in complex float on 3xTF32"),
+         ("adjoint", "ssb -> loss forward + backward, complex double k=100000 m=n=512 (AUTO)"),
+         ("ssbtr_float", "psgemm_ssbtr lower real float k=400000 m=n=1536 (AUTO)")]
+
+
+def run_suite(steps, warmup, timeout_s=300):
+    """Runs each SUITE workload as `bench.py --workload NAME` in a child process
+    and returns {name: its JSON line (or the failure), wall seconds}."""
+    out = {}
+    for name, what in SUITE:
+        t0 = time.time()
+        try:
+            p = subprocess.run([sys.executable, str(Path(__file__).resolve()), "--workload", name,
+                                "--steps", str(steps), "--warmup", str(warmup)],
+                               capture_output=True, text=True, timeout=timeout_s)
+            lines = [x for x in p.stdout.splitlines() if x.startswith("{")]
+            if p.returncode == 0 and lines:
+                res = json.loads(lines[-1])
+            else:
+                res = {"error": f"exit {p.returncode}: " + (p.stderr or p.stdout)[-400:]}
+        except subprocess.TimeoutExpired:
+            res = {"error": f"timed out after {timeout_s} s"}
+        res["suite_entry"] = what
+        res["wall_s"] = round(time.time() - t0, 1)
+        out[name] = res
+    return out
+
+
 def workload_ssbtr_float(torch, spla, steps, warmup, path=None):
     """psgemm_ssbtr lower fill, real float, k = 400000, m = n = 1536,
     Gaussian/sqrt(k)."""
@@ -731,7 +902,9 @@ def run_workload(name, steps, warmup):
     import torch
     import spla_b200 as spla
     torch.cuda.set_device(0)
-    fn = {"sbs": workload_sbs,
+    fn = {"dssb": workload_dssb,
+          "adjoint": workload_adjoint,
+          "sbs": workload_sbs,
           "sbs_dmma": lambda t, s, st, w: workload_sbs(t, s, st, w, 1),
           "sbs_ozaki": lambda t, s, st, w: workload_sbs(t, s, st, w, 2),
           "ssbtr_float": workload_ssbtr_float,
@@ -768,10 +941,13 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-peaks", action="store_true")
+    ap.add_argument("--no-suite", action="store_true",
+                    help="skip the other configurations (run by default at one GPU)")
     ap.add_argument("--m", type=int, default=1024, help="m = n (profiling of smaller cases)")
     ap.add_argument("--k", type=int, default=250000, help="k (profiling of smaller cases)")
     ap.add_argument("--workload", default="zgemm_ssb",
-                    choices=["zgemm_ssb", "sbs", "sbs_dmma", "sbs_ozaki", "ssbtr_float",
+                    choices=["zgemm_ssb", "dssb", "adjoint", "sbs", "sbs_dmma", "sbs_ozaki",
+                             "ssbtr_float",
                              "ssbtr_float_dmma",
                              "ssbtr_float_ozaki", "ssbtr_float_tf32x3", "cgemm_ssb_dmma",
                              "cgemm_ssb_ozaki", "cgemm_ssb_tf32x3", "zgemm_nn", "zgemm_nt",
@@ -934,6 +1110,15 @@ def main():
     if dd_check is not None:
         hr["dd_reference_vs_cpu_dot2_3cols"] = dd_check
 
+    suite = None
+    if world == 1 and not args.no_suite and (M, N, K) == (1024, 1024, 250000):
+        # the other configurations, each in a child process with the device memory
+        # of this one released first
+        del A, B
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        suite = run_suite(min(args.steps, 5), 3)
+
     line = {
         "metric": HEADLINE_METRIC,
         "value": hr["tflops"], "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -947,6 +1132,8 @@ def main():
         "roofline": roof, "peaks_measured": peaks, "e2e": e2e, "cpu_baseline": cpu,
         "clocks": clocks, "gpu_launches": launches,
     }
+    if suite is not None:
+        line["suite"] = suite
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -1,7 +1,8 @@
 """bench.py's clock record (host logic, CPU): nvidia-smi samples are kept only
 when they fall inside the timed region of the path asked for, their median SM
 clock and the throttle reasons seen there are reported, and all samples are
-used when none fell inside."""
+used when none fell inside. Also the run of the suite's other configurations
+(one child process each, failures recorded)."""
 import datetime
 import sys
 from pathlib import Path
@@ -47,3 +48,29 @@ def test_all_samples_when_none_inside(tmp_path, monkeypatch):
     monkeypatch.setattr(bench, "TIMED_WINDOWS", [(2, t0 + 5.0, t0 + 6.0)])
     s = clk.summary(2)
     assert s["samples_in_timed_regions"] == 0 and s["samples"] == 2 and s["sm_mhz"] == 1750
+
+
+def test_suite_records_each_configuration_and_its_failure(monkeypatch):
+    """bench.run_suite: one child process per configuration; a JSON line is kept
+    as the result, a non-zero exit or a timeout becomes an error entry and the
+    remaining configurations still run."""
+    import subprocess
+
+    calls = []
+
+    def fake_run(cmd, capture_output, text, timeout):
+        name = cmd[cmd.index("--workload") + 1]
+        calls.append((name, cmd[cmd.index("--steps") + 1], cmd[cmd.index("--warmup") + 1]))
+        if name == "b":
+            return subprocess.CompletedProcess(cmd, 1, "", "CUDA error: out of memory")
+        if name == "c":
+            raise subprocess.TimeoutExpired(cmd, timeout)
+        return subprocess.CompletedProcess(cmd, 0, 'log line\n{"value": 7.5}\n', "")
+
+    monkeypatch.setattr(bench, "SUITE", [("a", "first"), ("b", "second"), ("c", "third")])
+    monkeypatch.setattr(bench.subprocess, "run", fake_run)
+    out = bench.run_suite(5, 3, timeout_s=9)
+    assert [c[0] for c in calls] == ["a", "b", "c"] and calls[0][1:] == ("5", "3")
+    assert out["a"]["value"] == 7.5 and out["a"]["suite_entry"] == "first"
+    assert "out of memory" in out["b"]["error"] and out["b"]["suite_entry"] == "second"
+    assert out["c"]["error"] == "timed out after 9 s"
