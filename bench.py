@@ -688,51 +688,64 @@ def run_suite(steps, warmup, timeout_s=300):
 
 
 def workload_ssbtr_float(torch, spla, steps, warmup, path=None):
-    """psgemm_ssbtr lower fill, real float, k = 400000, m = n = 1536,
-    Gaussian/sqrt(k)."""
+    """psgemm_ssbtr lower fill, real float, k = 400000, m = n = 1536, op = T:
+    the headline figure on Gaussian/sqrt(k) operands, and the same call on
+    U[-1, 1] operands reported beside it (timing and error)."""
     m = n = 1536
     k = 400000
     g = torch.Generator(device="cuda")
     g.manual_seed(20250006)
-    s = (1.0 / k) ** 0.5
-    A = torch.randn((m, k), dtype=torch.float32, device="cuda", generator=g) * s
-    B = torch.randn((n, k), dtype=torch.float32, device="cuda", generator=g) * s
     C = torch.zeros((n, m), dtype=torch.float32, device="cuda")
     ctx = spla.Context(spla.PU_GPU)
     if path is not None:
         ctx.set_fp64_path(path)
+    resolved = spla.lib().splab_gemm_path(0, spla.PATH_AUTO if path is None else path, 1, 0, m,
+                                          n, k)
     dist = spla.MatrixDistribution.create_blacs_block_cyclic(spla.MPI_COMM_SELF, "R", 1, 1, 128,
                                                              128)
+    tri_mask = torch.tril(torch.ones((m, n), dtype=torch.bool, device="cuda")).T  # row >= col
 
-    def step():
-        spla.pgemm_ssbtr(m, n, k, spla.OP_TRANSPOSE, 1.0, A, k, B, k, 0.0, C, m, 0, 0,
-                         spla.FILL_MODE_LOWER, dist, ctx)
+    def measure(A, B):
+        def step():
+            spla.pgemm_ssbtr(m, n, k, spla.OP_TRANSPOSE, 1.0, A, k, B, k, 0.0, C, m, 0, 0,
+                             spla.FILL_MODE_LOWER, dist, ctx)
 
-    for _ in range(warmup):
-        step()
-    e0, e1 = _events(torch)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(steps):
-        step()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    # the whole lower triangle against the device double-double product
-    R = torch.zeros((n, m), dtype=torch.float64, device="cuda")
-    assert spla.gemm_dd(0, 1, 0, m, n, k, A, k, B, k, R, m) == 0
-    torch.cuda.synchronize()
-    tri = torch.tril(torch.ones((m, n), dtype=torch.bool, device="cuda")).T  # (n, m): row >= col
-    diff = (C.double() - R)[tri]
-    err = float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(R[tri]))
+        for _ in range(warmup):
+            step()
+        e0, e1 = _events(torch)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        # the whole lower triangle against the device double-double product
+        R = torch.zeros((n, m), dtype=torch.float64, device="cuda")
+        assert spla.gemm_dd(0, 1, 0, m, n, k, A, k, B, k, R, m) == 0
+        torch.cuda.synchronize()
+        diff = (C.double() - R)[tri_mask]
+        return ms, float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(R[tri_mask]))
+
+    s = (1.0 / k) ** 0.5
+    A = torch.randn((m, k), dtype=torch.float32, device="cuda", generator=g) * s
+    B = torch.randn((n, k), dtype=torch.float32, device="cuda", generator=g) * s
+    ms, err = measure(A, B)
+    A = torch.rand((m, k), dtype=torch.float32, device="cuda", generator=g) * 2 - 1
+    B = torch.rand((n, k), dtype=torch.float32, device="cuda", generator=g) * 2 - 1
+    ms_u, err_u = measure(A, B)
     tri = float(k) * m * (m + 1)
+    name = {1: "FP64-accumulated DMMA", 2: "Ozaki INT8", 3: "3xTF32"}[resolved]
     return {"metric": "SGEMM-SSBTR TFLOP/s (lower triangle, real float)",
             "value": tri / (ms / 1e3) / 1e12, "unit": "TFLOP/s", "ms_per_step": ms,
             "full_matrix_tflops": 2.0 * m * n * k / (ms / 1e3) / 1e12,
             "rel_err_triangle_vs_double_double": err,
-            "config": {"workload": "psgemm_ssbtr m=n=1536 k=400000 lower, op=T",
-                       "path": {None: "auto", 1: "FP64-accumulated DMMA", 2: "Ozaki INT8",
-                                3: "3xTF32"}[path]}}
+            "uniform_inputs": {"value": tri / (ms_u / 1e3) / 1e12, "ms_per_step": ms_u,
+                               "rel_err_triangle_vs_double_double": err_u,
+                               "data": "A, B U[-1,1]"},
+            "config": {"workload": "psgemm_ssbtr m=n=1536 k=400000 lower, op=T, "
+                                   "Gaussian/sqrt(k)",
+                       "path": ("auto: " if path is None else "") + name}}
 
 
 def workload_cgemm_ssb(torch, spla, steps, warmup, path=None):
