@@ -16,10 +16,10 @@ headline metric). One step = one contraction of the whole problem.
           whole C, against the device double-double product (splab_gemm_dd),
           which is itself checked against the CPU Dot2 oracle on three columns.
   suite : at one GPU and the default shape, the other configurations of the
-          benchmark suite (real-double ssb, sbs, the 64-instance batches,
-          the adjoint, ssbtr), each run afterwards by `bench.py --workload NAME` in a child
-          process with its own TFLOP/s, timing and whole-C error (--no-suite
-          skips them).
+          benchmark suite (real-double ssb, sbs, the 64-instance batches, the
+          adjoint, ssbtr), each run afterwards by `bench.py --workload NAME`
+          in a child process; the line keeps their TFLOP/s, time per step,
+          path and whole-C error (--no-suite skips them).
 
 Multi-GPU (torchrun, one rank per GPU): every rank runs its own replica of the
 single-rank problem (the single-rank path has no exchange step); value is the
@@ -664,11 +664,39 @@ SUITE = [("dssb", "pdgemm_ssb real double k=20000 m=n=256 (AUTO)"),
          ("ssbtr_float", "psgemm_ssbtr lower real float k=400000 m=n=1536 (AUTO)")]
 
 
+def _sig(x, digits=4):
+    """x rounded to `digits` significant digits (floats only)."""
+    if not isinstance(x, float) or x == 0.0 or x != x:
+        return x
+    return float(f"{x:.{digits}g}")
+
+
+def compact_entry(res):
+    """The figures of one suite entry that the headline line carries: metric,
+    value, unit, time per step (or per batch), path, every error or check
+    figure, the U[-1,1] figures of ssbtr; the full line is what
+    `bench.py --workload NAME` prints."""
+    out = {k: res[k] for k in ("metric", "unit") if k in res}
+    for k in ("value", "ms_per_step", "ms_per_batch"):
+        if k in res:
+            out[k] = _sig(res[k])
+    if "config" in res:
+        out["path"] = res["config"].get("path")
+    for k, v in res.items():
+        if "err" in k or k.startswith("fd_"):
+            out[k] = _sig(v, 3) if isinstance(v, float) else v
+    if "uniform_inputs" in res:
+        u = res["uniform_inputs"]
+        out["uniform_inputs"] = {"value": _sig(u["value"]),
+                                 "rel_err": _sig(u["rel_err_triangle_vs_double_double"], 3)}
+    return out
+
+
 def run_suite(steps, warmup, timeout_s=300):
     """Runs each SUITE workload as `bench.py --workload NAME` in a child process
-    and returns {name: its JSON line (or the failure), wall seconds}."""
+    and returns {name: its figures (compact_entry) or the failure, wall seconds}."""
     out = {}
-    for name, what in SUITE:
+    for name, _what in SUITE:
         t0 = time.time()
         try:
             p = subprocess.run([sys.executable, str(Path(__file__).resolve()), "--workload", name,
@@ -676,12 +704,11 @@ def run_suite(steps, warmup, timeout_s=300):
                                capture_output=True, text=True, timeout=timeout_s)
             lines = [x for x in p.stdout.splitlines() if x.startswith("{")]
             if p.returncode == 0 and lines:
-                res = json.loads(lines[-1])
+                res = compact_entry(json.loads(lines[-1]))
             else:
                 res = {"error": f"exit {p.returncode}: " + (p.stderr or p.stdout)[-400:]}
         except subprocess.TimeoutExpired:
             res = {"error": f"timed out after {timeout_s} s"}
-        res["suite_entry"] = what
         res["wall_s"] = round(time.time() - t0, 1)
         out[name] = res
     return out
@@ -1026,8 +1053,9 @@ def main():
             if pname == "ozaki":
                 results[pname]["slicing_parts_ms"] = parts
     clocks_by_path = {p: clk.summary(names[p]) for p in results}
-    for p in results:
-        results[p]["clocks"] = clocks_by_path[p]
+    for p in results:  # the sampling note once, in the line's own clocks
+        c = clocks_by_path[p]
+        results[p]["clocks"] = {k: v for k, v in c.items() if k != "sampling"} if c else c
     # accuracy on the whole C against the device double-double reference, which is
     # itself checked against the CPU Dot2 oracle on three columns
     R = dd_reference(torch, spla, A, B)

@@ -71,6 +71,25 @@ def test_suite_records_each_configuration_and_its_failure(monkeypatch):
     monkeypatch.setattr(bench.subprocess, "run", fake_run)
     out = bench.run_suite(5, 3, timeout_s=9)
     assert [c[0] for c in calls] == ["a", "b", "c"] and calls[0][1:] == ("5", "3")
-    assert out["a"]["value"] == 7.5 and out["a"]["suite_entry"] == "first"
-    assert "out of memory" in out["b"]["error"] and out["b"]["suite_entry"] == "second"
+    assert out["a"]["value"] == 7.5 and "wall_s" in out["a"]
+    assert "out of memory" in out["b"]["error"]
     assert out["c"]["error"] == "timed out after 9 s"
+
+
+def test_suite_entry_is_compacted():
+    """compact_entry keeps the figures (value, time, path, errors and checks,
+    the U[-1,1] figures) to 4 (errors 3) significant digits and drops the rest."""
+    full = {"metric": "SGEMM-SSBTR TFLOP/s", "value": 96.9234567, "unit": "TFLOP/s",
+            "ms_per_step": 10.170438385, "full_matrix_tflops": 193.8,
+            "rel_err_triangle_vs_double_double": 3.067538308e-08,
+            "uniform_inputs": {"value": 107.81835, "ms_per_step": 8.75,
+                               "rel_err_triangle_vs_double_double": 2.5299518e-08, "data": "U"},
+            "config": {"workload": "psgemm_ssbtr ...", "path": "auto: Ozaki INT8"},
+            "n_gpus": 1, "steps": 5, "warmup": 3, "data": "synthetic, seeded",
+            "autotune": [{"tile": 0}], "fd_central_h1e-3_plain_max_rel": 8.350186e-08}
+    c = bench.compact_entry(full)
+    assert c == {"metric": "SGEMM-SSBTR TFLOP/s", "unit": "TFLOP/s", "value": 96.92,
+                 "ms_per_step": 10.17, "path": "auto: Ozaki INT8",
+                 "rel_err_triangle_vs_double_double": 3.07e-08,
+                 "fd_central_h1e-3_plain_max_rel": 8.35e-08,
+                 "uniform_inputs": {"value": 107.8, "rel_err": 2.53e-08}}
