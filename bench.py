@@ -692,23 +692,33 @@ def compact_entry(res):
     return out
 
 
-def run_suite(steps, warmup, timeout_s=300):
+def run_suite(steps, warmup, timeout_s=150, budget_s=360):
     """Runs each SUITE workload as `bench.py --workload NAME` in a child process
-    and returns {name: its figures (compact_entry) or the failure, wall seconds}."""
+    and returns {name: its figures (compact_entry) or the failure, wall seconds}.
+    A child gets at most timeout_s seconds and the suite budget_s in all (about
+    80 s are needed on a B200); entries past the budget are skipped and say so,
+    so that the headline line is printed in bounded time."""
     out = {}
+    start = time.time()
     for name, _what in SUITE:
         t0 = time.time()
+        left = budget_s - (t0 - start)
+        if left < 10:
+            out[name] = {"error": f"skipped: the suite's {budget_s} s budget is spent",
+                         "wall_s": 0.0}
+            continue
+        limit = int(min(timeout_s, left))
         try:
             p = subprocess.run([sys.executable, str(Path(__file__).resolve()), "--workload", name,
                                 "--steps", str(steps), "--warmup", str(warmup)],
-                               capture_output=True, text=True, timeout=timeout_s)
+                               capture_output=True, text=True, timeout=limit)
             lines = [x for x in p.stdout.splitlines() if x.startswith("{")]
             if p.returncode == 0 and lines:
                 res = compact_entry(json.loads(lines[-1]))
             else:
                 res = {"error": f"exit {p.returncode}: " + (p.stderr or p.stdout)[-400:]}
         except subprocess.TimeoutExpired:
-            res = {"error": f"timed out after {timeout_s} s"}
+            res = {"error": f"timed out after {limit} s"}
         res["wall_s"] = round(time.time() - t0, 1)
         out[name] = res
     return out

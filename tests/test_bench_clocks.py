@@ -93,3 +93,26 @@ def test_suite_entry_is_compacted():
                  "rel_err_triangle_vs_double_double": 3.07e-08,
                  "fd_central_h1e-3_plain_max_rel": 8.35e-08,
                  "uniform_inputs": {"value": 107.8, "rel_err": 2.53e-08}}
+
+
+def test_suite_time_budget(monkeypatch):
+    """bench.run_suite: a child gets at most the per-child limit and what is
+    left of the suite's budget; once the budget is spent the remaining
+    configurations are skipped with a note instead of run."""
+    import subprocess
+
+    now = [1000.0]
+    limits = []
+
+    def fake_run(cmd, capture_output, text, timeout):
+        limits.append(timeout)
+        now[0] += 100.0  # every child takes 100 s
+        return subprocess.CompletedProcess(cmd, 0, '{"value": 1.0}\n', "")
+
+    monkeypatch.setattr(bench, "SUITE", [(c, c) for c in "abcde"])
+    monkeypatch.setattr(bench.subprocess, "run", fake_run)
+    monkeypatch.setattr(bench.time, "time", lambda: now[0])
+    out = bench.run_suite(5, 3, timeout_s=150, budget_s=305)
+    assert limits == [150, 150, 105]
+    assert [out[c].get("value") for c in "abc"] == [1.0, 1.0, 1.0]
+    assert all("budget" in out[c]["error"] and out[c]["wall_s"] == 0.0 for c in "de")
