@@ -348,3 +348,15 @@ def test_validation_order_and_errors():
 
 def test_local_size_matches_reference():
     _spawn("_local_size_case", {})
+
+
+def test_ssb_three_ranks_3x1_grid_with_mapping():
+    """An odd rank count: a 3 x 1 grid whose grid indices map to ranks 1, 2, 0."""
+    _spawn("_ssb_case", dict(dtype=np.complex64, m=17, n=13, ro=2, co=0, opA=2, dist="bc",
+                             grid=(3, 1, 3, 4), mapping=[1, 2, 0]), world=3)
+
+
+def test_sbs_three_ranks_1x3_grid_with_mapping():
+    """B's blocks gathered from three ranks of a 1 x 3 grid mapped to ranks 2, 0, 1."""
+    _spawn("_sbs_case", dict(dtype=np.complex128, k=31, n=16, bro=1, bco=2, grid=(1, 3, 4, 3),
+                             mapping=[2, 0, 1]), world=3)
