@@ -1,32 +1,37 @@
-"""CPU check of the residue arithmetic of the Ozaki slicer (oz_slice, the
-default complex-double form: four balanced base-2^15 digits, FP32 residues
-through a 1.5 * 2^23 magic constant).
-
-For every default odd modulus p and EVERY digit sum s the four digits of a
-scaled integer |x| < 2^58 can give (d0, d2 in [-2^14, 2^14), d1 in
-[-2^14, 2^14], d3 in [-2^13, 2^13]; s = d0 + c1 d1 + c2 d2 + c3 d3 with
-c_j = 2^(15 j) mod p centred, as the host sets them), the quotient step
-q = fl32(s * fl32(1/p) + M) - M, evaluated here in exact integer arithmetic
-with round-to-nearest-even as the FP32 FMA does, must give the nearest
-integer to s / p, so that the remainder r = s - q p is the centred residue
-with |r| <= 127 (one signed byte). The digit sums themselves stay below 2^24
-(exact in FP32). The same is checked for the third-plane step, t = r(re) +-
-r(im) with |t| <= 254. The moduli and their default count are read from the
-kernel header, so the check follows the code."""
+"""CPU check of the residue arithmetic of the Ozaki slicer (oz_slice):
+digits of the scaled integer x, their sum s = sum_j c_j d_j with c_j =
+base^j mod p centred (as the host sets them), and FP32 residues through a
+1.5 * 2^23 magic constant. Three digit forms, as the slicer picks them:
+  * double, default modulus count: four balanced base-2^15 digits of
+    |x| < 2^58 (d0, d2 in [-2^14, 2^14), d1 in [-2^14, 2^14], d3 in
+    [-2^13, 2^13]); the remainder is formed first, then biased;
+  * double, 16 moduli: five base-2^13 digits of |x| < 2^62 (d0, d2, d3 in
+    [0, 2^13), d1 in [-2^12, 2^12], d4 in [-2^10, 2^10]);
+  * float, default count: three base-2^13 digits of |x| < 2^38 (d0 in
+    [0, 2^13), d1, d2 in [-2^12 - 1, 2^12 + 1]);
+the last two add the bias to s before the remainder, so s + M must be exact
+(|s| < 2^22). For every odd modulus of the form and EVERY digit sum its
+digits can give, the quotient q = fl32(s * fl32(1/p) + M) - M, evaluated in
+exact integer arithmetic with round-to-nearest-even as the FP32 FMA does,
+must be the nearest integer to s / p, so that r = s - q p is the centred
+residue with |r| <= 127 (one signed byte). The same is checked for the
+third-plane step, t = r(re) +- r(im). The moduli and their default counts are
+read from the kernel header, so the check follows the code."""
 import re
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 HDR = Path(__file__).resolve().parent.parent / "spla_b200" / "csrc" / "kernels" / "ozaki_crt.cuh"
 M = 12582912  # 1.5 * 2^23
 
 
-def _moduli():
+def _moduli(count_name):
     text = HDR.read_text()
     table = re.search(r"kModuli\[kMaxModuli\]\s*=\s*\{([^}]*)\}", text).group(1)
     moduli = [int(v) for v in table.replace("\n", " ").split(",") if v.strip()]
-    n = int(re.search(r"kDefaultModuli\s*=\s*(\d+)", text).group(1))
+    n = int(re.search(count_name + r"\s*=\s*(\d+)", text).group(1))
     return moduli[:n]
 
 
@@ -49,14 +54,29 @@ def _quotient(s, p):
     return fl + up.astype(np.int64) - M
 
 
-def test_digit_sums_give_centred_byte_residues():
+# (moduli, digit base, largest |d_j| per digit, bias added before the remainder)
+FORMS = {
+    "double_4x15": (lambda: _moduli("kDefaultModuli"), 1 << 15,
+                    [1 << 14, 1 << 14, 1 << 14, 1 << 13], False),
+    "double_5x13": (lambda: _moduli("kMaxUsableModuli"), 1 << 13,
+                    [(1 << 13) - 1, 1 << 12, (1 << 13) - 1, (1 << 13) - 1, 1 << 10], True),
+    "float_3x13": (lambda: _moduli("kDefaultModuliFloat"), 1 << 13,
+                   [(1 << 13) - 1, (1 << 12) + 1, (1 << 12) + 1], True),
+}
+
+
+@pytest.mark.parametrize("form", list(FORMS))
+def test_digit_sums_give_centred_byte_residues(form):
+    moduli_of, base, dmax, bias_first = FORMS[form]
     checked = 0
-    for p in _moduli():
+    for p in moduli_of():
         if p == 256:  # residue = low byte of the lowest digit, no quotient step
             continue
-        c = [_centred(pow(1 << 15, j, p), p) for j in (1, 2, 3)]
-        smax = (1 << 14) + abs(c[0]) * (1 << 14) + abs(c[1]) * (1 << 14) + abs(c[2]) * (1 << 13)
+        c = [1] + [_centred(pow(base, j, p), p) for j in range(1, len(dmax))]
+        smax = sum(abs(cj) * dj for cj, dj in zip(c, dmax))
         assert smax < (1 << 23), (p, smax)  # FMA chain exact; quotient input in range
+        if bias_first:
+            assert smax < (1 << 22), (p, smax)  # s + M exact
         for lo in range(-smax, smax + 1, 1 << 22):
             s = np.arange(lo, min(lo + (1 << 22), smax + 1), dtype=np.int64)
             q = _quotient(s, p)
@@ -70,4 +90,4 @@ def test_digit_sums_give_centred_byte_residues():
         t = np.arange(-2 * h, 2 * h + 1, dtype=np.int64)
         r = t - _quotient(t, p) * p
         assert np.all(2 * np.abs(r) <= p) and np.all((r - t) % p == 0), p
-    assert checked > 50_000_000
+    assert checked > 1_000_000
