@@ -2,7 +2,8 @@
 when they fall inside the timed region of the path asked for, their median SM
 clock and the throttle reasons seen there are reported, and all samples are
 used when none fell inside. Also the run of the suite's other configurations
-(one child process each, failures recorded)."""
+(one child process each, failures recorded, a time budget), and the reference
+arm's line (the headline's metric and workload on the reference CPU path)."""
 import datetime
 import sys
 from pathlib import Path
@@ -116,3 +117,30 @@ def test_suite_time_budget(monkeypatch):
     assert limits == [150, 150, 105]
     assert [out[c].get("value") for c in "abc"] == [1.0, 1.0, 1.0]
     assert all("budget" in out[c]["error"] and out[c]["wall_s"] == 0.0 for c in "de")
+
+
+def test_reference_arm_line_matches_the_headline(tmp_path):
+    """`bench.py --impl reference` (the reference library's CPU path on the
+    whole headline workload) prints the headline's metric, unit, direction and
+    workload, a time per step and the e2e and cpu_baseline objects, so that its
+    value and the GPU arm's can be divided."""
+    import json
+    import os
+    import subprocess
+
+    import oracle
+    if not oracle.REF_LIB.exists():
+        import pytest
+        pytest.skip("reference library not built (oracle/_ref)")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    p = subprocess.run([sys.executable, str(Path(bench.__file__)), "--impl", "reference",
+                        "--steps", "1", "--warmup", "0"], capture_output=True, text=True,
+                       timeout=600, env=env)
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = json.loads([x for x in p.stdout.splitlines() if x.startswith("{")][-1])
+    assert line["metric"] == bench.HEADLINE_METRIC and line["unit"] == "TFLOP/s"
+    assert line["higher_is_better"] is True and line["impl"] == "reference"
+    assert line["config"]["workload"] == bench.workload_name()
+    assert line["steps"] == 1 and line["warmup"] == 0 and line["ms_per_step"] > 0
+    assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
